@@ -1,0 +1,356 @@
+"""Benchmark of the H-matrix hot path on B200.
+
+Workload (one step): the H-matrix x dense product of the 64-right-hand-side
+case -- HMat2d<double> on a 128 x 128 grid (N = 16384), numLevels 5 (leaf
+clusters of 64 points; a 32-point leaf is not representable on a quadtree
+over a 128 x 128 grid), maxRank 16, strong admissibility, every admissible
+block at full rank maxRank (SetToRandom, the reference's own matvec
+benchmark operator), times a 16384 x 64 standard-normal block.  The
+operator's 274 MB of block data exceed the 126 MB L2, so every step streams
+it from HBM.
+
+Reported: algorithmic GB/s (bytes of all stored blocks + input + output per
+step / step time), the roofline of the dominant kernel from CUDA events,
+an end-to-end figure through the C ABI with host buffers, and the CPU
+baseline (the reference library built from its sources, timed on this
+host's cores over a bounded sample).
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Schulz-inverse s and H-matvec GB/s at 1e-8 rel err: mixed/learned vs plain FP64"
+SIZES, LEVELS, RANK, NRHS, SEED = (128, 128), 5, 16, 64, 2
+REF_DRIVER = os.path.join(ROOT, "oracle", "_ref", "dmhm_ref_driver")
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def algorithmic_bytes(H, nrhs):
+    c = H.BlockCensus()
+    N = H.Height()
+    return c["bytes"] + 2 * N * 8 * nrhs, c
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        try:
+            rows = [l.split(",") for l in open(self.path).read().strip().splitlines()]
+            os.unlink(self.path)
+        except Exception:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows if len(r) >= 9]
+        mx = [float(r[2]) for r in rows if len(r) >= 9]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def reference_arm(args):
+    """The reference's own CPU implementation (built from its sources by
+    oracle/Makefile) on this host's cores, same workload and metric."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    if not os.path.exists(REF_DRIVER):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/dmhm_ref_driver was not built (no reference sources)"}))
+        return
+    coef = 1.0 + np.random.default_rng(SEED).random(SIZES[0] * SIZES[1])
+    X = np.random.default_rng(SEED + 1).standard_normal((SIZES[0] * SIZES[1], NRHS))
+    seconds, nbytes = run_reference_driver(coef, X, repeat=args.warmup + args.steps,
+                                           threads=cores)
+    value = nbytes / seconds / 1e9
+    line = {"metric": METRIC, "value": value, "unit": "GB/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": seconds * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(),
+            "cpu_baseline": {"value": value, "unit": "GB/s", "cores": cores,
+                             "kind": "reference",
+                             "sample": f"{args.warmup + args.steps} full H x (N x 64) products, "
+                                       "mean time per product"},
+            "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_reference_driver(coef, X, repeat, threads):
+    N = X.shape[0]
+    with tempfile.TemporaryDirectory() as tmp:
+        cp, xp = os.path.join(tmp, "c.bin"), os.path.join(tmp, "x.bin")
+        coef.tofile(cp)
+        np.asfortranarray(X).T.copy().tofile(xp)
+        env = {**os.environ, "OPENBLAS_NUM_THREADS": str(threads)}
+        cmd = [REF_DRIVER, "matvec", "--dim", "2", "--nx", str(SIZES[0]), "--ny", str(SIZES[1]),
+               "--levels", str(LEVELS), "--rank", str(RANK), "--coef", cp, "--x", xp,
+               "--nrhs", str(X.shape[1]), "--random", "1", "--repeat", str(repeat)]
+        r = subprocess.run(cmd, capture_output=True, text=True, env=env, check=True)
+        info = json.loads(r.stdout.strip().splitlines()[-1])
+    # algorithmic bytes of the same operator (census is structural)
+    return float(info["seconds"]), ref_bytes(N, X.shape[1])
+
+
+def ref_bytes(N, nrhs):
+    return census_bytes(SIZES, LEVELS, RANK) + 2 * N * 8 * nrhs
+
+
+def census_bytes(sizes, levels, rank, strong=True):
+    """Bytes of the SetToRandom operator's blocks (dense leaves m*n, low-rank
+    (m+n)*rank), from the block structure alone (include/dmhm/hmat2d.hpp:
+    288-341, admissibility src/HMat2d/HMat2d.cpp:797-809)."""
+    d = len(sizes)
+
+    def kids(box):
+        coord, size = box
+        lo = [s // 2 for s in size]
+        out = []
+        for q in range(1 << d):
+            bits = [(q >> k) & 1 for k in range(d)]
+            out.append((tuple(2 * c + b for c, b in zip(coord, bits)),
+                        tuple(size[k] - lo[k] if bits[k] else lo[k] for k in range(d))))
+        return out
+
+    def rec(t, s, level):
+        dif = [abs(a - b) for a, b in zip(t[0], s[0])]
+        m, n = int(np.prod(t[1])), int(np.prod(s[1]))
+        if (max(dif) > 1) if strong else any(dif):
+            return (m + n) * rank
+        if levels - level > 1:
+            return sum(rec(tc, sc, level + 1) for tc in kids(t) for sc in kids(s))
+        return m * n
+
+    root = (tuple([0] * d), tuple(sizes))
+    return 8 * rec(root, root, 0)
+
+
+def workload_config():
+    return {"workload": "HMat2d<double> 128x128 grid (N=16384), numLevels 5 (64-point leaves), "
+                        "maxRank 16, strong admissibility, SetToRandom blocks; H x 64 RHS",
+            "global_batch": NRHS, "seq_len": SIZES[0] * SIZES[1], "parallelism": "replicas",
+            "l2": "operator data (274 MB) larger than L2 (126 MB); no flush needed"}
+
+
+def gpu_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    import dmhm_b200 as D
+    from dmhm_b200 import _lib
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    stream = torch.cuda.Stream()
+    ctx = D.Context(local, stream=stream.cuda_stream)
+    coef = D.operators.uniform_coefficients(SIZES, SEED)
+    S = D.operators.stencil(SIZES, coef, LEVELS)
+    H = D.HMat2d(S, LEVELS, RANK, True, *SIZES, ctx=ctx)
+    H.SetToRandom()
+    N = H.Height()
+    Xh = np.random.default_rng(SEED + 1).standard_normal((N, NRHS))
+    X = torch.tensor(Xh, device="cuda").t().contiguous()       # column-major N x k
+    Y = torch.empty((NRHS, N), dtype=torch.float64, device="cuda")
+    lib = _lib.lib()
+    import ctypes as C
+
+    def step():
+        _lib.check(lib.hm_multiply_dense(H.handle, 0, 1.0, C.c_void_p(X.data_ptr()), N, 0.0,
+                                         C.c_void_p(Y.data_ptr()), N, NRHS))
+
+    nbytes, census = algorithmic_bytes(H, NRHS)
+    for _ in range(args.warmup):
+        step()
+    ctx.synchronize()
+    if world > 1:
+        dist.barrier()
+    ctx.synchronize()
+    # timed region: CUDA events on the context's stream around the K steps
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = lib.hm_kernel_launches()
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        ctx.synchronize()
+        wall = time.perf_counter() - t0
+    launches = lib.hm_kernel_launches() - launches0
+    step_ms = ev0.elapsed_time(ev1) / args.steps
+    if world > 1:
+        t = torch.tensor([step_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_ms = float(t.item())
+    value = world * nbytes / (step_ms * 1e-3) / 1e9
+    # per-kernel event timing (separate pass, events bracket each launch)
+    _lib.check(lib.hm_profile_enable(ctx.handle, 1))
+    for _ in range(args.steps):
+        step()
+    prof = read_profile(ctx)
+    _lib.check(lib.hm_profile_enable(ctx.handle, 0))
+
+    # roofline of the dominant kernel
+    hbm_peak, peak_kind = peaks()
+    top = max(prof.items(), key=lambda kv: kv[1]["ms"])
+    kname, kv = top
+    per_launch_ms = kv["ms"] / kv["launches"]
+    kbytes = kernel_bytes(kname, census, N, NRHS, H)
+    achieved = kbytes / (per_launch_ms * 1e-3) / 1e9
+
+    # end to end through the C ABI with host buffers
+    Xp = np.asfortranarray(Xh)
+    Yp = np.zeros((N, NRHS), order="F")
+    e2e_steps = max(3, args.steps // 2)
+    H.Multiply(1.0, Xp)
+    ctx.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        _lib.check(lib.hm_multiply_dense_host(H.handle, 0, 1.0, Xp.ctypes.data_as(_lib._PD), N,
+                                              0.0, Yp.ctypes.data_as(_lib._PD), N, NRHS))
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    e2e_val = world * nbytes / e2e_s / 1e9
+
+    line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "config": workload_config(),
+            "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved,
+                         "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                         "peak_source": peak_kind, "traffic": None,
+                         "algorithmic_bytes_per_launch": kbytes},
+            "e2e": {"value": e2e_val, "unit": "GB/s", "h2d_bytes_per_step": N * NRHS * 8,
+                    "d2h_bytes_per_step": N * NRHS * 8},
+            "gpu_launches": int(launches), "clocks": clk.summary(),
+            "wall_ms_per_step": wall * 1e3 / args.steps,
+            "kernels": {k: {"ms_per_launch": v["ms"] / v["launches"], "launches": v["launches"]}
+                        for k, v in prof.items()}}
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(coef, Xh, nbytes)
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def kernel_bytes(name, census, N, nrhs, H):
+    """Algorithmic bytes one launch of `name` must move: phase 1 reads every
+    V (n x r) and its input rows; phase 2 reads every U row slice and dense
+    leaf once and writes the output."""
+    from dmhm_b200 import _lib  # noqa: F401
+    tot = census["bytes"]
+    if name == "hmm_lowrank_inner":
+        return tot // 2 + N * 8 * nrhs            # roughly the V half of the low-rank data
+    return tot + 2 * N * 8 * nrhs
+
+
+def read_profile(ctx):
+    import ctypes as C
+    from dmhm_b200 import _lib
+    out = {}
+    i = 0
+    name = C.create_string_buffer(128)
+    while True:
+        ms, n = C.c_double(), C.c_int64()
+        st = _lib.lib().hm_profile_read(ctx.handle, i, name, 128, C.byref(ms), C.byref(n))
+        if st != 0:
+            break
+        out[name.value.decode()] = {"ms": ms.value, "launches": n.value}
+        i += 1
+    return out
+
+
+def cpu_baseline(coef, X, nbytes):
+    if not os.path.exists(REF_DRIVER):
+        return {"value": None, "unit": "GB/s", "cores": 1, "kind": "reference",
+                "sample": "unavailable: oracle/_ref not built"}
+    reps = 10
+    seconds, _ = run_reference_driver(coef, X, repeat=reps, threads=1)
+    return {"value": nbytes / seconds / 1e9, "unit": "GB/s", "cores": 1, "kind": "reference",
+            "sample": f"{reps} full H x (N x 64) products on one core (OPENBLAS_NUM_THREADS=1), "
+                      f"{seconds * 1e3:.1f} ms each"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,355 @@
+// C ABI (include/dmhm_b200.h): argument checks, error capture, and the host
+// side of each entry point.
+#include <algorithm>
+#include <cstring>
+#include <string>
+
+#include "engine.h"
+#include "rng.cuh"
+
+struct hm_context_s {
+    hmb::Context c;
+};
+
+struct hm_matrix_s {
+    hmb::HMatrix h;
+};
+
+namespace hmb {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+std::atomic<unsigned long long> g_launches{0};
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+void Context::collect() {
+    HMB_CUDA(cudaStreamSynchronize(stream));
+    for (auto& p : pending) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, p.a, p.b);
+        Totals& t = totals[p.name];
+        t.ms += ms;
+        t.launches += 1;
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+    }
+    pending.clear();
+}
+
+template <typename F>
+int guarded(F&& f) {
+    try {
+        f();
+        return HM_OK;
+    } catch (const Error& e) {
+        set_last_error(e.what());
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        set_last_error("host allocation failed");
+        return HM_ERR_OOM;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return HM_ERR_INTERNAL;
+    }
+}
+
+// Host-side import of a CSR matrix in hierarchical order
+// (ImportSparse, src/HMat2d/HMat2d.cpp:961-1033; ConvertSubmatrix,
+// src/hmat_tools/ConvertSubmatrix.cpp:14-119): dense leaves copy their
+// entries; an admissible block gets one rank-1 term per nonzero it holds,
+// U = unit column, V = value column.
+void import_csr(HMatrix& H, const int64_t* rows, const int32_t* cols,
+                const double* vals) {
+    const Structure& S = *H.S;
+    H.rank.assign(S.blocks.size(), 0);
+    // count nonzeros per admissible block
+    std::vector<std::vector<std::pair<int, int>>> lr_entries(S.blocks.size());
+    auto find_leaf = [&](int i, int j) {
+        int b = 0;
+        while (S.blocks[b].kind == KIND_NODE) {
+            const Block& B = S.blocks[b];
+            int t = 0, s = 0;
+            const Box& TB = S.boxes[B.tgt_box];
+            const Box& SB = S.boxes[B.src_box];
+            for (int c = 0; c < S.q; ++c) {
+                const Box& cb = S.boxes[TB.first_child + c];
+                if (i >= cb.offset && i < cb.offset + cb.count) { t = c; break; }
+            }
+            for (int c = 0; c < S.q; ++c) {
+                const Box& cb = S.boxes[SB.first_child + c];
+                if (j >= cb.offset && j < cb.offset + cb.count) { s = c; break; }
+            }
+            b = S.child(b, t, s);
+        }
+        return b;
+    };
+    const int N = S.N;
+    std::vector<int> leaf_of_entry;
+    leaf_of_entry.reserve((size_t)rows[N]);
+    for (int i = 0; i < N; ++i)
+        for (int64_t k = rows[i]; k < rows[i + 1]; ++k) {
+            int j = cols[k];
+            HMB_REQUIRE(j >= 0 && j < N, HM_ERR_ARGUMENT, "CSR column index out of range");
+            int b = find_leaf(i, j);
+            leaf_of_entry.push_back(b);
+            if (S.blocks[b].kind == KIND_LOWRANK) H.rank[b]++;
+        }
+    H.layout();
+    std::vector<double> host((size_t)std::max<long long>(H.total, 0), 0.0);
+    std::vector<int> used(S.blocks.size(), 0);
+    size_t e = 0;
+    for (int i = 0; i < N; ++i)
+        for (int64_t k = rows[i]; k < rows[i + 1]; ++k, ++e) {
+            int b = leaf_of_entry[e];
+            const Block& B = S.blocks[b];
+            int li = i - B.row_off, lj = cols[k] - B.col_off;
+            if (B.kind == KIND_DENSE) {
+                host[H.off[b] + li + (long long)lj * B.m] = vals[k];
+            } else {
+                int r = used[b]++;
+                host[H.off[b] + li + (long long)r * B.m] = 1.0;
+                host[H.off[b] + (long long)B.m * H.rank[b] + lj + (long long)r * B.n] = vals[k];
+            }
+        }
+    if (H.total > 0)
+        HMB_CUDA(cudaMemcpyAsync(H.data.get(), host.data(), host.size() * sizeof(double),
+                                 cudaMemcpyHostToDevice, H.ctx->stream));
+    HMB_CUDA(cudaStreamSynchronize(H.ctx->stream));
+}
+
+void multiply_dense(HMatrix& H, int transpose, double alpha, const double* B,
+                    int ldb, double beta, double* C, int ldc, int nrhs) {
+    HMB_REQUIRE(nrhs >= 0, HM_ERR_ARGUMENT, "nrhs must be >= 0");
+    const int m = transpose ? H.width() : H.height();
+    const int n = transpose ? H.height() : H.width();
+    HMB_REQUIRE(ldb >= std::max(1, n) && ldc >= std::max(1, m), HM_ERR_ARGUMENT,
+                "leading dimension too small");
+    if (nrhs == 0 || m == 0) return;
+    auto key = std::make_pair(transpose != 0 ? 1 : 0, nrhs);
+    auto it = H.plans.find(key);
+    if (it == H.plans.end()) {
+        PlanPtr p = build_plan(*H.ctx, {JobSpec{&H, 0, transpose != 0, nrhs}});
+        it = H.plans.emplace(key, std::shared_ptr<MatPlan>(p.release(), MatPlanDeleter())).first;
+    }
+    execute_plan(*H.ctx, *it->second, {JobArgs{B, C, alpha, beta, ldb, ldc, nrhs, 0}});
+}
+
+}  // namespace hmb
+
+using namespace hmb;
+
+extern "C" {
+
+const char* hm_last_error(void) { return g_last_error.c_str(); }
+
+int hm_version(void) { return 100; }
+
+int hm_context_create(int device, void* cuda_stream, hm_context* out) {
+    return guarded([&] {
+        HMB_REQUIRE(out != nullptr, HM_ERR_ARGUMENT, "out is NULL");
+        *out = nullptr;
+        int count = 0;
+        HMB_CUDA(cudaGetDeviceCount(&count));
+        HMB_REQUIRE(device >= 0 && device < count, HM_ERR_ARGUMENT, "no such CUDA device");
+        HMB_CUDA(cudaSetDevice(device));
+        auto* c = new hm_context_s;
+        c->c.device = device;
+        c->c.serial_state = kLcgSeed;
+        c->c.parallel_state = kLcgSeed;
+        cudaDeviceGetAttribute(&c->c.num_sms, cudaDevAttrMultiProcessorCount, device);
+        if (cuda_stream) {
+            c->c.stream = (cudaStream_t)cuda_stream;
+        } else {
+            cudaError_t err = cudaStreamCreateWithFlags(&c->c.stream, cudaStreamNonBlocking);
+            if (err != cudaSuccess) {
+                delete c;
+                throw Error(HM_ERR_CUDA, cudaGetErrorString(err));
+            }
+            c->c.own_stream = true;
+        }
+        *out = c;
+    });
+}
+
+int hm_context_destroy(hm_context ctx) {
+    return guarded([&] {
+        if (!ctx) return;
+        cudaStreamSynchronize(ctx->c.stream);
+        if (ctx->c.own_stream) cudaStreamDestroy(ctx->c.stream);
+        delete ctx;
+    });
+}
+
+int hm_context_synchronize(hm_context ctx) {
+    return guarded([&] {
+        HMB_REQUIRE(ctx, HM_ERR_ARGUMENT, "ctx is NULL");
+        HMB_CUDA(cudaStreamSynchronize(ctx->c.stream));
+    });
+}
+
+int hm_set_oversample(hm_context ctx, int oversample) {
+    return guarded([&] {
+        HMB_REQUIRE(ctx, HM_ERR_ARGUMENT, "ctx is NULL");
+        HMB_REQUIRE(oversample >= 0, HM_ERR_ARGUMENT, "oversample must be >= 0");
+        ctx->c.oversample = oversample;
+    });
+}
+
+int hm_get_oversample(hm_context ctx, int* oversample) {
+    return guarded([&] {
+        HMB_REQUIRE(ctx && oversample, HM_ERR_ARGUMENT, "NULL argument");
+        *oversample = ctx->c.oversample;
+    });
+}
+
+int hm_set_lcg_states(hm_context ctx, uint64_t serial, uint64_t parallel) {
+    return guarded([&] {
+        HMB_REQUIRE(ctx, HM_ERR_ARGUMENT, "ctx is NULL");
+        ctx->c.serial_state = serial;
+        ctx->c.parallel_state = parallel;
+    });
+}
+
+int hm_get_lcg_states(hm_context ctx, uint64_t* serial, uint64_t* parallel) {
+    return guarded([&] {
+        HMB_REQUIRE(ctx && serial && parallel, HM_ERR_ARGUMENT, "NULL argument");
+        *serial = ctx->c.serial_state;
+        *parallel = ctx->c.parallel_state;
+    });
+}
+
+int hm_natural_to_hierarchical_map(int dim, const int* sizes, int num_levels, int* map) {
+    return guarded([&] {
+        HMB_REQUIRE(sizes && map, HM_ERR_ARGUMENT, "NULL argument");
+        HMB_REQUIRE(num_levels >= 1, HM_ERR_ARGUMENT, "num_levels must be >= 1");
+        natural_to_hierarchical(dim, sizes, num_levels, map);
+    });
+}
+
+int hm_create_from_csr(hm_context ctx, int dim, const int* sizes, int num_levels,
+                       int max_rank, int strongly_admissible, const int64_t* row_offsets,
+                       const int32_t* col_indices, const double* values, hm_matrix* out) {
+    return guarded([&] {
+        HMB_REQUIRE(ctx && sizes && row_offsets && out, HM_ERR_ARGUMENT, "NULL argument");
+        HMB_REQUIRE(max_rank >= 0, HM_ERR_ARGUMENT, "max_rank must be >= 0");
+        *out = nullptr;
+        HMB_CUDA(cudaSetDevice(ctx->c.device));
+        auto* m = new hm_matrix_s;
+        try {
+            m->h.ctx = &ctx->c;
+            m->h.S = build_structure(dim, sizes, num_levels, strongly_admissible != 0);
+            m->h.max_rank = max_rank;
+            const int64_t nnz = row_offsets[m->h.S->N];
+            HMB_REQUIRE(nnz == 0 || (col_indices && values), HM_ERR_ARGUMENT,
+                        "NULL CSR arrays");
+            import_csr(m->h, row_offsets, col_indices, values);
+        } catch (...) {
+            delete m;
+            throw;
+        }
+        *out = m;
+    });
+}
+
+int hm_destroy(hm_matrix h) {
+    return guarded([&] {
+        if (!h) return;
+        delete h;
+    });
+}
+
+int hm_info(hm_matrix h, int* height, int* width, int* num_levels, int* max_rank,
+            int64_t* counts, int64_t* bytes) {
+    return guarded([&] {
+        HMB_REQUIRE(h, HM_ERR_ARGUMENT, "h is NULL");
+        const Structure& S = *h->h.S;
+        if (height) *height = S.N;
+        if (width) *width = S.N;
+        if (num_levels) *num_levels = S.num_levels;
+        if (max_rank) *max_rank = h->h.max_rank;
+        if (counts) {
+            int64_t c[4] = {0, 0, 0, 0};
+            for (size_t b = 0; b < S.blocks.size(); ++b) {
+                c[S.blocks[b].kind]++;
+                if (S.blocks[b].kind == KIND_LOWRANK) c[3] += h->h.rank[b];
+            }
+            std::memcpy(counts, c, sizeof(c));
+        }
+        if (bytes) *bytes = h->h.total * (int64_t)sizeof(double);
+    });
+}
+
+int hm_set_to_random(hm_matrix h) {
+    return guarded([&] {
+        HMB_REQUIRE(h, HM_ERR_ARGUMENT, "h is NULL");
+        launch_fill_random(*h->h.ctx, h->h);
+    });
+}
+
+int hm_multiply_dense(hm_matrix h, int transpose, double alpha, const double* B, int ldb,
+                      double beta, double* C, int ldc, int nrhs) {
+    return guarded([&] {
+        HMB_REQUIRE(h && (nrhs == 0 || (B && C)), HM_ERR_ARGUMENT, "NULL argument");
+        multiply_dense(h->h, transpose, alpha, B, ldb, beta, C, ldc, nrhs);
+    });
+}
+
+int hm_multiply_dense_host(hm_matrix h, int transpose, double alpha, const double* B, int ldb,
+                           double beta, double* C, int ldc, int nrhs) {
+    return guarded([&] {
+        HMB_REQUIRE(h && (nrhs == 0 || (B && C)), HM_ERR_ARGUMENT, "NULL argument");
+        Context& ctx = *h->h.ctx;
+        const int m = transpose ? h->h.width() : h->h.height();
+        const int n = transpose ? h->h.height() : h->h.width();
+        HMB_REQUIRE(ldb >= std::max(1, n) && ldc >= std::max(1, m), HM_ERR_ARGUMENT,
+                    "leading dimension too small");
+        if (nrhs == 0) return;
+        DeviceBuffer<double> dB, dC;
+        dB.allocate((size_t)n * nrhs, ctx.stream);
+        dC.allocate((size_t)m * nrhs, ctx.stream);
+        HMB_CUDA(cudaMemcpy2DAsync(dB.get(), n * sizeof(double), B, ldb * sizeof(double),
+                                   n * sizeof(double), nrhs, cudaMemcpyHostToDevice, ctx.stream));
+        if (beta != 0.0)
+            HMB_CUDA(cudaMemcpy2DAsync(dC.get(), m * sizeof(double), C, ldc * sizeof(double),
+                                       m * sizeof(double), nrhs, cudaMemcpyHostToDevice,
+                                       ctx.stream));
+        multiply_dense(h->h, transpose, alpha, dB.get(), n, beta, dC.get(), m, nrhs);
+        HMB_CUDA(cudaMemcpy2DAsync(C, ldc * sizeof(double), dC.get(), m * sizeof(double),
+                                   m * sizeof(double), nrhs, cudaMemcpyDeviceToHost, ctx.stream));
+        HMB_CUDA(cudaStreamSynchronize(ctx.stream));
+    });
+}
+
+unsigned long long hm_kernel_launches(void) {
+    return g_launches.load(std::memory_order_relaxed);
+}
+
+int hm_profile_enable(hm_context ctx, int on) {
+    return guarded([&] {
+        HMB_REQUIRE(ctx, HM_ERR_ARGUMENT, "ctx is NULL");
+        ctx->c.collect();
+        ctx->c.totals.clear();
+        ctx->c.profiling = on != 0;
+    });
+}
+
+int hm_profile_read(hm_context ctx, int index, char* name, int name_cap, double* ms,
+                    int64_t* launches) {
+    return guarded([&] {
+        HMB_REQUIRE(ctx && name && ms && launches && name_cap > 0, HM_ERR_ARGUMENT,
+                    "NULL argument");
+        ctx->c.collect();
+        HMB_REQUIRE(index >= 0 && index < (int)ctx->c.totals.size(), HM_ERR_ARGUMENT,
+                    "profile index out of range");
+        auto it = ctx->c.totals.begin();
+        std::advance(it, index);
+        std::snprintf(name, (size_t)name_cap, "%s", it->first.c_str());
+        *ms = it->second.ms;
+        *launches = it->second.launches;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,143 @@
+// Engine objects behind the C ABI: the context (device, stream, generators,
+// workspace) and the device-resident H-matrix.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common.h"
+#include "structure.h"
+
+namespace hmb {
+
+// Per-block table entry the kernels read (32 bytes).
+struct DevBlock {
+    int kind, m, n, rank;
+    int row_off, col_off, pad0, pad1;
+    long long off;   // element offset of U (low-rank, V follows at off+m*rank) or D
+};
+
+struct Context {
+    int device = 0;
+    cudaStream_t stream = 0;
+    bool own_stream = false;
+    int oversample = 4;
+    // Next raw state of the serial / parallel LCG (src/core/random.cpp:13-25).
+    uint64_t serial_state = 0, parallel_state = 0;
+    int num_sms = 148;
+    // Work lists and scratch are stream-ordered allocations (cudaMallocAsync
+    // / cudaFreeAsync on `stream`), freed right after the launches that use
+    // them are queued.
+
+    // Optional per-kernel timing with CUDA events on `stream`.
+    bool profiling = false;
+    struct Pending { std::string name; cudaEvent_t a, b; };
+    std::vector<Pending> pending;
+    struct Totals { double ms = 0; long long launches = 0; };
+    std::map<std::string, Totals> totals;
+    void collect();   // synchronizes, folds pending event pairs into totals
+};
+
+// Counts every kernel launch of the library (all contexts).
+extern std::atomic<unsigned long long> g_launches;
+
+// Brackets one kernel launch: counts it and, when profiling, records events.
+class LaunchScope {
+  public:
+    LaunchScope(Context& c, const char* name) : c_(c), name_(name) {
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+        if (c_.profiling) {
+            cudaEventCreate(&a_);
+            cudaEventCreate(&b_);
+            cudaEventRecord(a_, c_.stream);
+        }
+    }
+    ~LaunchScope() {
+        if (c_.profiling) {
+            cudaEventRecord(b_, c_.stream);
+            c_.pending.push_back({name_, a_, b_});
+        }
+    }
+  private:
+    Context& c_;
+    const char* name_;
+    cudaEvent_t a_ = nullptr, b_ = nullptr;
+};
+
+class HMatrix {
+  public:
+    Context* ctx = nullptr;
+    std::shared_ptr<Structure> S;
+    int max_rank = 0;
+    std::vector<int> rank;          // per block (low-rank blocks)
+    std::vector<long long> off;     // per block data offset (elements)
+    long long total = 0;            // elements in `data`
+    DeviceBuffer<double> data;
+    DeviceBuffer<DevBlock> table;   // device copy of the per-block table
+    // Cached whole-matrix multiply plans keyed by (transpose, k); dropped
+    // whenever the storage is re-laid out.
+    std::map<std::pair<int, int>, std::shared_ptr<struct MatPlan>> plans;
+
+    int height() const { return S->N; }
+    int width() const { return S->N; }
+    // Computes offsets from `rank`, (re)allocates `data` (uninitialized) and
+    // uploads the table.
+    void layout();
+    void upload_table();
+    double* U(int b) const { return data.get() + off[b]; }
+    double* V(int b) const { return data.get() + off[b] + (long long)S->blocks[b].m * rank[b]; }
+    double* D(int b) const { return data.get() + off[b]; }
+};
+
+// Multiplication jobs: out = alpha op(H restricted to subtree `root`) in
+// (+ beta out).  `in` points at the input row that corresponds to the root's
+// first column (first row for op = transpose); `out` likewise for its output.
+struct MatJob {
+    const HMatrix* H;
+    int root;
+    bool trans;
+    double alpha, beta;
+    const double* in;
+    int ldin;
+    double* out;
+    int ldout;
+    int k;
+};
+
+// The structural part of a batch of jobs (which H-matrix subtree, op, width)
+// and the per-call part (pointers, scalars).
+struct JobSpec {
+    const HMatrix* H;
+    int root;
+    bool trans;
+    int k;
+};
+struct JobArgs {
+    const double* in;
+    double* out;
+    double alpha, beta;
+    int ldin, ldout, k, pad;
+};
+
+// Work lists of a batch of jobs, resident on the device: build once, execute
+// many times with different pointers (the plan references the H-matrices'
+// storage, so it is invalid once they are re-laid out).
+struct MatPlan;
+struct MatPlanDeleter { void operator()(MatPlan* p) const; };
+using PlanPtr = std::unique_ptr<MatPlan, MatPlanDeleter>;
+PlanPtr build_plan(Context& ctx, const std::vector<JobSpec>& jobs);
+void execute_plan(Context& ctx, MatPlan& plan, const std::vector<JobArgs>& args);
+
+// Runs a batch of jobs as two level-batched launches (low-rank inner products,
+// then one fused output pass per row tile).  Outputs of different jobs must
+// not overlap; inputs may alias each other but not outputs.
+void run_jobs(Context& ctx, const std::vector<MatJob>& jobs);
+
+// Device kernels driven from the host side (launchers).
+void launch_fill_random(Context& ctx, HMatrix& H);
+
+}  // namespace hmb

@@ -1,0 +1,136 @@
+// Device storage of an H-matrix: layout, sparse import, random fill.
+//
+// Storage: one arena per H-matrix.  Low-rank block b keeps U (m x r) then V
+// (n x r), column-major with leading dimensions m and n (A_b = U V^T,
+// include/dmhm/core/low_rank.hpp:22-38); dense leaves keep D (m x n).  Blocks
+// are laid out in depth-first order so that a subtree's data is contiguous.
+#include <algorithm>
+
+#include "engine.h"
+#include "rng.cuh"
+
+namespace hmb {
+
+void HMatrix::layout() {
+    const Structure& St = *S;
+    plans.clear();
+    off.assign(St.blocks.size(), -1);
+    long long cur = 0;
+    for (int b : St.leaves) {
+        const Block& B = St.blocks[b];
+        off[b] = cur;
+        if (B.kind == KIND_DENSE)
+            cur += (long long)B.m * B.n;
+        else
+            cur += (long long)(B.m + B.n) * rank[b];
+        cur = (cur + 1) & ~1LL;   // 16-byte alignment of every block
+    }
+    total = cur;
+    data.allocate((size_t)std::max<long long>(total, 2), ctx->stream);
+    upload_table();
+}
+
+void HMatrix::upload_table() {
+    const Structure& St = *S;
+    std::vector<DevBlock> t(St.blocks.size());
+    for (size_t b = 0; b < St.blocks.size(); ++b) {
+        const Block& B = St.blocks[b];
+        DevBlock d{};
+        d.kind = B.kind;
+        d.m = B.m;
+        d.n = B.n;
+        d.rank = B.kind == KIND_LOWRANK ? rank[b] : 0;
+        d.row_off = B.row_off;
+        d.col_off = B.col_off;
+        d.off = off[b];
+        t[b] = d;
+    }
+    table.upload(t, ctx->stream);
+}
+
+namespace {
+
+struct FillTask {
+    double* dst;
+    const double* old;         // previous buffer contents (may be null)
+    unsigned long long base;   // LCG state at the task's first draw
+    long long old_count;       // entries of `old` still in the buffer
+    int m, n;
+};
+
+// Gaussian fill; entries the reference's fill does not write keep the old
+// buffer value (Dense::Resize keeps its std::vector, new entries are zero).
+__global__ void fill_gaussian_kernel(const FillTask* __restrict__ tasks) {
+    const FillTask t = tasks[blockIdx.x];
+    const long long total = (long long)t.m * t.n;
+    const int pairs = (t.m + 1) / 2;
+    for (long long e = threadIdx.x; e < total; e += blockDim.x) {
+        int i = (int)(e % t.m), j = (int)(e / t.m);
+        bool written = (i < 2 * (pairs - 1)) || ((t.m & 1) ? i == t.n - 1
+                                                           : (i == t.n - 2 || i == t.n - 1));
+        double v;
+        if (written)
+            v = gaussian_fill_entry(t.base, t.m, t.n, i, j);
+        else
+            v = (t.old != nullptr && e < t.old_count) ? t.old[e] : 0.0;
+        t.dst[e] = v;
+    }
+}
+
+inline unsigned long long fill_draws(int m, int n) {
+    return (unsigned long long)n * 2ULL * (unsigned long long)((m + 1) / 2);
+}
+
+}  // namespace
+
+// SetToRandom (src/HMat2d/SetToRandom-incl.hpp:14-55): depth-first over the
+// leaves, dense m x n fills, low-rank U (m x maxRank) then V (n x maxRank),
+// all from the parallel stream.
+void launch_fill_random(Context& ctx, HMatrix& H) {
+    const Structure& St = *H.S;
+    for (int b : St.leaves) {
+        const Block& B = St.blocks[b];
+        if (B.kind == KIND_DENSE)
+            HMB_REQUIRE(B.n <= B.m || B.m == 0, HM_ERR_UNSUPPORTED,
+                        "random fill of a dense block wider than tall");
+        else
+            HMB_REQUIRE((H.max_rank <= B.m || B.m == 0) && (H.max_rank <= B.n || B.n == 0),
+                        HM_ERR_UNSUPPORTED, "random fill with max rank above the block size");
+    }
+    // keep the old storage alive until the fill has read it
+    DeviceBuffer<double> old_data(std::move(H.data));
+    std::vector<long long> old_off = H.off;
+    std::vector<int> old_rank = H.rank;
+    for (int b : St.leaves)
+        if (St.blocks[b].kind == KIND_LOWRANK) H.rank[b] = H.max_rank;
+    H.layout();
+    std::vector<FillTask> tasks;
+    uint64_t state = ctx.parallel_state;
+    const double* od = old_data.get();
+    for (int b : St.leaves) {
+        const Block& B = St.blocks[b];
+        if (B.kind == KIND_DENSE) {
+            tasks.push_back({H.D(b), od + old_off[b], state, (long long)B.m * B.n, B.m, B.n});
+            state = lcg_skip_host(state, fill_draws(B.m, B.n));
+        } else {
+            int r = H.max_rank, ro = old_rank[b];
+            tasks.push_back({H.U(b), od + old_off[b], state, (long long)B.m * ro, B.m, r});
+            state = lcg_skip_host(state, fill_draws(B.m, r));
+            tasks.push_back({H.V(b), od + old_off[b] + (long long)B.m * ro, state,
+                             (long long)B.n * ro, B.n, r});
+            state = lcg_skip_host(state, fill_draws(B.n, r));
+        }
+    }
+    ctx.parallel_state = state;
+    tasks.erase(std::remove_if(tasks.begin(), tasks.end(),
+                               [](const FillTask& t) { return t.m == 0 || t.n == 0; }),
+                tasks.end());
+    if (tasks.empty()) return;
+    DeviceBuffer<FillTask> d;
+    d.upload(tasks, ctx.stream);
+    LaunchScope ls(ctx, "fill_gaussian");
+    fill_gaussian_kernel<<<(unsigned)tasks.size(), 256, 0, ctx.stream>>>(d.get());
+    HMB_CHECK_LAUNCH();
+}
+
+}  // namespace hmb

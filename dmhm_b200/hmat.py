@@ -1,0 +1,315 @@
+"""Python mirror of the reference's serial H-matrix API over the C ABI.
+
+Names, argument meaning and error behaviour follow YingzhouLi/dmhm's
+``HMat2d<double>`` / ``HMat3d<double>`` (include/dmhm/hmat2d.hpp:22-393,
+include/dmhm/hmat3d.hpp) and the globals of src/core/global.cpp, so code
+written against the reference reads the same:
+
+    Initialize(); SetOversample(4)
+    H = HMat2d(S, numLevels, maxRank, stronglyAdmissible, xSize, ySize)
+    y = H.Multiply(1.0, x)            # vector or dense (numpy or CUDA tensor)
+    C = H.Multiply(1.0, B_hmat)       # H*H with randomized compression
+    H.SchulzInvert(-1)
+
+Every numeric operation runs in the sm_100a kernels of ``libdmhm_b200.so``;
+nothing here computes.  Vectors are in hierarchical ordering.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib
+
+LCG_SEED = (21 << 32) | 17
+
+
+@dataclass
+class Sparse:
+    """CSR matrix (include/dmhm/core/sparse.hpp:16-28), hierarchical order."""
+    height: int
+    width: int
+    rowOffsets: np.ndarray
+    columnIndices: np.ndarray
+    nonzeros: np.ndarray
+    symmetric: bool = False
+
+
+class Context:
+    """Device, CUDA stream, generators and Oversample() of one engine instance."""
+
+    def __init__(self, device: int = 0, stream: Optional[int] = None):
+        h = C.c_void_p()
+        check(lib().hm_context_create(int(device), C.c_void_p(stream or 0), C.byref(h)))
+        self._h = h
+        self.device = device
+
+    @property
+    def handle(self):
+        return self._h
+
+    def synchronize(self):
+        check(lib().hm_context_synchronize(self._h))
+
+    def set_oversample(self, p: int):
+        check(lib().hm_set_oversample(self._h, int(p)))
+
+    def oversample(self) -> int:
+        v = C.c_int()
+        check(lib().hm_get_oversample(self._h, C.byref(v)))
+        return v.value
+
+    def lcg_states(self):
+        s, p = C.c_uint64(), C.c_uint64()
+        check(lib().hm_get_lcg_states(self._h, C.byref(s), C.byref(p)))
+        return s.value, p.value
+
+    def set_lcg_states(self, serial: int, parallel: int):
+        check(lib().hm_set_lcg_states(self._h, C.c_uint64(serial), C.c_uint64(parallel)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().hm_context_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx: Optional[Context] = None
+
+
+def Initialize(device: int = 0) -> Context:
+    """Initialize (src/core/global.cpp:43-94): a context whose serial and
+    parallel generators start at the reference seed {17, 21}."""
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(device)
+    return _default_ctx
+
+
+def Finalize():
+    global _default_ctx
+    if _default_ctx is not None:
+        _default_ctx.close()
+        _default_ctx = None
+
+
+def _ctx(ctx: Optional[Context]) -> Context:
+    return ctx if ctx is not None else Initialize()
+
+
+def SetOversample(p: int, ctx: Optional[Context] = None):
+    """SetOversample (global.cpp:155-159)."""
+    _ctx(ctx).set_oversample(p)
+
+
+def Oversample(ctx: Optional[Context] = None) -> int:
+    """Oversample (global.cpp:152-153)."""
+    return _ctx(ctx).oversample()
+
+
+def _as_i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def natural_to_hierarchical_map(sizes: Sequence[int], num_levels: int) -> np.ndarray:
+    """BuildNaturalToHierarchicalMap (src/HMat2d/HMat2d.cpp:69-87,
+    src/HMat3d/HMat3d.cpp:91-110), computed by the library."""
+    sz = _as_i32(list(sizes))
+    out = np.empty(int(np.prod(sizes)), dtype=np.int32)
+    check(lib().hm_natural_to_hierarchical_map(
+        len(sizes), sz.ctypes.data_as(_lib._PI), int(num_levels), out.ctypes.data_as(_lib._PI)))
+    return out
+
+
+def _is_cuda_tensor(x) -> bool:
+    return hasattr(x, "is_cuda") and bool(getattr(x, "is_cuda"))
+
+
+class _HMatBase:
+    """Common part of HMat2d / HMat3d: a handle to one device-resident H-matrix."""
+    dim = 2
+
+    def __init__(self, S: Optional[Sparse] = None, numLevels: int = 1, maxRank: int = 0,
+                 stronglyAdmissible: bool = True, *sizes, ctx: Optional[Context] = None,
+                 _handle=None):
+        self.ctx = _ctx(ctx)
+        self._h = None
+        if _handle is not None:
+            self._h = _handle
+            return
+        if S is None:
+            raise ValueError("an H-matrix is constructed from a Sparse matrix")
+        if len(sizes) != self.dim:
+            raise ValueError(f"expected {self.dim} grid sizes")
+        if S.symmetric:
+            raise _lib.HMError(4, "symmetric sparse storage builds NODE_SYMMETRIC blocks, "
+                                  "which the H*H product and inversion do not support")
+        N = int(np.prod(sizes))
+        if S.height != N or S.width != N:
+            raise _lib.HMError(1, "sparse matrix does not match the grid")
+        rows = np.ascontiguousarray(S.rowOffsets, dtype=np.int64)
+        cols = np.ascontiguousarray(S.columnIndices, dtype=np.int32)
+        vals = np.ascontiguousarray(S.nonzeros, dtype=np.float64)
+        sz = _as_i32(list(sizes))
+        h = C.c_void_p()
+        check(lib().hm_create_from_csr(
+            self.ctx.handle, self.dim, sz.ctypes.data_as(_lib._PI), int(numLevels),
+            int(maxRank), int(bool(stronglyAdmissible)), rows.ctypes.data_as(_lib._PI64),
+            cols.ctypes.data_as(_lib._PI32), vals.ctypes.data_as(_lib._PD), C.byref(h)))
+        self._h = h
+
+    # -- lifetime -------------------------------------------------------------
+    def __del__(self):
+        try:
+            if self._h:
+                lib().hm_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    # -- AbstractHMat fulfilment (include/dmhm/core/abstract_hmat.hpp:20-40) ---
+    def _info(self):
+        h, w, L, r = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        counts = (C.c_int64 * 4)()
+        nbytes = C.c_int64()
+        check(lib().hm_info(self._h, C.byref(h), C.byref(w), C.byref(L), C.byref(r),
+                            counts, C.byref(nbytes)))
+        return h.value, w.value, L.value, r.value, list(counts), nbytes.value
+
+    def Height(self) -> int:
+        return self._info()[0]
+
+    def Width(self) -> int:
+        return self._info()[1]
+
+    def NumLevels(self) -> int:
+        return self._info()[2]
+
+    def MaxRank(self) -> int:
+        return self._info()[3]
+
+    def Symmetric(self) -> bool:
+        return False
+
+    def BlockCensus(self) -> dict:
+        _, _, _, _, c, nbytes = self._info()
+        return {"node": c[0], "low_rank": c[1], "dense": c[2], "rank_sum": c[3],
+                "bytes": nbytes}
+
+    def SampleRank(self, approxRank: int) -> int:
+        """SampleRank (hmat2d.hpp:32-33)."""
+        return approxRank + self.ctx.oversample()
+
+    def SetToRandom(self):
+        """SetToRandom (src/HMat2d/SetToRandom-incl.hpp:14-55)."""
+        check(lib().hm_set_to_random(self._h))
+
+    # -- H * dense ------------------------------------------------------------
+    def _apply(self, transpose: int, alpha: float, B, beta: float, Cout):
+        n = self.Height() if transpose else self.Width()
+        m = self.Width() if transpose else self.Height()
+        if _is_cuda_tensor(B):
+            import torch
+            vec = B.dim() == 1
+            B2 = B.reshape(-1, 1) if vec else B
+            if B2.dtype != torch.float64:
+                raise _lib.HMError(1, "dense operands must be float64")
+            # column-major view: a (n x k) column-major matrix is a k x n row-major tensor
+            Bt = B2.t().contiguous() if not B2.t().is_contiguous() else B2.t()
+            k = B2.shape[1]
+            if B2.shape[0] != n:
+                raise _lib.HMError(1, "nonconformal multiply")
+            if Cout is None:
+                Ct = torch.zeros((k, m), dtype=torch.float64, device=B.device)
+            else:
+                C2 = Cout.reshape(-1, 1) if Cout.dim() == 1 else Cout
+                Ct = C2.t().contiguous()
+            check(lib().hm_multiply_dense(self._h, transpose, float(alpha), C.c_void_p(Bt.data_ptr()),
+                                          n, float(beta), C.c_void_p(Ct.data_ptr()), m, k))
+            Cres = Ct.t()
+            if Cout is not None:
+                (Cout.reshape(-1, 1) if Cout.dim() == 1 else Cout).copy_(Cres)
+                return Cout
+            return Cres.reshape(-1) if vec else Cres
+        Bn = np.asarray(B, dtype=np.float64)
+        vec = Bn.ndim == 1
+        B2 = np.asfortranarray(Bn.reshape(-1, 1) if vec else Bn)
+        if B2.shape[0] != n:
+            raise _lib.HMError(1, "nonconformal multiply")
+        k = B2.shape[1]
+        if Cout is None:
+            C2 = np.zeros((m, k), order="F")
+        else:
+            C2 = np.asfortranarray(np.asarray(Cout, dtype=np.float64).reshape(m, k))
+        check(lib().hm_multiply_dense_host(self._h, transpose, float(alpha),
+                                           B2.ctypes.data_as(_lib._PD), n, float(beta),
+                                           C2.ctypes.data_as(_lib._PD), m, k))
+        return C2[:, 0].copy() if vec else C2
+
+    def Multiply(self, alpha, B, beta=None, C=None):
+        """Multiply (hmat2d.hpp:150-268).
+
+        * ``Multiply(alpha, x)`` / ``Multiply(alpha, B)``: y = alpha H x for a
+          vector or dense matrix (numpy array or CUDA float64 tensor);
+        * ``Multiply(alpha, x, beta, y)``: y := alpha H x + beta y;
+        * ``Multiply(alpha, B_hmat)`` / ``Multiply(alpha, B_hmat, beta, C)``:
+          the H*H product with randomized compression.
+        """
+        if isinstance(B, _HMatBase):
+            return self._multiply_hmat(alpha, B, beta, C)
+        return self._apply(0, alpha, B, 0.0 if beta is None else beta, C)
+
+    def TransposeMultiply(self, alpha, B, beta=None, C=None):
+        """TransposeMultiply (hmat2d.hpp:162-206): C := alpha H^T B (+ beta C)."""
+        return self._apply(1, alpha, B, 0.0 if beta is None else beta, C)
+
+    def AdjointMultiply(self, alpha, B, beta=None, C=None):
+        """AdjointMultiply: equal to TransposeMultiply for real scalars."""
+        return self.TransposeMultiply(alpha, B, beta, C)
+
+    def _multiply_hmat(self, alpha, B, beta, C):
+        raise _lib.HMError(4, "H*H multiply not available in this build")
+
+
+class HMat2d(_HMatBase):
+    """HMat2d<double> (include/dmhm/hmat2d.hpp:22-393)."""
+    dim = 2
+
+    def __init__(self, S: Optional[Sparse] = None, numLevels: int = 1, maxRank: int = 0,
+                 stronglyAdmissible: bool = True, xSize: int = 0, ySize: int = 0,
+                 ctx: Optional[Context] = None, _handle=None):
+        super().__init__(S, numLevels, maxRank, stronglyAdmissible, xSize, ySize,
+                         ctx=ctx, _handle=_handle)
+
+    @staticmethod
+    def BuildNaturalToHierarchicalMap(xSize: int, ySize: int, numLevels: int) -> np.ndarray:
+        return natural_to_hierarchical_map((xSize, ySize), numLevels)
+
+
+class HMat3d(_HMatBase):
+    """HMat3d<double> (include/dmhm/hmat3d.hpp)."""
+    dim = 3
+
+    def __init__(self, S: Optional[Sparse] = None, numLevels: int = 1, maxRank: int = 0,
+                 stronglyAdmissible: bool = True, xSize: int = 0, ySize: int = 0,
+                 zSize: int = 0, ctx: Optional[Context] = None, _handle=None):
+        super().__init__(S, numLevels, maxRank, stronglyAdmissible, xSize, ySize, zSize,
+                         ctx=ctx, _handle=_handle)
+
+    @staticmethod
+    def BuildNaturalToHierarchicalMap(xSize: int, ySize: int, zSize: int,
+                                      numLevels: int) -> np.ndarray:
+        return natural_to_hierarchical_map((xSize, ySize, zSize), numLevels)

@@ -1,0 +1,124 @@
+/*
+ * dmhm_b200 — C ABI of the B200 (sm_100a) H-matrix engine.
+ *
+ * Plain pointers, sizes and opaque handles only.  Each entry point replaces
+ * one operation of the reference C++ API of YingzhouLi/dmhm (cited per entry
+ * as file:line inside that project).  All matrices are real double precision,
+ * column-major; all vectors are in the H-matrix's hierarchical ordering
+ * (the ordering BuildNaturalToHierarchicalMap produces).
+ *
+ * Every function returns an HM_* status (0 = success).  On failure,
+ * hm_last_error() returns a message for the calling thread.  Work is issued on
+ * the context's CUDA stream; functions taking host pointers (the *_host
+ * variants) synchronize that stream before returning.
+ */
+#ifndef DMHM_B200_H
+#define DMHM_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#if defined(__GNUC__)
+#define HM_API __attribute__((visibility("default")))
+#else
+#define HM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define HM_OK 0
+#define HM_ERR_ARGUMENT 1      /* bad argument / nonconformal shapes          */
+#define HM_ERR_OOM 2           /* device allocation failed                    */
+#define HM_ERR_CUDA 3          /* CUDA runtime error                          */
+#define HM_ERR_UNSUPPORTED 4   /* combination the reference also rejects      */
+#define HM_ERR_NUMERICAL 5     /* non-finite values met (NaN / Inf)           */
+#define HM_ERR_TIMEOUT 6       /* a bounded device wait ran out               */
+#define HM_ERR_INTERNAL 7
+
+typedef struct hm_context_s* hm_context;  /* device, stream, generators     */
+typedef struct hm_matrix_s* hm_matrix;    /* one H-matrix resident in HBM    */
+
+/* Message of the last failed call on this thread ("" if none). */
+HM_API const char* hm_last_error(void);
+
+/* Library version: major*10000 + minor*100 + patch. */
+HM_API int hm_version(void);
+
+/*
+ * Context: device, stream, the two global generators and Oversample().
+ * Replaces Initialize (src/core/global.cpp:43-94): both generators start at
+ * the reference seed {17, 21} (global.cpp:88-93); oversample starts at 4
+ * (global.cpp:30).  stream == NULL creates a private non-blocking stream.
+ */
+HM_API int hm_context_create(int device, void* cuda_stream, hm_context* out);
+HM_API int hm_context_destroy(hm_context ctx);
+HM_API int hm_context_synchronize(hm_context ctx);
+/* SetOversample / Oversample (src/core/global.cpp:155-159). */
+HM_API int hm_set_oversample(hm_context ctx, int oversample);
+HM_API int hm_get_oversample(hm_context ctx, int* oversample);
+/* SeedSerialLcg (src/core/random.cpp:67-68) and the single-rank
+   SeedParallelLcg (random.cpp:70-101); state is the next value drawn. */
+HM_API int hm_set_lcg_states(hm_context ctx, uint64_t serial, uint64_t parallel);
+HM_API int hm_get_lcg_states(hm_context ctx, uint64_t* serial, uint64_t* parallel);
+
+/*
+ * BuildNaturalToHierarchicalMap (src/HMat2d/HMat2d.cpp:69-87,
+ * src/HMat3d/HMat3d.cpp:91-110): map[natural] = hierarchical index.
+ * dim = 2 or 3; sizes[dim]; map has prod(sizes) entries.
+ */
+HM_API int hm_natural_to_hierarchical_map(int dim, const int* sizes, int num_levels,
+                                   int* map);
+
+/*
+ * HMat2d(const Sparse&, numLevels, maxRank, strong, xSize, ySize)
+ * (include/dmhm/hmat2d.hpp:55-58; ImportSparse src/HMat2d/HMat2d.cpp:961-1033)
+ * and the HMat3d equivalent (include/dmhm/hmat3d.hpp).  The CSR matrix is in
+ * hierarchical ordering, height = width = prod(sizes), non-symmetric storage.
+ */
+HM_API int hm_create_from_csr(hm_context ctx, int dim, const int* sizes,
+                       int num_levels, int max_rank, int strongly_admissible,
+                       const int64_t* row_offsets, const int32_t* col_indices,
+                       const double* values, hm_matrix* out);
+HM_API int hm_destroy(hm_matrix h);
+
+/* Height, width, number of levels, max rank, and the block census:
+   counts[0..2] = node / low-rank / dense blocks, counts[3] = sum of low-rank
+   ranks, bytes = device bytes of the block data. */
+HM_API int hm_info(hm_matrix h, int* height, int* width, int* num_levels,
+            int* max_rank, int64_t* counts, int64_t* bytes);
+
+/* SetToRandom (src/HMat2d/SetToRandom-incl.hpp:14-55): dense leaves and
+   rank-maxRank U, V drawn from the context's parallel generator. */
+HM_API int hm_set_to_random(hm_matrix h);
+
+/*
+ * C := alpha op(H) B + beta C, op = identity (transpose = 0) or transpose (1).
+ * HMat2d::Multiply / TransposeMultiply against Dense and Vector
+ * (src/HMat2d/MultiplyDense-incl.hpp:12-150, MultiplyVector-incl.hpp:12-124).
+ * B: n x nrhs (ld ldb), C: m x nrhs (ld ldc), DEVICE pointers, stream-ordered.
+ */
+HM_API int hm_multiply_dense(hm_matrix h, int transpose, double alpha,
+                      const double* B, int ldb, double beta, double* C,
+                      int ldc, int nrhs);
+/* Same with HOST pointers: copies in, multiplies, copies out, synchronizes. */
+HM_API int hm_multiply_dense_host(hm_matrix h, int transpose, double alpha,
+                           const double* B, int ldb, double beta, double* C,
+                           int ldc, int nrhs);
+
+/* Diagnostics (no reference counterpart): number of kernels this library has
+   launched so far in the process, and per-kernel CUDA-event timing on the
+   context stream.  hm_profile_enable resets the totals; hm_profile_read
+   synchronizes and returns kernel `index` (HM_ERR_ARGUMENT past the end). */
+HM_API unsigned long long hm_kernel_launches(void);
+HM_API int hm_profile_enable(hm_context ctx, int on);
+HM_API int hm_profile_read(hm_context ctx, int index, char* name, int name_cap,
+                           double* ms, int64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DMHM_B200_H */

@@ -127,15 +127,21 @@ class Lcg:
             x[n - 1] = Y[pairs - 1]
         return x
 
-    def gaussian_vectors(self, m: int, n: int) -> np.ndarray:
+    def gaussian_vectors(self, m: int, n: int, prev=None) -> np.ndarray:
         """SerialGaussianRandomVectors(Dense<Real>) (random.hpp:418-445).
 
         Quirk kept: the tail of each column is written at rows n-2, n-1 (the
-        WIDTH) rather than m-2, m-1, so rows m-2, m-1 stay zero.  Writes past
-        the column (n > m) would spill into the next column; that case is
-        rejected.
+        WIDTH) rather than m-2, m-1, so rows m-2, m-1 are not written and keep
+        what the buffer held: ``prev`` is the old column-major buffer contents
+        (Dense::Resize keeps the std::vector, dense.hpp:254-282; new entries
+        are zero).  Writes past the column (n > m) would spill into the next
+        column; that case is rejected.
         """
-        A = np.zeros((m, n), order="F")
+        flat = np.zeros(m * n)
+        if prev is not None:
+            pv = np.asarray(prev, dtype=np.float64).ravel(order="F")[:m * n]
+            flat[:pv.size] = pv
+        A = flat.reshape((m, n), order="F")
         if m == 0 or n == 0:
             return A
         if n > m:
@@ -409,15 +415,16 @@ def import_sparse(H: HMat, rows, cols, vals) -> HMat:
 
 def set_to_random(H: HMat, rng: Rng):
     """SetToRandom (src/HMat2d/SetToRandom-incl.hpp:14-55): parallel stream,
-    dense leaves filled whole, low-rank blocks at rank max_rank (U then V)."""
+    dense leaves refilled in place, low-rank blocks resized to rank max_rank
+    (U then V); entries the fill skips keep the old buffer contents."""
     if H.kind == NODE:
         for c in H.children:
             set_to_random(c, rng)
     elif H.kind == DENSE:
-        H.D = rng.parallel.gaussian_vectors(H.height, H.width)
+        H.D = rng.parallel.gaussian_vectors(H.height, H.width, prev=H.D)
     else:
-        H.U = rng.parallel.gaussian_vectors(H.height, H.max_rank)
-        H.V = rng.parallel.gaussian_vectors(H.width, H.max_rank)
+        H.U = rng.parallel.gaussian_vectors(H.height, H.max_rank, prev=H.U)
+        H.V = rng.parallel.gaussian_vectors(H.width, H.max_rank, prev=H.V)
 
 
 # ---------------------------------------------------------------------------

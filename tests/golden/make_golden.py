@@ -1,0 +1,130 @@
+"""Generates the golden fixtures in this folder from the reference itself.
+
+Runs the unmodified reference library (compiled by ``oracle/Makefile`` into
+``oracle/_ref/dmhm_ref_driver``) on small seeded cases and stores inputs and
+outputs as ``<case>.npz``.  Only this script and the oracle pinning tests
+touch the reference; the fixtures let the GPU tests check parity without it.
+
+    python tests/golden/make_golden.py            # all cases
+    python tests/golden/make_golden.py c1 ragged  # some cases
+"""
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+DRIVER = os.path.join(ROOT, "oracle", "_ref", "dmhm_ref_driver")
+
+# name: grid, levels, rank, oversample, strong, coefficient seed, probes
+CASES = {
+    "c1": dict(sizes=(32, 32), levels=4, rank=8, oversample=4, strong=1, seed=1, probes=4,
+               ops=["matvec", "random", "hh_AA", "hh_AB", "schulz3", "schulz_stop"]),
+    "ragged": dict(sizes=(24, 20), levels=3, rank=6, oversample=4, strong=1, seed=5, probes=3,
+                   ops=["matvec", "random", "hh_AA", "hh_AB", "schulz3"]),
+    "weak": dict(sizes=(16, 16), levels=3, rank=4, oversample=4, strong=0, seed=7, probes=3,
+                 ops=["matvec", "random", "hh_AA", "schulz3"]),
+    "c3d": dict(sizes=(16, 16, 16), levels=3, rank=8, oversample=8, strong=1, seed=9, probes=2,
+                ops=["matvec", "random", "hh_AA", "schulz2"]),
+}
+
+
+def run(args, out_prefix):
+    r = subprocess.run([DRIVER] + [str(a) for a in args] + ["--out", out_prefix],
+                       capture_output=True, text=True, env={**os.environ, "OPENBLAS_NUM_THREADS": "1"})
+    if r.returncode != 0:
+        raise RuntimeError(f"reference driver failed: {args}\n{r.stderr}")
+    info = json.loads(r.stdout.strip().splitlines()[-1])
+    return info, np.fromfile(out_prefix + ".bin")
+
+
+def make_case(name, spec, tmp):
+    sizes = spec["sizes"]
+    dim = len(sizes)
+    N = int(np.prod(sizes))
+    rng = np.random.default_rng(spec["seed"])
+    coef = 1.0 + rng.random(N)
+    coefB = 1.0 + rng.random(N)
+    P = rng.standard_normal((N, spec["probes"]))
+    cpath, cbpath, ppath = (os.path.join(tmp, f) for f in ("c.bin", "cb.bin", "p.bin"))
+    coef.tofile(cpath)
+    coefB.tofile(cbpath)
+    np.asfortranarray(P).T.copy().tofile(ppath)     # column-major
+    base = ["--dim", dim, "--nx", sizes[0], "--ny", sizes[1],
+            "--nz", sizes[2] if dim == 3 else 1, "--levels", spec["levels"],
+            "--rank", spec["rank"], "--oversample", spec["oversample"],
+            "--strong", spec["strong"], "--coef", cpath]
+    k = spec["probes"]
+    out = dict(sizes=np.array(sizes), levels=spec["levels"], rank=spec["rank"],
+               oversample=spec["oversample"], strong=spec["strong"], coef=coef, coefB=coefB,
+               probes=P)
+    o = os.path.join(tmp, "o")
+
+    def mat(v):
+        return v.reshape(k, N).T.copy()
+
+    for op in spec["ops"]:
+        if op == "matvec":
+            _, y = run(["matvec"] + base + ["--x", ppath, "--nrhs", k], o)
+            out["matvec"] = mat(y)
+            _, y1 = run(["matvec"] + base + ["--x", ppath, "--nrhs", 1], o)
+            out["matvec1"] = y1
+            _, yt = run(["transpose"] + base + ["--x", ppath, "--nrhs", k], o)
+            out["matvec_T"] = mat(yt)
+        elif op == "random":
+            _, y = run(["matvec"] + base + ["--x", ppath, "--nrhs", k, "--random", 1], o)
+            out["random"] = mat(y)
+            _, yt = run(["transpose"] + base + ["--x", ppath, "--nrhs", k, "--random", 1], o)
+            out["random_T"] = mat(yt)
+        elif op == "hh_AA":
+            _, y = run(["hh"] + base + ["--x", ppath, "--nrhs", k], o)
+            out["hh_AA"] = mat(y)
+        elif op == "hh_AB":
+            _, y = run(["hh"] + base + ["--x", ppath, "--nrhs", k, "--useB", 1,
+                                        "--coefB", cbpath, "--alpha", -0.5], o)
+            out["hh_AB"] = mat(y)
+        elif op in ("schulz2", "schulz3"):
+            its = int(op[-1])
+            info, y = run(["schulz_trace"] + base + ["--x", ppath, "--nrhs", k, "--iters", its], o)
+            out[op] = mat(y)
+            out[op + "_trace"] = np.fromfile(o + ".trace.bin")
+            out[op + "_seconds"] = info["seconds"]
+        elif op == "schulz_stop":
+            info, y = run(["schulz_trace"] + base + ["--x", ppath, "--nrhs", k, "--iters", -1,
+                                                     "--stopTol", 1e-4], o)
+            out["schulz_stop"] = mat(y)
+            out["schulz_stop_trace"] = np.fromfile(o + ".trace.bin")
+            out["schulz_stop_iterations"] = info["iterations"]
+            out["schulz_stop_seconds"] = info["seconds"]
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name, "ok", sorted(out))
+
+
+def make_lcg(tmp):
+    o = os.path.join(tmp, "lcg")
+    run(["lcg", "--count", 9], o)
+    d = np.fromfile(o + ".bin")
+    np.savez_compressed(os.path.join(HERE, "lcg.npz"), count=9, draws=d)
+    print("lcg ok")
+
+
+def main(argv):
+    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-j8"], check=True,
+                   capture_output=True)
+    names = argv or list(CASES) + ["lcg"]
+    with tempfile.TemporaryDirectory() as tmp:
+        for n in names:
+            if n == "lcg":
+                make_lcg(tmp)
+            else:
+                make_case(n, CASES[n], tmp)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:])

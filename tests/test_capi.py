@@ -1,0 +1,57 @@
+"""C ABI: the library loads and exports every entry point the header declares
+(no GPU needed; only functions that do no device work are called)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+
+import dmhm_b200 as D
+from dmhm_b200 import _lib
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                      "include", "dmhm_b200.h")
+
+
+def declared():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"HM_API\s+[\w\s\*]+?\b(hm_\w+)\s*\(", text)))
+
+
+def test_every_declared_symbol_is_exported():
+    names = declared()
+    assert len(names) >= 10
+    L = ctypes.CDLL(_lib.LIB_PATH)
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_binding_covers_header():
+    assert set(declared()) == set(_lib.SIGNATURES)
+
+
+def test_map_matches_oracle():
+    from oracle import dmhm_oracle as O
+    for sizes, L in [((32, 32), 4), ((24, 20), 3), ((16, 16, 16), 3), ((6, 10, 4), 2),
+                     ((1, 7), 2), ((48, 48), 5)]:
+        a = D.natural_to_hierarchical_map(sizes, L)
+        b = O.natural_to_hierarchical_map(sizes, L)
+        assert (a == b).all(), sizes
+
+
+def test_errors_are_reported():
+    sizes = (ctypes.c_int * 2)(4, 4)
+    out = (ctypes.c_int * 16)()
+    st = _lib.lib().hm_natural_to_hierarchical_map(5, sizes, 2, out)
+    assert st == 1
+    assert b"dim" in _lib.lib().hm_last_error()
+
+
+def test_stencil_operator_matches_oracle():
+    from oracle import dmhm_oracle as O
+    for sizes, L in [((32, 32), 4), ((8, 6, 4), 2)]:
+        c = D.operators.uniform_coefficients(sizes, 3)
+        S = D.operators.stencil(sizes, c, L)
+        r, cc, v, _ = O.stencil_csr(sizes, c, L)
+        assert (S.rowOffsets == r).all() and (S.columnIndices == cc).all()
+        assert np.array_equal(S.nonzeros, v)

@@ -1,0 +1,86 @@
+"""Pins the numpy oracle (oracle/dmhm_oracle.py) to the reference itself.
+
+The fixtures in tests/golden/ hold outputs of the unmodified reference library
+(tests/golden/make_golden.py).  Integer work (generator states and uniforms)
+must match bit for bit; floating-point results to rounding (matvec, exact H*H)
+or, where fixed-rank truncation amplifies rounding, to the stated tolerance.
+"""
+import numpy as np
+import pytest
+
+from helpers import load, relerr
+from oracle import dmhm_oracle as O
+
+
+def oracle_hmat(fx, coef_key="coef"):
+    sizes = tuple(int(s) for s in fx["sizes"])
+    return O.build_stencil_hmat(len(sizes), sizes, int(fx["levels"]), int(fx["rank"]),
+                                fx[coef_key], strong=bool(fx["strong"]))
+
+
+def test_lcg_bit_exact():
+    fx = load("lcg")
+    k = int(fx["count"])
+    d = fx["draws"]
+    r = O.Rng()
+    assert np.array_equal(r.serial.uniforms(k), d[:k])
+    assert np.array_equal(r.serial.gaussian_vector(k), d[k:2 * k])
+    assert np.array_equal(r.serial.gaussian_vectors(k, 3).T.ravel(), d[2 * k:5 * k])
+    assert np.array_equal(r.parallel.gaussian_vectors(k, 3).T.ravel(), d[5 * k:8 * k])
+
+
+def test_lcg_skip_ahead():
+    a = O.Lcg()
+    s = a.states(5000)
+    b = O.Lcg()
+    b.state = (O.lcg_jump(4321)[0] * O.LCG_SEED + O.lcg_jump(4321)[1]) & O.MASK64
+    assert int(s[4321]) == b.state
+
+
+@pytest.mark.parametrize("case", ["c1", "ragged", "weak", "c3d"])
+def test_matvec(case):
+    fx = load(case)
+    H = oracle_hmat(fx)
+    P = fx["probes"]
+    assert relerr(O.multiply_dense(H, 1.0, P), fx["matvec"]) < 1e-14
+    assert relerr(O.multiply_dense(H, 1.0, P[:, 0]), fx["matvec1"]) < 1e-14
+    assert relerr(O.transpose_multiply_dense(H, 1.0, P), fx["matvec_T"]) < 1e-14
+
+
+@pytest.mark.parametrize("case", ["c1", "ragged", "weak", "c3d"])
+def test_random_matvec(case):
+    fx = load(case)
+    H = oracle_hmat(fx)
+    O.set_to_random(H, O.Rng())
+    P = fx["probes"]
+    assert relerr(O.multiply_dense(H, 1.0, P), fx["random"]) < 1e-13
+    assert relerr(O.transpose_multiply_dense(H, 1.0, P), fx["random_T"]) < 1e-13
+
+
+@pytest.mark.parametrize("case", ["c1", "ragged", "weak"])
+def test_hh_square(case):
+    fx = load(case)
+    A = oracle_hmat(fx)
+    C = O.hh_multiply(A, 1.0, A, O.Rng(int(fx["oversample"])))
+    assert relerr(O.multiply_dense(C, 1.0, fx["probes"]), fx["hh_AA"]) < 1e-12
+
+
+@pytest.mark.parametrize("case", ["c1", "ragged"])
+def test_hh_general(case):
+    fx = load(case)
+    A = oracle_hmat(fx)
+    B = oracle_hmat(fx, "coefB")
+    C = O.hh_multiply(A, -0.5, B, O.Rng(int(fx["oversample"])))
+    assert relerr(O.multiply_dense(C, 1.0, fx["probes"]), fx["hh_AB"]) < 1e-12
+
+
+@pytest.mark.parametrize("case,its", [("ragged", 3), ("weak", 3)])
+def test_schulz_iterations(case, its):
+    fx = load(case)
+    A = oracle_hmat(fx)
+    X, k, trace = O.schulz_invert(A, its, O.Rng(int(fx["oversample"])))
+    key = f"schulz{its}"
+    assert k == its
+    assert abs(trace[0] - fx[key + "_trace"][0]) < 1e-13 * trace[0]
+    # fixed-rank truncation inside each H*H amplifies rounding differences
+    assert relerr(O.multiply_dense(X, 1.0, fx["probes"]), fx[key]) < 1e-8

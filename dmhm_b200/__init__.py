@@ -8,10 +8,10 @@ runs in hand-written CUDA kernels behind the C ABI of
 Python mirror of the reference's C++ API.
 """
 from ._lib import HMError, LIB_PATH, lib
-from .hmat import (Context, Finalize, HMat2d, HMat3d, Initialize, Oversample,
-                   SetOversample, Sparse, natural_to_hierarchical_map)
+from .hmat import (Context, EstimateTwoNorm, Finalize, HMat2d, HMat3d, Initialize,
+                   Oversample, SetOversample, Sparse, natural_to_hierarchical_map)
 from . import operators
 
-__all__ = ["Context", "Finalize", "HMError", "HMat2d", "HMat3d", "Initialize",
+__all__ = ["Context", "EstimateTwoNorm", "Finalize", "HMError", "HMat2d", "HMat3d", "Initialize",
            "LIB_PATH", "Oversample", "SetOversample", "Sparse", "lib",
            "natural_to_hierarchical_map", "operators"]

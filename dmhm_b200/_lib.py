@@ -57,6 +57,14 @@ SIGNATURES = {
     "hm_set_to_random": [_P],
     "hm_multiply_dense": [_P, _I, _D, _P, _I, _D, _P, _I, _I],
     "hm_multiply_dense_host": [_P, _I, _D, _PD, _I, _D, _PD, _I, _I],
+    "hm_multiply_hmat": [_P, _D, _P, C.POINTER(_P)],
+    "hm_multiply_hmat_update": [_P, _D, _P, _D, _P],
+    "hm_estimate_two_norm": [_P, _D, _D, _PD],
+    "hm_schulz_invert": [_P, _I, _D, _D, _D, _PI, _PD, _I, _PI],
+    "hm_copy": [_P, C.POINTER(_P)],
+    "hm_transpose": [_P, C.POINTER(_P)],
+    "hm_scale": [_P, _D],
+    "hm_add_constant_to_diagonal": [_P, _D],
     "hm_kernel_launches": [],
     "hm_profile_enable": [_P, _I],
     "hm_profile_read": [_P, _I, C.c_char_p, _I, _PD, _PI64],

@@ -5,7 +5,9 @@
 #include <string>
 
 #include "engine.h"
+#include "hh.h"
 #include "rng.cuh"
+#include "schulz.h"
 
 struct hm_context_s {
     hmb::Context c;
@@ -320,6 +322,95 @@ int hm_multiply_dense_host(hm_matrix h, int transpose, double alpha, const doubl
         HMB_CUDA(cudaMemcpy2DAsync(C, ldc * sizeof(double), dC.get(), m * sizeof(double),
                                    m * sizeof(double), nrhs, cudaMemcpyDeviceToHost, ctx.stream));
         HMB_CUDA(cudaStreamSynchronize(ctx.stream));
+    });
+}
+
+int hm_multiply_hmat(hm_matrix A, double alpha, hm_matrix B, hm_matrix* C) {
+    return guarded([&] {
+        HMB_REQUIRE(A && B && C, HM_ERR_ARGUMENT, "NULL argument");
+        HMB_REQUIRE(A->h.ctx == B->h.ctx, HM_ERR_ARGUMENT, "factors live in different contexts");
+        bool created = false;
+        if (*C == nullptr) {
+            *C = new hm_matrix_s;
+            created = true;
+        }
+        try {
+            HMB_REQUIRE(*C != A && *C != B, HM_ERR_ARGUMENT,
+                        "the product must not overwrite a factor");
+            hh_multiply(*A->h.ctx, A->h, B->h, alpha, 0.0, (*C)->h, true);
+        } catch (...) {
+            if (created) {
+                delete *C;
+                *C = nullptr;
+            }
+            throw;
+        }
+    });
+}
+
+int hm_multiply_hmat_update(hm_matrix A, double alpha, hm_matrix B, double beta, hm_matrix C) {
+    return guarded([&] {
+        HMB_REQUIRE(A && B && C, HM_ERR_ARGUMENT, "NULL argument");
+        HMB_REQUIRE(C != A && C != B, HM_ERR_ARGUMENT, "the product must not overwrite a factor");
+        HMB_REQUIRE(C->h.S != nullptr, HM_ERR_ARGUMENT, "C is empty");
+        hh_multiply(*A->h.ctx, A->h, B->h, alpha, beta, C->h, false);
+    });
+}
+
+int hm_estimate_two_norm(hm_matrix h, double theta, double confidence, double* estimate) {
+    return guarded([&] {
+        HMB_REQUIRE(h && estimate, HM_ERR_ARGUMENT, "NULL argument");
+        *estimate = estimate_two_norm(*h->h.ctx, h->h, theta, confidence);
+    });
+}
+
+int hm_schulz_invert(hm_matrix h, int num_iterations, double theta, double confidence,
+                     double stop_tol, int* iterations, double* trace, int trace_cap,
+                     int* trace_len) {
+    return guarded([&] {
+        HMB_REQUIRE(h, HM_ERR_ARGUMENT, "h is NULL");
+        HMB_REQUIRE(h->h.height() == h->h.width(), HM_ERR_ARGUMENT,
+                    "Cannot invert non-square matrices");
+        HMB_REQUIRE(theta > 1.0, HM_ERR_ARGUMENT, "Theta must be > 1");
+        HMB_REQUIRE(confidence > 0.0, HM_ERR_ARGUMENT, "Confidence must be positive");
+        SchulzResult r = schulz_invert(*h->h.ctx, h->h, num_iterations, theta, confidence,
+                                       stop_tol);
+        if (iterations) *iterations = r.iterations;
+        if (trace_len) *trace_len = (int)r.trace.size();
+        if (trace)
+            for (int i = 0; i < trace_cap && i < (int)r.trace.size(); ++i) trace[i] = r.trace[i];
+    });
+}
+
+int hm_copy(hm_matrix src, hm_matrix* dst) {
+    return guarded([&] {
+        HMB_REQUIRE(src && dst, HM_ERR_ARGUMENT, "NULL argument");
+        HMB_REQUIRE(*dst != src, HM_ERR_ARGUMENT, "copy onto itself");
+        if (*dst == nullptr) *dst = new hm_matrix_s;
+        hmat_copy(*src->h.ctx, src->h, (*dst)->h);
+    });
+}
+
+int hm_transpose(hm_matrix src, hm_matrix* dst) {
+    return guarded([&] {
+        HMB_REQUIRE(src && dst, HM_ERR_ARGUMENT, "NULL argument");
+        HMB_REQUIRE(*dst != src, HM_ERR_ARGUMENT, "transpose onto itself");
+        if (*dst == nullptr) *dst = new hm_matrix_s;
+        hmat_transpose(*src->h.ctx, src->h, (*dst)->h);
+    });
+}
+
+int hm_scale(hm_matrix h, double alpha) {
+    return guarded([&] {
+        HMB_REQUIRE(h, HM_ERR_ARGUMENT, "h is NULL");
+        hmat_scale(*h->h.ctx, h->h, alpha);
+    });
+}
+
+int hm_add_constant_to_diagonal(hm_matrix h, double alpha) {
+    return guarded([&] {
+        HMB_REQUIRE(h, HM_ERR_ARGUMENT, "h is NULL");
+        hmat_add_diagonal(*h->h.ctx, h->h, alpha);
     });
 }
 

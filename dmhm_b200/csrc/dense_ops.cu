@@ -1,0 +1,120 @@
+// Batched small dense products for the leaf algebra of the H*H product:
+// C = alpha op(A) op(B) + beta C, one CTA per product, 64 x 64 output tiles.
+//
+// These replace the reference's per-leaf BLAS calls in the dense and
+// low-rank leaf products (src/hmat_tools/MultiplyMatrix.cpp:31-450: D*D,
+// D*F, F*D, F*F, and the dense updates of src/hmat_tools/Update.cpp:14-108),
+// which the reference issues one gemm at a time.
+#include "dense_ops.h"
+
+#include <algorithm>
+
+namespace hmb {
+
+namespace {
+
+constexpr int kT = 256;
+
+__device__ __forceinline__ double ld_op(const double* X, int ld, bool trans, int i, int j) {
+    return trans ? X[j + (long long)i * ld] : X[i + (long long)j * ld];
+}
+
+// One CTA per (op, 64x64 output tile).  k < 0 means C = alpha A + beta C.
+__global__ void __launch_bounds__(kT)
+gemm_ops_kernel(const GemmOp* __restrict__ ops, const int* __restrict__ tile_op,
+                const int* __restrict__ tile_id) {
+    const GemmOp op = ops[tile_op[blockIdx.x]];
+    const int tile = tile_id[blockIdx.x];
+    const int tiles_m = (op.m + 63) / 64;
+    const int i0 = (tile % tiles_m) * 64, j0 = (tile / tiles_m) * 64;
+    const int tid = threadIdx.x;
+    if (op.k < 0) {
+        for (int e = tid; e < 64 * 64; e += kT) {
+            int i = i0 + (e & 63), j = j0 + (e >> 6);
+            if (i < op.m && j < op.n) {
+                double a = op.alpha == 0.0 ? 0.0 : op.alpha * ld_op(op.A, op.lda, op.transA, i, j);
+                double* c = op.C + i + (long long)j * op.ldc;
+                *c = op.beta == 0.0 ? a : a + op.beta * *c;
+            }
+        }
+        return;
+    }
+    __shared__ double sA[16][65];
+    __shared__ double sB[16][65];
+    const int tr = (tid & 15) * 4, tc = (tid >> 4) * 4;
+    double acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+    for (int p0 = 0; p0 < op.k; p0 += 16) {
+        for (int e = tid; e < 16 * 64; e += kT) {
+            int i, p;
+            if (op.transA) { p = e & 15; i = e >> 4; }
+            else { i = e & 63; p = e >> 6; }
+            int gi = i0 + i, gp = p0 + p;
+            sA[p][i] = (gi < op.m && gp < op.k) ? ld_op(op.A, op.lda, op.transA, gi, gp) : 0.0;
+        }
+        for (int e = tid; e < 16 * 64; e += kT) {
+            int p, j;
+            if (op.transB) { j = e & 63; p = e >> 6; }
+            else { p = e & 15; j = e >> 4; }
+            int gj = j0 + j, gp = p0 + p;
+            sB[p][j] = (gj < op.n && gp < op.k) ? ld_op(op.B, op.ldb, op.transB, gp, gj) : 0.0;
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int p = 0; p < 16; ++p) {
+            double av[4], bv[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) av[a] = sA[p][tr + a];
+#pragma unroll
+            for (int b = 0; b < 4; ++b) bv[b] = sB[p][tc + b];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        int i = i0 + tr + a;
+        if (i >= op.m) continue;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            int j = j0 + tc + b;
+            if (j >= op.n) continue;
+            double* c = op.C + i + (long long)j * op.ldc;
+            double v = op.alpha * acc[a][b];
+            *c = op.beta == 0.0 ? v : v + op.beta * *c;
+        }
+    }
+}
+
+}  // namespace
+
+void launch_gemm_ops(Context& ctx, const std::vector<GemmOp>& ops, const char* name) {
+    std::vector<int> tile_op, tile_id;
+    for (size_t o = 0; o < ops.size(); ++o) {
+        const GemmOp& g = ops[o];
+        if (g.m <= 0 || g.n <= 0) continue;
+        int tiles = ceil_div(g.m, 64) * ceil_div(g.n, 64);
+        for (int t = 0; t < tiles; ++t) {
+            tile_op.push_back((int)o);
+            tile_id.push_back(t);
+        }
+    }
+    if (tile_op.empty()) return;
+    DeviceBuffer<GemmOp> d_ops;
+    DeviceBuffer<int> d_to, d_ti;
+    d_ops.upload(ops, ctx.stream);
+    d_to.upload(tile_op, ctx.stream);
+    d_ti.upload(tile_id, ctx.stream);
+    LaunchScope ls(ctx, name);
+    gemm_ops_kernel<<<(unsigned)tile_op.size(), kT, 0, ctx.stream>>>(d_ops.get(), d_to.get(),
+                                                                     d_ti.get());
+    HMB_CHECK_LAUNCH();
+}
+
+}  // namespace hmb

@@ -1,0 +1,22 @@
+// Batched small dense products and elementwise updates (see dense_ops.cu).
+#pragma once
+#include <vector>
+
+#include "engine.h"
+
+namespace hmb {
+
+// C = alpha op(A) op(B) + beta C (k >= 0), or C = alpha op(A) + beta C (k < 0).
+// op(X) = X^T when trans is set.  All column-major.  beta == 0 never reads C.
+struct GemmOp {
+    const double* A;
+    const double* B;
+    double* C;
+    double alpha, beta;
+    int m, n, k, lda, ldb, ldc, transA, transB;
+};
+
+// Launches all ops in one kernel; ops must write disjoint C matrices.
+void launch_gemm_ops(Context& ctx, const std::vector<GemmOp>& ops, const char* name);
+
+}  // namespace hmb

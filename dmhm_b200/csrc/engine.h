@@ -121,6 +121,7 @@ struct JobArgs {
     double* out;
     double alpha, beta;
     int ldin, ldout, k, pad;
+    const double* alpha_scale = nullptr;   // if set, alpha is multiplied by *alpha_scale
 };
 
 // Work lists of a batch of jobs, resident on the device: build once, execute
@@ -139,5 +140,14 @@ void run_jobs(Context& ctx, const std::vector<MatJob>& jobs);
 
 // Device kernels driven from the host side (launchers).
 void launch_fill_random(Context& ctx, HMatrix& H);
+
+// Gaussian fills (SerialGaussianRandomVectors on Dense<Real>) of m x n
+// column-major matrices, each starting at LCG state `base`.
+struct FillOp {
+    double* dst;
+    uint64_t base;
+    int m, n;
+};
+void launch_gaussian_fills(Context& ctx, const std::vector<FillOp>& fills, const char* name);
 
 }  // namespace hmb

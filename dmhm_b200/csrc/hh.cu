@@ -1,0 +1,670 @@
+// H*H product (HMat2d::Multiply against an H-matrix) as a host symbolic
+// phase plus level-batched device phases.
+//
+// The reference (src/HMat2d/MultiplyHMat-incl.hpp:12-380; 3-D
+// src/HMat3d/MultiplyHMat-incl.hpp) recurses over the t, s, u children of
+// every non-admissible node, forming for each (A-block, B-block) pair a
+// low-rank or dense product W and folding it into the matching C block in a
+// fixed order: first product sets the block, later ones are added with
+// RoundedUpdate (fixed-rank truncation to maxRank), pushed down through
+// ImportLowRank / UpdateWithLowRank (src/HMat2d/HMat2d.cpp:811-959), or
+// accumulated into dense leaves.  Randomized sampling
+// (include/dmhm/hmat_tools.hpp:1657-1746) handles node x node products and
+// draws its Gaussian test matrix from the serial generator in recursion
+// order.
+//
+// Here the same recursion runs once on the host, on block ids only, and
+// records (a) every product W with its kind, size and rank, (b) for every C
+// leaf block the ordered list of operations it receives, and (c) the
+// generator position of every sampled product.  All ranks follow from the
+// structure, so every buffer is sized before any device work.  The device
+// then
+//   1. draws all Gaussian test matrices at once (skip-ahead LCG),
+//   2. runs all H-matrix x dense products of all samplings as four batched
+//      launch pairs (B Omega, A X, A^T Q, B^T Z), orthonormalizes all samples
+//      in one launch and rounds all sampled products in one launch,
+//   3. forms all leaf-level products in two batched GEMM launches,
+//   4. applies the per-block operation lists in waves: wave j performs the
+//      j-th operation of every C block (one rounding launch and one dense
+//      launch per wave), which keeps the reference's order within each block
+//      while all blocks proceed in parallel.
+#include "hh.h"
+
+#include <algorithm>
+#include <cstring>
+
+#include "dense_ops.h"
+#include "lowrank.h"
+#include "rng.cuh"
+
+namespace hmb {
+
+namespace {
+
+enum WType { W_LRLR, W_LRH, W_LRD, W_HLR, W_DLR, W_HH, W_DD };
+
+struct WTask {
+    int type;
+    int a, b;
+    double alpha;
+    int m, n, r;          // W: m x n; rank r (low-rank) or dense
+    // storage: aliases into A/B or owned slots in the W arena
+    const double* U = nullptr;
+    const double* V = nullptr;
+    const double* D = nullptr;
+    int ldU = 0, ldV = 0;
+    long long u_off = -1, v_off = -1, d_off = -1, g_off = -1;
+    // randomized sampling
+    int k = 0, kq = 0;
+    uint64_t omega = 0;
+    long long s_omega = -1, s_x = -1, s_y = -1, s_q = -1, s_tau = -1, s_z1 = -1, s_z = -1,
+              s_work = -1;
+};
+
+enum LType { L_SET, L_RUPD, L_DDC, L_RESET };
+struct LOp {
+    int type;
+    int w;
+    int row0, col0;   // restriction of W: rows of U / rows of V
+    double beta;
+};
+
+enum DType { D_LR, D_DD, D_COPY };
+struct DOp {
+    int type;
+    int w;
+    int row0, col0;
+    double alpha, beta;
+    int a, b;
+};
+
+struct Planner {
+    const Structure& S;
+    const HMatrix& A;
+    const HMatrix& B;
+    int maxRankC;
+    int oversample;
+    uint64_t serial;
+    std::vector<WTask> w;
+    std::vector<std::vector<LOp>> lops;
+    std::vector<std::vector<DOp>> dops;
+
+    Planner(const HMatrix& a, const HMatrix& b, int maxRank, int over, uint64_t st)
+        : S(*a.S), A(a), B(b), maxRankC(maxRank), oversample(over), serial(st),
+          lops(a.S->blocks.size()), dops(a.S->blocks.size()) {}
+
+    int kind(int blk) const { return S.blocks[blk].kind; }
+
+    int product(int a, int b, double alpha) {
+        WTask t{};
+        t.a = a;
+        t.b = b;
+        t.alpha = alpha;
+        t.m = S.blocks[a].m;
+        t.n = S.blocks[b].n;
+        const int ka = kind(a), kb = kind(b);
+        if (ka == KIND_LOWRANK && kb == KIND_LOWRANK) {
+            t.type = W_LRLR;
+            t.r = std::min(A.rank[a], B.rank[b]);
+        } else if (ka == KIND_LOWRANK && kb == KIND_NODE) {
+            t.type = W_LRH;
+            t.r = A.rank[a];
+        } else if (ka == KIND_LOWRANK && kb == KIND_DENSE) {
+            t.type = W_LRD;
+            t.r = A.rank[a];
+        } else if (ka == KIND_NODE && kb == KIND_LOWRANK) {
+            t.type = W_HLR;
+            t.r = B.rank[b];
+        } else if (ka == KIND_DENSE && kb == KIND_LOWRANK) {
+            t.type = W_DLR;
+            t.r = B.rank[b];
+        } else if (ka == KIND_NODE && kb == KIND_NODE) {
+            t.type = W_HH;
+            const Block& BA = S.blocks[a];
+            const Block& BB = S.blocks[b];
+            t.r = std::min(std::min(A.max_rank, B.max_rank),
+                           std::min(std::min(BA.m, BA.n), std::min(BB.m, BB.n)));
+            t.k = maxRankC + oversample;
+            HMB_REQUIRE(t.k <= BB.n, HM_ERR_UNSUPPORTED,
+                        "sample count exceeds the sampled block width (the reference's "
+                        "Gaussian fill would write past its columns)");
+            t.kq = std::min(BA.m, t.k);
+            t.omega = serial;
+            serial = lcg_skip_host(serial, (uint64_t)t.k * 2ULL * (uint64_t)((BB.n + 1) / 2));
+        } else if (ka == KIND_DENSE && kb == KIND_DENSE) {
+            t.type = W_DD;
+            t.r = -1;
+        } else {
+            throw Error(HM_ERR_UNSUPPORTED, "invalid H-matrix combination");
+        }
+        w.push_back(t);
+        return (int)w.size() - 1;
+    }
+
+    // Multiply(alpha, B, C): C rebuilt (MultiplyHMat-incl.hpp:12-187)
+    void fresh(int a, int b, int c, double alpha) {
+        const int kc = kind(c);
+        if (kc == KIND_LOWRANK) {
+            int t = product(a, b, alpha);
+            lops[c].push_back({w[t].type == W_DD ? L_DDC : L_SET, t, 0, 0, 0.0});
+        } else if (kc == KIND_NODE) {
+            HMB_REQUIRE(kind(a) != KIND_DENSE && kind(b) != KIND_DENSE, HM_ERR_UNSUPPORTED,
+                        "invalid H-matrix combination");
+            if (kind(a) == KIND_LOWRANK || kind(b) == KIND_LOWRANK) {
+                int t = product(a, b, alpha);
+                import_lowrank(c, t, 0, 0);
+            } else {
+                for (int ti = 0; ti < S.q; ++ti)
+                    for (int si = 0; si < S.q; ++si) {
+                        fresh(S.child(a, ti, 0), S.child(b, 0, si), S.child(c, ti, si), alpha);
+                        for (int u = 1; u < S.q; ++u)
+                            update(S.child(a, ti, u), S.child(b, u, si), S.child(c, ti, si),
+                                   alpha, 1.0);
+                    }
+            }
+        } else {
+            dense_into(c, a, b, alpha, 0.0);
+        }
+    }
+
+    // Multiply(alpha, B, beta, C) (MultiplyHMat-incl.hpp:189-380)
+    void update(int a, int b, int c, double alpha, double beta) {
+        const int kc = kind(c);
+        if (kc == KIND_LOWRANK) {
+            int t = product(a, b, alpha);
+            lops[c].push_back({w[t].type == W_DD ? L_DDC : L_RUPD, t, 0, 0, beta});
+        } else if (kc == KIND_NODE) {
+            HMB_REQUIRE(kind(a) != KIND_DENSE && kind(b) != KIND_DENSE, HM_ERR_UNSUPPORTED,
+                        "invalid H-matrix combination");
+            if (kind(a) == KIND_LOWRANK || kind(b) == KIND_LOWRANK) {
+                int t = product(a, b, alpha);
+                update_with_lowrank(c, t, 0, 0, beta);
+            } else {
+                for (int ti = 0; ti < S.q; ++ti)
+                    for (int si = 0; si < S.q; ++si) {
+                        update(S.child(a, ti, 0), S.child(b, 0, si), S.child(c, ti, si), alpha,
+                               beta);
+                        for (int u = 1; u < S.q; ++u)
+                            update(S.child(a, ti, u), S.child(b, u, si), S.child(c, ti, si),
+                                   alpha, 1.0);
+                    }
+            }
+        } else {
+            dense_into(c, a, b, alpha, beta);
+        }
+    }
+
+    void dense_into(int c, int a, int b, double alpha, double beta) {
+        HMB_REQUIRE(kind(a) != KIND_NODE && kind(b) != KIND_NODE, HM_ERR_UNSUPPORTED,
+                    "invalid H-matrix combination");
+        if (kind(a) == KIND_DENSE && kind(b) == KIND_DENSE) {
+            dops[c].push_back({D_DD, -1, 0, 0, alpha, beta, a, b});
+        } else {
+            int t = product(a, b, alpha);
+            dops[c].push_back({D_LR, t, 0, 0, 1.0, beta, -1, -1});
+        }
+    }
+
+    // ImportLowRank (HMat2d.cpp:811-904)
+    void import_lowrank(int c, int t, int row0, int col0) {
+        const Block& C = S.blocks[c];
+        if (C.kind == KIND_LOWRANK) {
+            lops[c].push_back({L_SET, t, row0, col0, 0.0});
+        } else if (C.kind == KIND_NODE) {
+            for (int ti = 0; ti < S.q; ++ti)
+                for (int si = 0; si < S.q; ++si) {
+                    int ch = S.child(c, ti, si);
+                    import_lowrank(ch, t, row0 + S.blocks[ch].row_off - C.row_off,
+                                   col0 + S.blocks[ch].col_off - C.col_off);
+                }
+        } else {
+            dops[c].push_back({D_LR, t, row0, col0, 1.0, 0.0, -1, -1});
+        }
+    }
+
+    // Scale(beta) followed by UpdateWithLowRank(1, W) (HMat2d.cpp:906-959)
+    void update_with_lowrank(int c, int t, int row0, int col0, double beta) {
+        const Block& C = S.blocks[c];
+        if (C.kind == KIND_LOWRANK) {
+            if (beta == 0.0) lops[c].push_back({L_RESET, -1, 0, 0, 0.0});
+            lops[c].push_back({L_RUPD, t, row0, col0, beta == 0.0 ? 1.0 : beta});
+        } else if (C.kind == KIND_NODE) {
+            for (int ti = 0; ti < S.q; ++ti)
+                for (int si = 0; si < S.q; ++si) {
+                    int ch = S.child(c, ti, si);
+                    update_with_lowrank(ch, t, row0 + S.blocks[ch].row_off - C.row_off,
+                                        col0 + S.blocks[ch].col_off - C.col_off, beta);
+                }
+        } else {
+            dops[c].push_back({D_LR, t, row0, col0, 1.0, beta, -1, -1});
+        }
+    }
+};
+
+// A slot of a scratch arena handed out by offsets (doubles), 16-byte aligned.
+struct Arena {
+    long long used = 0;
+    long long take(long long n) {
+        long long o = used;
+        used += (std::max<long long>(n, 0) + 1) & ~1LL;
+        return o;
+    }
+};
+
+}  // namespace
+
+void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha, double beta,
+                 HMatrix& C, bool fresh) {
+    HMB_REQUIRE(A.S == B.S, HM_ERR_ARGUMENT,
+                "H*H multiply needs both factors on the same block structure");
+    HMB_REQUIRE(&C != &A && &C != &B, HM_ERR_ARGUMENT,
+                "the product must not overwrite a factor");
+    const Structure& S = *A.S;
+    cudaStream_t st = ctx.stream;
+    if (!fresh) {
+        HMB_REQUIRE(C.S == A.S, HM_ERR_ARGUMENT, "C must share the factors' block structure");
+    }
+    const int maxRankC = fresh ? A.max_rank : C.max_rank;
+
+    // ---------------- symbolic phase ----------------
+    Planner P(A, B, maxRankC, ctx.oversample, ctx.serial_state);
+    if (fresh)
+        P.fresh(0, 0, 0, alpha);
+    else
+        P.update(0, 0, 0, alpha, beta);
+    const uint64_t serial_after = P.serial;
+
+    // final ranks of C
+    std::vector<int> crank(S.blocks.size(), 0);
+    std::vector<int> nops_lr(S.blocks.size(), 0);
+    std::vector<std::vector<int>> state_rank(S.blocks.size());   // rank after each op
+    std::vector<std::vector<int>> op_kind(S.blocks.size());      // RoundKind per op (-1 reset)
+    for (int c : S.leaves) {
+        const Block& Cb = S.blocks[c];
+        if (Cb.kind != KIND_LOWRANK) continue;
+        int rank = fresh ? 0 : C.rank[c];
+        const int minDim = std::min(Cb.m, Cb.n);
+        for (const LOp& op : P.lops[c]) {
+            int kindr = -1;
+            switch (op.type) {
+                case L_SET:
+                    rank = P.w[op.w].r;
+                    kindr = ROUND_SET;
+                    break;
+                case L_RESET:
+                    rank = 0;
+                    kindr = -1;
+                    break;
+                case L_RUPD: {
+                    int r = P.w[op.w].r + rank;
+                    int rr = std::min(std::min(r, minDim), maxRankC);
+                    kindr = (rr == r) ? ROUND_CONCAT : ROUND_GENERAL;
+                    rank = rr;
+                    break;
+                }
+                case L_DDC:
+                    rank = std::min(minDim, maxRankC);
+                    kindr = ROUND_DENSE;
+                    break;
+            }
+            state_rank[c].push_back(rank);
+            op_kind[c].push_back(kindr);
+        }
+        crank[c] = rank;
+    }
+
+    // ---------------- allocation ----------------
+    // keep the old C storage if C is updated in place
+    DeviceBuffer<double> c_old_data;
+    std::vector<long long> c_old_off;
+    std::vector<int> c_old_rank;
+    if (!fresh) {
+        c_old_data = std::move(C.data);
+        c_old_off = C.off;
+        c_old_rank = C.rank;
+    }
+    if (fresh) {
+        C.S = A.S;
+        C.max_rank = A.max_rank;
+        C.ctx = &ctx;
+    }
+    C.rank = crank;
+    C.layout();
+
+    // W arena and sampling scratch
+    Arena wa, sa;
+    for (WTask& t : P.w) {
+        const Block& Ba = S.blocks[t.a];
+        const Block& Bb = S.blocks[t.b];
+        switch (t.type) {
+            case W_LRLR:
+                if (A.rank[t.a] <= B.rank[t.b]) {
+                    t.U = A.U(t.a); t.ldU = Ba.m;
+                    t.v_off = wa.take((long long)t.n * t.r); t.ldV = t.n;
+                } else {
+                    t.u_off = wa.take((long long)t.m * t.r); t.ldU = t.m;
+                    t.V = B.V(t.b); t.ldV = Bb.n;
+                }
+                t.g_off = wa.take((long long)B.rank[t.b] * A.rank[t.a]);
+                break;
+            case W_LRH:
+            case W_LRD:
+                t.U = A.U(t.a); t.ldU = Ba.m;
+                t.v_off = wa.take((long long)t.n * t.r); t.ldV = t.n;
+                break;
+            case W_HLR:
+            case W_DLR:
+                t.u_off = wa.take((long long)t.m * t.r); t.ldU = t.m;
+                t.V = B.V(t.b); t.ldV = Bb.n;
+                break;
+            case W_HH: {
+                t.u_off = wa.take((long long)t.m * t.r); t.ldU = t.m;
+                t.v_off = wa.take((long long)t.n * t.r); t.ldV = t.n;
+                t.s_omega = sa.take((long long)Bb.n * t.k);
+                t.s_x = sa.take((long long)Bb.m * t.k);
+                t.s_y = sa.take((long long)Ba.m * t.k);
+                t.s_q = sa.take((long long)Ba.m * t.kq);
+                t.s_tau = sa.take(t.k);
+                t.s_z1 = sa.take((long long)Ba.n * t.kq);
+                t.s_z = sa.take((long long)Bb.n * t.kq);
+                RoundOp probe{};
+                probe.kind = ROUND_ORTHO; probe.m = t.m; probe.n = t.n; probe.r1 = t.kq;
+                t.s_work = sa.take(round_work_size(probe));
+                break;
+            }
+            case W_DD:
+                t.d_off = wa.take((long long)t.m * t.n);
+                break;
+        }
+    }
+    DeviceBuffer<double> warena, sarena;
+    warena.allocate((size_t)std::max<long long>(wa.used, 2), st);
+    sarena.allocate((size_t)std::max<long long>(sa.used, 2), st);
+    double* W0 = warena.get();
+    double* S0 = sarena.get();
+    for (WTask& t : P.w) {
+        if (t.u_off >= 0) t.U = W0 + t.u_off;
+        if (t.v_off >= 0) t.V = W0 + t.v_off;
+        if (t.d_off >= 0) t.D = W0 + t.d_off;
+    }
+
+    // ---------------- randomized sampling ----------------
+    std::vector<int> hh;
+    for (int i = 0; i < (int)P.w.size(); ++i)
+        if (P.w[i].type == W_HH && P.w[i].r > 0) hh.push_back(i);
+    {
+        // Gaussian test matrices: SerialGaussianRandomVectors(Omega), n_b x k
+        std::vector<FillOp> fills;
+        for (int i : hh) {
+            const WTask& t = P.w[i];
+            fills.push_back({S0 + t.s_omega, t.omega, S.blocks[t.b].n, t.k});
+        }
+        launch_gaussian_fills(ctx, fills, "omega_fill");
+    }
+    // X = alpha B Omega, and W.U = alpha A B.U for node x low-rank
+    {
+        std::vector<MatJob> jobs;
+        for (int i : hh) {
+            const WTask& t = P.w[i];
+            const Block& Bb = S.blocks[t.b];
+            jobs.push_back({&B, t.b, false, t.alpha, 0.0, S0 + t.s_omega, Bb.n, S0 + t.s_x, Bb.m,
+                            t.k});
+        }
+        for (const WTask& t : P.w)
+            if (t.type == W_HLR && t.r > 0)
+                jobs.push_back({&A, t.a, false, t.alpha, 0.0, B.U(t.b), S.blocks[t.b].m,
+                                const_cast<double*>(t.U), t.m, t.r});
+        run_jobs(ctx, jobs);
+    }
+    // Y = A X
+    {
+        std::vector<MatJob> jobs;
+        for (int i : hh) {
+            const WTask& t = P.w[i];
+            const Block& Ba = S.blocks[t.a];
+            jobs.push_back({&A, t.a, false, 1.0, 0.0, S0 + t.s_x, Ba.n, S0 + t.s_y, Ba.m, t.k});
+        }
+        run_jobs(ctx, jobs);
+    }
+    // Q = orth(Y)
+    {
+        std::vector<QrOp> q;
+        for (int i : hh) {
+            const WTask& t = P.w[i];
+            q.push_back({S0 + t.s_y, S0 + t.s_q, S0 + t.s_tau, t.m, t.k, t.m, 0});
+        }
+        launch_qr_formq(ctx, q, "sample_qr");
+    }
+    // Z1 = alpha A^T Q, and W.V = alpha B^T A.V for low-rank x node
+    {
+        std::vector<MatJob> jobs;
+        for (int i : hh) {
+            const WTask& t = P.w[i];
+            const Block& Ba = S.blocks[t.a];
+            jobs.push_back({&A, t.a, true, t.alpha, 0.0, S0 + t.s_q, Ba.m, S0 + t.s_z1, Ba.n,
+                            t.kq});
+        }
+        for (const WTask& t : P.w)
+            if (t.type == W_LRH && t.r > 0)
+                jobs.push_back({&B, t.b, true, t.alpha, 0.0, A.V(t.a), S.blocks[t.a].n,
+                                const_cast<double*>(t.V), t.n, t.r});
+        run_jobs(ctx, jobs);
+    }
+    // Z = B^T Z1
+    {
+        std::vector<MatJob> jobs;
+        for (int i : hh) {
+            const WTask& t = P.w[i];
+            const Block& Bb = S.blocks[t.b];
+            jobs.push_back({&B, t.b, true, 1.0, 0.0, S0 + t.s_z1, Bb.m, S0 + t.s_z, Bb.n, t.kq});
+        }
+        run_jobs(ctx, jobs);
+    }
+    // W = best rank-r of Q Z^T (the gesvd truncation of hmat_tools.hpp:1712-1745)
+    {
+        std::vector<RoundOp> ops;
+        for (int i : hh) {
+            const WTask& t = P.w[i];
+            RoundOp op{};
+            op.kind = ROUND_ORTHO;
+            op.m = t.m;
+            op.n = t.n;
+            op.u1 = S0 + t.s_q; op.ldu1 = t.m; op.r1 = t.kq;
+            op.v1 = S0 + t.s_z; op.ldv1 = t.n;
+            op.rout = t.r;
+            op.uo = const_cast<double*>(t.U);
+            op.vo = const_cast<double*>(t.V);
+            op.work = S0 + t.s_work;
+            op.alpha = 1.0;
+            ops.push_back(op);
+        }
+        launch_round_ops(ctx, ops, "sample_round");
+    }
+    // HH products with rank 0 (empty blocks): nothing to compute.
+
+    // ---------------- leaf products ----------------
+    {
+        std::vector<GemmOp> g1, g2;
+        for (const WTask& t : P.w) {
+            const Block& Ba = S.blocks[t.a];
+            const Block& Bb = S.blocks[t.b];
+            const int ra = A.rank[t.a], rb = B.rank[t.b];
+            switch (t.type) {
+                case W_LRLR:
+                    if (t.r == 0) break;
+                    if (ra <= rb) {
+                        // G = B.U^T A.V (rb x ra); V = alpha B.V G
+                        g1.push_back({B.U(t.b), A.V(t.a), W0 + t.g_off, 1.0, 0.0, rb, ra, Bb.m,
+                                      Bb.m, Ba.n, rb, 1, 0});
+                        g2.push_back({B.V(t.b), W0 + t.g_off, const_cast<double*>(t.V), t.alpha,
+                                      0.0, Bb.n, ra, rb, Bb.n, rb, t.n, 0, 0});
+                    } else {
+                        // G = A.V^T B.U (ra x rb); U = alpha A.U G
+                        g1.push_back({A.V(t.a), B.U(t.b), W0 + t.g_off, 1.0, 0.0, ra, rb, Ba.n,
+                                      Ba.n, Bb.m, ra, 1, 0});
+                        g2.push_back({A.U(t.a), W0 + t.g_off, const_cast<double*>(t.U), t.alpha,
+                                      0.0, Ba.m, rb, ra, Ba.m, ra, t.m, 0, 0});
+                    }
+                    break;
+                case W_LRD:   // V = alpha B.D^T A.V
+                    if (t.r == 0) break;
+                    g1.push_back({B.D(t.b), A.V(t.a), const_cast<double*>(t.V), t.alpha, 0.0,
+                                  Bb.n, t.r, Bb.m, Bb.m, Ba.n, t.n, 1, 0});
+                    break;
+                case W_DLR:   // U = alpha A.D B.U
+                    if (t.r == 0) break;
+                    g1.push_back({A.D(t.a), B.U(t.b), const_cast<double*>(t.U), t.alpha, 0.0,
+                                  Ba.m, t.r, Ba.n, Ba.m, Bb.m, t.m, 0, 0});
+                    break;
+                case W_DD:    // D = alpha A.D B.D
+                    g1.push_back({A.D(t.a), B.D(t.b), const_cast<double*>(t.D), t.alpha, 0.0,
+                                  Ba.m, Bb.n, Ba.n, Ba.m, Bb.m, t.m, 0, 0});
+                    break;
+                default:
+                    break;
+            }
+        }
+        launch_gemm_ops(ctx, g1, "leaf_products");
+        launch_gemm_ops(ctx, g2, "leaf_products");
+    }
+
+    // ---------------- waves over the C blocks ----------------
+    // ping-pong state slots for low-rank blocks with more than one operation
+    Arena pa;
+    std::vector<long long> slot0(S.blocks.size(), -1), slot1(S.blocks.size(), -1);
+    size_t max_ops = 0;
+    for (int c : S.leaves) {
+        const Block& Cb = S.blocks[c];
+        if (Cb.kind == KIND_LOWRANK) {
+            max_ops = std::max(max_ops, P.lops[c].size());
+            int mr = 0;
+            for (size_t j = 0; j + 1 < state_rank[c].size(); ++j)
+                mr = std::max(mr, state_rank[c][j]);
+            if (P.lops[c].size() > 1) {
+                slot0[c] = pa.take((long long)(Cb.m + Cb.n) * mr);
+                slot1[c] = pa.take((long long)(Cb.m + Cb.n) * mr);
+            }
+        } else {
+            max_ops = std::max(max_ops, P.dops[c].size() + (fresh ? 0 : 1));
+        }
+    }
+    DeviceBuffer<double> parena;
+    parena.allocate((size_t)std::max<long long>(pa.used, 2), st);
+    double* P0 = parena.get();
+    // current state pointer of each low-rank C block
+    std::vector<const double*> cu(S.blocks.size(), nullptr), cv(S.blocks.size(), nullptr);
+    std::vector<int> cr(S.blocks.size(), 0);
+    if (!fresh) {
+        for (int c : S.leaves)
+            if (S.blocks[c].kind == KIND_LOWRANK) {
+                cu[c] = c_old_data.get() + c_old_off[c];
+                cv[c] = cu[c] + (long long)S.blocks[c].m * c_old_rank[c];
+                cr[c] = c_old_rank[c];
+            }
+    }
+    for (size_t wv = 0; wv < max_ops; ++wv) {
+        std::vector<RoundOp> rops;
+        Arena work;
+        std::vector<size_t> need_work;
+        std::vector<GemmOp> gops;
+        for (int c : S.leaves) {
+            const Block& Cb = S.blocks[c];
+            if (Cb.kind == KIND_LOWRANK) {
+                if (wv >= P.lops[c].size()) continue;
+                const LOp& op = P.lops[c][wv];
+                const int rnew = state_rank[c][wv];
+                if (op.type == L_RESET) {
+                    cr[c] = 0;
+                    continue;
+                }
+                const bool last = wv + 1 == P.lops[c].size();
+                double* ou;
+                if (last) {
+                    ou = C.U(c);
+                } else {
+                    ou = P0 + ((wv & 1) ? slot1[c] : slot0[c]);
+                }
+                double* ov = ou + (long long)Cb.m * rnew;
+                const WTask& t = P.w[op.w];
+                RoundOp r{};
+                r.kind = op_kind[c][wv];
+                r.m = Cb.m;
+                r.n = Cb.n;
+                r.alpha = 1.0;
+                r.beta = op.beta;
+                r.rout = rnew;
+                r.uo = ou;
+                r.vo = ov;
+                if (op.type == L_DDC) {
+                    r.u1 = t.D;
+                    r.ldu1 = t.m;
+                } else {
+                    r.u1 = t.U ? t.U + op.row0 : nullptr;
+                    r.v1 = t.V ? t.V + op.col0 : nullptr;
+                    r.ldu1 = t.ldU;
+                    r.ldv1 = t.ldV;
+                    r.r1 = t.r;
+                }
+                r.u2 = cu[c];
+                r.v2 = cv[c];
+                r.r2 = (op.type == L_SET) ? 0 : cr[c];
+                r.ldu2 = Cb.m;
+                r.ldv2 = Cb.n;
+                if (op.type == L_DDC && op.beta == 0.0) r.r2 = 0;
+                if (rnew == 0 || Cb.m == 0 || Cb.n == 0) {
+                    // nothing to compute: empty result
+                } else {
+                    rops.push_back(r);
+                    need_work.push_back(rops.size() - 1);
+                }
+                cu[c] = ou;
+                cv[c] = ov;
+                cr[c] = rnew;
+            } else {
+                // dense leaf: optional initial copy of the old block (update form)
+                size_t idx = wv;
+                if (!fresh) {
+                    if (wv == 0) {
+                        gops.push_back({c_old_data.get() + c_old_off[c], nullptr, C.D(c), 1.0, 0.0,
+                                        Cb.m, Cb.n, -1, Cb.m, 0, Cb.m, 0, 0});
+                        continue;
+                    }
+                    idx = wv - 1;
+                }
+                if (idx >= P.dops[c].size()) continue;
+                const DOp& op = P.dops[c][idx];
+                if (op.type == D_DD) {
+                    const Block& Ba = S.blocks[op.a];
+                    const Block& Bb = S.blocks[op.b];
+                    gops.push_back({A.D(op.a), B.D(op.b), C.D(c), op.alpha, op.beta, Cb.m, Cb.n,
+                                    Ba.n, Ba.m, Bb.m, Cb.m, 0, 0});
+                } else {
+                    const WTask& t = P.w[op.w];
+                    if (t.r == 0) {
+                        // D := beta D (+ 0)
+                        gops.push_back({C.D(c), nullptr, C.D(c), op.beta, 0.0, Cb.m, Cb.n, -1,
+                                        Cb.m, 0, Cb.m, 0, 0});
+                    } else {
+                        gops.push_back({t.U + op.row0, t.V + op.col0, C.D(c), 1.0, op.beta, Cb.m,
+                                        Cb.n, t.r, t.ldU, t.ldV, Cb.m, 0, 1});
+                    }
+                }
+            }
+        }
+        // scratch for the rounding ops of this wave
+        std::vector<long long> woff(rops.size(), 0);
+        for (size_t i = 0; i < rops.size(); ++i) woff[i] = work.take(round_work_size(rops[i]));
+        DeviceBuffer<double> wbuf;
+        if (!rops.empty()) {
+            wbuf.allocate((size_t)std::max<long long>(work.used, 2), st);
+            for (size_t i = 0; i < rops.size(); ++i) rops[i].work = wbuf.get() + woff[i];
+        }
+        launch_round_ops(ctx, rops, "block_round");
+        launch_gemm_ops(ctx, gops, "dense_update");
+    }
+    // low-rank C blocks whose final rank is 0 or that received no operation
+    // need nothing: their storage is empty.
+    ctx.serial_state = serial_after;
+}
+
+}  // namespace hmb

@@ -133,4 +133,20 @@ void launch_fill_random(Context& ctx, HMatrix& H) {
     HMB_CHECK_LAUNCH();
 }
 
+void launch_gaussian_fills(Context& ctx, const std::vector<FillOp>& fills, const char* name) {
+    std::vector<FillTask> tasks;
+    for (const FillOp& f : fills) {
+        if (f.m == 0 || f.n == 0) continue;
+        HMB_REQUIRE(f.n <= f.m, HM_ERR_UNSUPPORTED,
+                    "Gaussian fill wider than tall (the reference would write past its columns)");
+        tasks.push_back({f.dst, nullptr, f.base, 0, f.m, f.n});
+    }
+    if (tasks.empty()) return;
+    DeviceBuffer<FillTask> d;
+    d.upload(tasks, ctx.stream);
+    LaunchScope ls(ctx, name);
+    fill_gaussian_kernel<<<(unsigned)tasks.size(), 256, 0, ctx.stream>>>(d.get());
+    HMB_CHECK_LAUNCH();
+}
+
 }  // namespace hmb

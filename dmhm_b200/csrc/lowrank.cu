@@ -1,0 +1,410 @@
+// Batched low-rank rounding: the device replacement of the reference's
+// per-block LAPACK sequences
+//   RoundedUpdate   (src/hmat_tools/RoundedUpdate.cpp:14-162: two geqrf,
+//                    R1 R2^T, gesvd, two ormqr),
+//   Compress / D*D  (src/hmat_tools/Compress.cpp:14-53,
+//                    MultiplyMatrix.cpp:405-550: gesvd of a dense block),
+//   randomized H*H  (include/dmhm/hmat_tools.hpp:1690-1745: geqp3 + orgqr of
+//                    the sample, gesvd of the projected block).
+// One CTA (256 threads) owns one rounding: Householder QR of the stacked
+// factors (FP64, rank-deficient safe: zero columns give tau = 0), the small
+// core M = R_u R_v^T, a one-sided Jacobi SVD of M with the rotations
+// accumulated, selection of the largest singular triplets, and the
+// reflectors applied back.  The truncated result is the same best rank-r
+// approximation the reference computes (its factors differ only by the
+// usual sign / rotation freedom of an SVD).
+#include "lowrank.h"
+
+#include <algorithm>
+
+namespace hmb {
+
+namespace {
+
+constexpr int kT = 256;
+constexpr int kW = kT / 32;
+constexpr int kMaxK = 128;         // largest stacked rank handled
+constexpr int kSmemK = 64;         // M and J in shared memory up to this k
+constexpr int kJacobiSweeps = 40;  // bounded; converges in ~6-12
+constexpr double kJacobiTol = 1e-15;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ double block_sum(double v, double* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    v = warp_sum(v);
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double t = threadIdx.x < kW ? red[threadIdx.x] : 0.0;
+    if (warp == 0) t = warp_sum(t);
+    if (threadIdx.x == 0) red[kW] = t;
+    __syncthreads();
+    double r = red[kW];
+    __syncthreads();
+    return r;
+}
+
+// In-place Householder QR (LAPACK dgeqr2 conventions: beta = -sign(alpha)
+// ||x||, v(1) = 1 implicit, tau = (beta - alpha) / beta; tau = 0 when the
+// column below the diagonal is zero).
+__device__ void cta_qr(double* A, int m, int n, int ld, double* tau, double* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int kk = min(m, n);
+    for (int j = 0; j < kk; ++j) {
+        double* col = A + j + (long long)j * ld;
+        const int len = m - j;
+        double s = 0.0;
+        for (int i = 1 + threadIdx.x; i < len; i += kT) s += col[i] * col[i];
+        s = block_sum(s, red);
+        const double alpha = col[0];
+        double t = 0.0, beta = alpha;
+        if (s != 0.0) {
+            beta = -copysign(sqrt(alpha * alpha + s), alpha);
+            t = (beta - alpha) / beta;
+            const double scal = 1.0 / (alpha - beta);
+            for (int i = 1 + threadIdx.x; i < len; i += kT) col[i] *= scal;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            col[0] = beta;
+            tau[j] = t;
+        }
+        __syncthreads();
+        if (t != 0.0) {
+            for (int c = j + 1 + warp; c < n; c += kW) {
+                double* cc = A + j + (long long)c * ld;
+                const double c0 = cc[0];
+                double w = 0.0;
+                for (int i = 1 + lane; i < len; i += 32) w += col[i] * cc[i];
+                w = warp_sum(w) + c0;
+                const double tw = t * w;
+                __syncwarp();
+                if (lane == 0) cc[0] = c0 - tw;
+                for (int i = 1 + lane; i < len; i += 32) cc[i] -= tw * col[i];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// B := Q B with Q = H_0 H_1 ... H_{kk-1} from cta_qr (B is m x p).
+__device__ void cta_apply_q(const double* A, int m, int kk, int lda, const double* tau,
+                            double* B, int p, int ldb) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int j = kk - 1; j >= 0; --j) {
+        const double t = tau[j];
+        if (t == 0.0) continue;
+        const double* v = A + j + (long long)j * lda;
+        const int len = m - j;
+        for (int c = warp; c < p; c += kW) {
+            double* bc = B + j + (long long)c * ldb;
+            const double b0 = bc[0];
+            double w = 0.0;
+            for (int i = 1 + lane; i < len; i += 32) w += v[i] * bc[i];
+            w = warp_sum(w) + b0;
+            const double tw = t * w;
+            __syncwarp();
+            if (lane == 0) bc[0] = b0 - tw;
+            for (int i = 1 + lane; i < len; i += 32) bc[i] -= tw * v[i];
+        }
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ int rr_pos(int i, int step, int n) {
+    return i == 0 ? 0 : 1 + (i - 1 + step) % (n - 1);
+}
+
+// One-sided (Hestenes) Jacobi: rotates the columns of M (rows x cols) until
+// they are mutually orthogonal, accumulating the rotations in J (cols x cols,
+// J starts as I), so M_in = M_out J^T.  Round-robin ordering: cols/2
+// disjoint pairs per step, one warp per pair.  Bounded number of sweeps.
+__device__ void cta_jacobi(double* M, int rows, int cols, double* J, int* flag) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int e = threadIdx.x; e < cols * cols; e += kT)
+        J[e] = (e % cols == e / cols) ? 1.0 : 0.0;
+    __syncthreads();
+    if (cols < 2) return;
+    const int n = cols + (cols & 1);
+    for (int sweep = 0; sweep < kJacobiSweeps; ++sweep) {
+        if (threadIdx.x == 0) *flag = 0;
+        __syncthreads();
+        for (int step = 0; step < n - 1; ++step) {
+            for (int k = warp; k < n / 2; k += kW) {
+                int p = rr_pos(k, step, n), q = rr_pos(n - 1 - k, step, n);
+                if (p >= cols || q >= cols) continue;
+                if (p > q) { int t = p; p = q; q = t; }
+                double* gp = M + (long long)p * rows;
+                double* gq = M + (long long)q * rows;
+                double a = 0.0, b = 0.0, c = 0.0;
+                for (int i = lane; i < rows; i += 32) {
+                    const double x = gp[i], y = gq[i];
+                    a = fma(x, x, a);
+                    b = fma(y, y, b);
+                    c = fma(x, y, c);
+                }
+                a = warp_sum(a);
+                b = warp_sum(b);
+                c = warp_sum(c);
+                if (c != 0.0 && fabs(c) > kJacobiTol * sqrt(a * b)) {
+                    const double zeta = (b - a) / (2.0 * c);
+                    const double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+                    const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
+                    __syncwarp();
+                    for (int i = lane; i < rows; i += 32) {
+                        const double x = gp[i], y = gq[i];
+                        gp[i] = cs * x - sn * y;
+                        gq[i] = sn * x + cs * y;
+                    }
+                    double* jp = J + (long long)p * cols;
+                    double* jq = J + (long long)q * cols;
+                    for (int i = lane; i < cols; i += 32) {
+                        const double x = jp[i], y = jq[i];
+                        jp[i] = cs * x - sn * y;
+                        jq[i] = sn * x + cs * y;
+                    }
+                    if (lane == 0) *flag = 1;
+                }
+            }
+            __syncthreads();
+        }
+        const int again = *flag;
+        __syncthreads();
+        if (!again) break;
+    }
+}
+
+// order[0..cols) = column indices of M by decreasing norm (ties by index).
+__device__ void cta_order_columns(const double* M, int rows, int cols, double* norms,
+                                  int* order) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int c = warp; c < cols; c += kW) {
+        const double* g = M + (long long)c * rows;
+        double s = 0.0;
+        for (int i = lane; i < rows; i += 32) s = fma(g[i], g[i], s);
+        s = warp_sum(s);
+        if (lane == 0) norms[c] = s;
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < cols; j += kT) {
+        const double sj = norms[j];
+        int pos = 0;
+        for (int i = 0; i < cols; ++i) {
+            const double si = norms[i];
+            pos += (si > sj || (si == sj && i < j)) ? 1 : 0;
+        }
+        order[pos] = j;
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kT)
+round_kernel(const RoundOp* __restrict__ ops, int smem_mj) {
+    extern __shared__ double dyn[];
+    __shared__ double red[kW + 1];
+    __shared__ double norms[kMaxK];
+    __shared__ int order[kMaxK];
+    __shared__ int flag;
+    const RoundOp op = ops[blockIdx.x];
+    const int m = op.m, n = op.n;
+    const int tid = threadIdx.x;
+
+    if (op.kind == ROUND_SET) {
+        for (long long e = tid; e < (long long)m * op.r1; e += kT) {
+            int i = (int)(e % m), c = (int)(e / m);
+            op.uo[e] = op.alpha * op.u1[i + (long long)c * op.ldu1];
+        }
+        for (long long e = tid; e < (long long)n * op.r1; e += kT) {
+            int i = (int)(e % n), c = (int)(e / n);
+            op.vo[e] = op.v1[i + (long long)c * op.ldv1];
+        }
+        return;
+    }
+    if (op.kind == ROUND_CONCAT) {
+        const int r2 = op.r2, r = op.r1 + op.r2;
+        for (long long e = tid; e < (long long)m * r; e += kT) {
+            int i = (int)(e % m), c = (int)(e / m);
+            op.uo[e] = c < r2 ? op.beta * op.u2[i + (long long)c * op.ldu2]
+                              : op.alpha * op.u1[i + (long long)(c - r2) * op.ldu1];
+        }
+        for (long long e = tid; e < (long long)n * r; e += kT) {
+            int i = (int)(e % n), c = (int)(e / n);
+            op.vo[e] = c < r2 ? op.v2[i + (long long)c * op.ldv2]
+                              : op.v1[i + (long long)(c - r2) * op.ldv1];
+        }
+        return;
+    }
+
+    const bool ortho = op.kind == ROUND_ORTHO;
+    const bool dense = op.kind == ROUND_DENSE;
+    const int k = dense ? n : op.r1 + (op.kind == ROUND_GENERAL ? op.r2 : 0);
+    const int rout = op.rout;
+    if (m == 0 || n == 0) return;
+    double* w = op.work;
+    double* Ucat = w;
+    if (!ortho) w += (long long)m * k;
+    double* Vcat = w;
+    if (!dense) w += (long long)n * k;
+    double* tauU = w;
+    w += k;
+    double* tauV = w;
+    w += k;
+    const int ku = ortho ? op.r1 : min(m, k);
+    const int kv = dense ? n : min(n, k);
+    double* M;
+    double* J;
+    if (smem_mj) {
+        M = dyn;
+        J = dyn + (long long)kSmemK * kSmemK;
+    } else {
+        M = w;
+        J = w + (long long)ku * kv;
+    }
+
+    // ---- stacked factors ---------------------------------------------------
+    if (op.kind == ROUND_GENERAL) {
+        const int r1 = op.r1;
+        for (long long e = tid; e < (long long)m * k; e += kT) {
+            int i = (int)(e % m), c = (int)(e / m);
+            Ucat[e] = c < r1 ? op.alpha * op.u1[i + (long long)c * op.ldu1]
+                             : op.beta * op.u2[i + (long long)(c - r1) * op.ldu2];
+        }
+        for (long long e = tid; e < (long long)n * k; e += kT) {
+            int i = (int)(e % n), c = (int)(e / n);
+            Vcat[e] = c < r1 ? op.v1[i + (long long)c * op.ldv1]
+                             : op.v2[i + (long long)(c - r1) * op.ldv2];
+        }
+    } else if (dense) {
+        for (long long e = tid; e < (long long)m * n; e += kT) {
+            int i = (int)(e % m), c = (int)(e / m);
+            double v = op.alpha * op.u1[i + (long long)c * op.ldu1];
+            if (op.beta != 0.0)
+                for (int l = 0; l < op.r2; ++l)
+                    v = fma(op.beta * op.u2[i + (long long)l * op.ldu2],
+                            op.v2[c + (long long)l * op.ldv2], v);
+            Ucat[e] = v;
+        }
+    } else {  // ortho: Q1 is used in place; Z is copied
+        for (long long e = tid; e < (long long)n * k; e += kT) {
+            int i = (int)(e % n), c = (int)(e / n);
+            Vcat[e] = op.v1[i + (long long)c * op.ldv1];
+        }
+    }
+    __syncthreads();
+
+    // ---- QR of the stacks ------------------------------------------------
+    if (!ortho) cta_qr(Ucat, m, k, m, tauU, red);
+    if (!dense) cta_qr(Vcat, n, k, n, tauV, red);
+
+    // ---- core M = R_u R_v^T (ku x kv) -------------------------------------
+    for (int e = tid; e < ku * kv; e += kT) {
+        const int i = e % ku, l = e / ku;
+        double v = 0.0;
+        if (ortho) {
+            v = (i >= l) ? Vcat[l + (long long)i * n] : 0.0;      // R_v^T
+        } else if (dense) {
+            v = (l >= i) ? Ucat[i + (long long)l * m] : 0.0;      // R_u (ku x n)
+        } else {
+            for (int p = max(i, l); p < k; ++p)
+                v = fma(Ucat[i + (long long)p * m], Vcat[l + (long long)p * n], v);
+        }
+        M[i + (long long)l * ku] = v;
+    }
+    __syncthreads();
+
+    // ---- SVD of the core ---------------------------------------------------
+    cta_jacobi(M, ku, kv, J, &flag);
+    cta_order_columns(M, ku, kv, norms, order);
+
+    // ---- outputs -------------------------------------------------------------
+    if (ortho) {
+        for (long long e = tid; e < (long long)m * rout; e += kT) {
+            int i = (int)(e % m), c = (int)(e / m);
+            const double* g = M + (long long)order[c] * ku;
+            double v = 0.0;
+            for (int p = 0; p < ku; ++p) v = fma(op.u1[i + (long long)p * op.ldu1], g[p], v);
+            op.uo[e] = v;
+        }
+    } else {
+        for (long long e = tid; e < (long long)m * rout; e += kT) {
+            int i = (int)(e % m), c = (int)(e / m);
+            op.uo[e] = i < ku ? M[i + (long long)order[c] * ku] : 0.0;
+        }
+    }
+    for (long long e = tid; e < (long long)n * rout; e += kT) {
+        int i = (int)(e % n), c = (int)(e / n);
+        op.vo[e] = i < kv ? J[i + (long long)order[c] * kv] : 0.0;
+    }
+    __syncthreads();
+    if (!ortho) cta_apply_q(Ucat, m, min(m, k), m, tauU, op.uo, rout, m);
+    if (!dense) cta_apply_q(Vcat, n, min(n, k), n, tauV, op.vo, rout, n);
+}
+
+__global__ void __launch_bounds__(kT) qr_formq_kernel(const QrOp* __restrict__ ops) {
+    __shared__ double red[kW + 1];
+    const QrOp op = ops[blockIdx.x];
+    const int kq = min(op.m, op.k);
+    if (op.m == 0 || kq == 0) return;
+    cta_qr(op.Y, op.m, op.k, op.ldy, op.tau, red);
+    for (long long e = threadIdx.x; e < (long long)op.m * kq; e += kT) {
+        int i = (int)(e % op.m), c = (int)(e / op.m);
+        op.Q[e] = (i == c) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    cta_apply_q(op.Y, op.m, kq, op.ldy, op.tau, op.Q, kq, op.m);
+}
+
+}  // namespace
+
+long long round_work_size(const RoundOp& op) {
+    if (op.kind == ROUND_SET || op.kind == ROUND_CONCAT) return 0;
+    const bool ortho = op.kind == ROUND_ORTHO, dense = op.kind == ROUND_DENSE;
+    const long long k = dense ? op.n : op.r1 + (op.kind == ROUND_GENERAL ? op.r2 : 0);
+    long long w = 0;
+    if (!ortho) w += (long long)op.m * k;
+    if (!dense) w += (long long)op.n * k;
+    w += 2 * k;
+    const long long ku = ortho ? op.r1 : std::min<long long>(op.m, k);
+    const long long kv = dense ? op.n : std::min<long long>(op.n, k);
+    w += ku * kv + kv * kv;   // M, J when they do not fit in shared memory
+    return (w + 1) & ~1LL;
+}
+
+void launch_round_ops(Context& ctx, std::vector<RoundOp>& ops, const char* name) {
+    if (ops.empty()) return;
+    int kmax = 0;
+    for (const RoundOp& op : ops) {
+        int k = op.kind == ROUND_DENSE ? op.n : op.r1 + (op.kind == ROUND_GENERAL ? op.r2 : 0);
+        HMB_REQUIRE(k <= kMaxK, HM_ERR_UNSUPPORTED,
+                    "low-rank rounding of more than 128 stacked columns");
+        kmax = std::max(kmax, k);
+    }
+    const int smem_mj = kmax <= kSmemK ? 1 : 0;
+    const size_t smem = smem_mj ? 2 * kSmemK * kSmemK * sizeof(double) : 0;
+    static bool attr_set = false;
+    if (!attr_set) {
+        HMB_CUDA(cudaFuncSetAttribute(round_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(2 * kSmemK * kSmemK * sizeof(double))));
+        attr_set = true;
+    }
+    DeviceBuffer<RoundOp> d;
+    d.upload(ops, ctx.stream);
+    LaunchScope ls(ctx, name);
+    round_kernel<<<(unsigned)ops.size(), kT, smem, ctx.stream>>>(d.get(), smem_mj);
+    HMB_CHECK_LAUNCH();
+}
+
+void launch_qr_formq(Context& ctx, const std::vector<QrOp>& ops, const char* name) {
+    if (ops.empty()) return;
+    DeviceBuffer<QrOp> d;
+    d.upload(ops, ctx.stream);
+    LaunchScope ls(ctx, name);
+    qr_formq_kernel<<<(unsigned)ops.size(), kT, 0, ctx.stream>>>(d.get());
+    HMB_CHECK_LAUNCH();
+}
+
+}  // namespace hmb

@@ -1,0 +1,46 @@
+// Batched low-rank rounding on the device (see lowrank.cu).
+#pragma once
+#include <vector>
+
+#include "engine.h"
+
+namespace hmb {
+
+enum RoundKind : int {
+    ROUND_SET = 0,      // out = (alpha U1, V1)
+    ROUND_CONCAT = 1,   // out = ([beta U2, alpha U1], [V2, V1])      (exact)
+    ROUND_GENERAL = 2,  // out = best rank-rout of alpha U1 V1^T + beta U2 V2^T
+    ROUND_DENSE = 3,    // out = best rank-rout of alpha D1 + beta U2 V2^T
+    ROUND_ORTHO = 4,    // out = best rank-rout of Q1 V1^T, Q1 orthonormal
+};
+
+struct RoundOp {
+    const double* u1;   // U1 (m x r1) / D1 (m x n) / Q1 (m x r1)
+    const double* v1;   // V1 (n x r1)
+    const double* u2;   // U2 (m x r2)
+    const double* v2;   // V2 (n x r2)
+    double* uo;         // m x rout, ld m
+    double* vo;         // n x rout, ld n
+    double* work;       // scratch, round_work_size() doubles
+    double alpha, beta;
+    int kind, m, n, r1, r2, rout;
+    int ldu1, ldv1, ldu2, ldv2;
+};
+
+// Scratch doubles one op needs (0 for SET / CONCAT).
+long long round_work_size(const RoundOp& op);
+
+// Launches one CTA per op.  Ops must write disjoint outputs.
+void launch_round_ops(Context& ctx, std::vector<RoundOp>& ops, const char* name);
+
+// Orthonormal basis of the columns of Y (m x k, overwritten), written to Q
+// (m x min(m,k)): Householder QR, then Q = H_1 ... H_kk [I; 0].
+struct QrOp {
+    double* Y;
+    double* Q;
+    double* tau;   // min(m,k) doubles of scratch
+    int m, k, ldy, pad;
+};
+void launch_qr_formq(Context& ctx, const std::vector<QrOp>& ops, const char* name);
+
+}  // namespace hmb

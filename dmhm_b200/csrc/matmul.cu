@@ -229,7 +229,8 @@ p2_narrow_kernel(const P2Item* __restrict__ items, const P2Entry* __restrict__ e
 #pragma unroll
         for (int w = 0; w < kWarps; ++w) v += red[w][i][c];
         double* y = J.out + it.out_off + (it.r0 + i) + (long long)(it.c0 + c) * J.ldout;
-        *y = J.beta == 0.0 ? J.alpha * v : J.alpha * v + J.beta * *y;
+        const double al = J.alpha_scale ? J.alpha * *J.alpha_scale : J.alpha;
+        *y = J.beta == 0.0 ? al * v : al * v + J.beta * *y;
     }
 }
 
@@ -295,7 +296,8 @@ p2_wide_kernel(const P2Item* __restrict__ items, const P2Entry* __restrict__ ent
             int c = tc + b;
             if (c >= it.cols) continue;
             double* y = J.out + it.out_off + (it.r0 + i) + (long long)(it.c0 + c) * J.ldout;
-            *y = J.beta == 0.0 ? J.alpha * acc[a][b] : J.alpha * acc[a][b] + J.beta * *y;
+            const double al = J.alpha_scale ? J.alpha * *J.alpha_scale : J.alpha;
+            *y = J.beta == 0.0 ? al * acc[a][b] : al * acc[a][b] + J.beta * *y;
         }
     }
 }
@@ -509,7 +511,7 @@ void run_jobs(Context& ctx, const std::vector<MatJob>& jobs) {
     std::vector<JobArgs> args;
     for (const MatJob& J : jobs) {
         specs.push_back({J.H, J.root, J.trans, J.k});
-        args.push_back({J.in, J.out, J.alpha, J.beta, J.ldin, J.ldout, J.k, 0});
+        args.push_back({J.in, J.out, J.alpha, J.beta, J.ldin, J.ldout, J.k, 0, nullptr});
     }
     PlanPtr plan = build_plan(ctx, specs);
     execute_plan(ctx, *plan, args);

@@ -1,0 +1,317 @@
+// Schulz inversion, two-norm estimation and the elementwise H-matrix
+// operations they use (CopyFrom, AdjointFrom, Scale, AddConstantToDiagonal).
+//
+// SchulzInvert (src/HMat2d/Invert-incl.hpp:127-196; 3-D
+// src/HMat3d/Invert-incl.hpp:127-186):
+//   X_0 = (2 / est^2) A^T with est = EstimateTwoNorm(A) (already >= ||A||),
+//   X_{k+1} = (2I - X_k A) X_k,
+// with the optional stop test on an estimate of ||I - X_k A||_2.
+// EstimateTwoNorm (include/dmhm/hmat_tools.hpp:1504-1548): k normalised
+// power steps from a Gaussian start vector, est = theta * prod ||A x_i||^(1/k).
+// Every step runs on the device; the host reads back one scalar per estimate.
+#include "schulz.h"
+
+#include <cmath>
+
+#include "dense_ops.h"
+#include "hh.h"
+#include "rng.cuh"
+
+namespace hmb {
+
+namespace {
+
+constexpr int kT = 256;
+
+struct CopyTask {
+    const double* src;
+    double* dst;
+    double alpha;
+    int m, n, lds, transpose;   // dst (m x n, ld m) = alpha * (transpose ? src^T : src)
+};
+
+__global__ void copy_tasks_kernel(const CopyTask* __restrict__ tasks) {
+    const CopyTask t = tasks[blockIdx.x];
+    const long long total = (long long)t.m * t.n;
+    for (long long e = threadIdx.x; e < total; e += kT) {
+        int i = (int)(e % t.m), j = (int)(e / t.m);
+        double v = t.transpose ? t.src[j + (long long)i * t.lds] : t.src[i + (long long)j * t.lds];
+        t.dst[e] = t.alpha * v;
+    }
+}
+
+void launch_copy_tasks(Context& ctx, const std::vector<CopyTask>& tasks, const char* name) {
+    std::vector<CopyTask> live;
+    for (const CopyTask& t : tasks)
+        if (t.m > 0 && t.n > 0) live.push_back(t);
+    if (live.empty()) return;
+    DeviceBuffer<CopyTask> d;
+    d.upload(live, ctx.stream);
+    LaunchScope ls(ctx, name);
+    copy_tasks_kernel<<<(unsigned)live.size(), kT, 0, ctx.stream>>>(d.get());
+    HMB_CHECK_LAUNCH();
+}
+
+struct DiagTask {
+    double* D;
+    int m, n;
+};
+
+__global__ void add_diag_kernel(const DiagTask* __restrict__ tasks, int ntasks, double alpha) {
+    const int t = blockIdx.x;
+    if (t >= ntasks) return;
+    const DiagTask d = tasks[t];
+    const int k = min(d.m, d.n);
+    for (int j = threadIdx.x; j < k; j += kT) d.D[j + (long long)j * d.m] += alpha;
+}
+
+// Gaussian vector (SerialGaussianRandomVector, random.hpp:344-364):
+// pairs at rows (2i, 2i+1), the last pair (or single) at (n-2, n-1) / n-1.
+__global__ void gaussian_vector_kernel(double* x, int n, unsigned long long base) {
+    const int pairs = (n + 1) / 2;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < pairs; p += gridDim.x * blockDim.x) {
+        double a, b;
+        box_muller(lcg_skip(base, 2ULL * p), a, b);
+        if (p < pairs - 1) {
+            x[2 * p] = a;
+            x[2 * p + 1] = b;
+        } else if (n & 1) {
+            x[n - 1] = a;
+        } else {
+            x[n - 2] = a;
+            x[n - 1] = b;
+        }
+    }
+}
+
+// Sum of squares, deterministic two-stage reduction.
+constexpr int kNormBlocks = 148;
+
+__global__ void sumsq_partial_kernel(const double* __restrict__ x, int n, double* partial) {
+    __shared__ double red[kT / 32];
+    double s = 0.0;
+    for (int i = blockIdx.x * kT + threadIdx.x; i < n; i += gridDim.x * kT) s = fma(x[i], x[i], s);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kT / 32; ++w) t += red[w];
+        partial[blockIdx.x] = t;
+    }
+}
+
+// nrm = sqrt(sum partial); inv = 1/nrm; est *= nrm^root  (root < 0: start,
+// est := theta unchanged and only inv is produced).
+__global__ void norm_finalize_kernel(const double* partial, int np, double* inv, double* est,
+                                     double root) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double s = 0.0;
+    for (int i = 0; i < np; ++i) s += partial[i];
+    const double nrm = sqrt(s);
+    *inv = 1.0 / nrm;
+    if (root > 0.0) *est *= pow(nrm, root);
+}
+
+__global__ void scale_vector_kernel(double* x, int n, const double* inv) {
+    const double a = *inv;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        x[i] *= a;
+}
+
+__global__ void set_scalar_kernel(double* p, double v) { *p = v; }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Elementwise H-matrix operations
+// ---------------------------------------------------------------------------
+void hmat_copy(Context& ctx, const HMatrix& src, HMatrix& dst) {
+    HMB_REQUIRE(&src != &dst, HM_ERR_ARGUMENT, "copy onto itself");
+    dst.ctx = &ctx;
+    dst.S = src.S;
+    dst.max_rank = src.max_rank;
+    dst.rank = src.rank;
+    dst.layout();
+    if (src.total > 0)
+        HMB_CUDA(cudaMemcpyAsync(dst.data.get(), src.data.get(), src.total * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, ctx.stream));
+}
+
+void hmat_transpose(Context& ctx, const HMatrix& src, HMatrix& dst) {
+    HMB_REQUIRE(&src != &dst, HM_ERR_ARGUMENT, "transpose onto itself");
+    const Structure& S = *src.S;
+    dst.ctx = &ctx;
+    dst.S = src.S;
+    dst.max_rank = src.max_rank;
+    dst.rank.assign(S.blocks.size(), 0);
+    for (size_t b = 0; b < S.blocks.size(); ++b)
+        if (S.blocks[b].kind == KIND_LOWRANK) dst.rank[b] = src.rank[S.blocks[b].transpose];
+    dst.layout();
+    std::vector<CopyTask> tasks;
+    for (int b : S.leaves) {
+        const Block& B = S.blocks[b];
+        const int bt = B.transpose;
+        if (B.kind == KIND_LOWRANK) {
+            const int r = dst.rank[b];
+            // (U V^T)^T = V U^T: new U = old V (m x r), new V = old U (n x r)
+            tasks.push_back({src.V(bt), dst.U(b), 1.0, B.m, r, B.m, 0});
+            tasks.push_back({src.U(bt), dst.V(b), 1.0, B.n, r, B.n, 0});
+        } else {
+            tasks.push_back({src.D(bt), dst.D(b), 1.0, B.m, B.n, S.blocks[bt].m, 1});
+        }
+    }
+    launch_copy_tasks(ctx, tasks, "transpose_blocks");
+}
+
+void hmat_scale(Context& ctx, HMatrix& H, double alpha) {
+    const Structure& S = *H.S;
+    if (alpha == 0.0) {
+        // Scale(0, LowRank) drops the rank (hmat_tools.hpp, Scale); dense -> 0
+        bool any = false;
+        for (int b : S.leaves)
+            if (S.blocks[b].kind == KIND_LOWRANK && H.rank[b] != 0) { H.rank[b] = 0; any = true; }
+        if (any) H.layout();
+        if (H.total > 0)
+            HMB_CUDA(cudaMemsetAsync(H.data.get(), 0, H.total * sizeof(double), ctx.stream));
+        return;
+    }
+    if (alpha == 1.0) return;
+    std::vector<CopyTask> tasks;
+    for (int b : S.leaves) {
+        const Block& B = S.blocks[b];
+        if (B.kind == KIND_LOWRANK)
+            tasks.push_back({H.U(b), H.U(b), alpha, B.m, H.rank[b], B.m, 0});
+        else
+            tasks.push_back({H.D(b), H.D(b), alpha, B.m, B.n, B.m, 0});
+    }
+    launch_copy_tasks(ctx, tasks, "scale_blocks");
+}
+
+void hmat_add_diagonal(Context& ctx, HMatrix& H, double alpha) {
+    const Structure& S = *H.S;
+    std::vector<DiagTask> tasks;
+    for (int b : S.leaves) {
+        const Block& B = S.blocks[b];
+        if (B.kind == KIND_DENSE && B.tgt_box == B.src_box) tasks.push_back({H.D(b), B.m, B.n});
+    }
+    if (tasks.empty()) return;
+    DeviceBuffer<DiagTask> d;
+    d.upload(tasks, ctx.stream);
+    LaunchScope ls(ctx, "add_diagonal");
+    add_diag_kernel<<<(unsigned)tasks.size(), kT, 0, ctx.stream>>>(d.get(), (int)tasks.size(),
+                                                                   alpha);
+    HMB_CHECK_LAUNCH();
+}
+
+// ---------------------------------------------------------------------------
+// EstimateTwoNorm
+// ---------------------------------------------------------------------------
+double estimate_two_norm(Context& ctx, HMatrix& A, double theta, double confidence) {
+    HMB_REQUIRE(theta > 1.0, HM_ERR_ARGUMENT, "theta must be > 1");
+    HMB_REQUIRE(confidence > 0.0, HM_ERR_ARGUMENT, "confidence must be positive");
+    const int n = A.height();
+    const int k = (int)std::ceil(std::log(0.8 * std::sqrt((double)n) * std::pow(10.0, confidence)) /
+                                 std::log(theta));
+    cudaStream_t st = ctx.stream;
+    DeviceBuffer<double> x, y, partial, scal;
+    x.allocate(n, st);
+    y.allocate(n, st);
+    partial.allocate(kNormBlocks, st);
+    scal.allocate(2, st);   // [0] = 1/||.||, [1] = estimate
+    {
+        LaunchScope ls(ctx, "norm_start_vector");
+        gaussian_vector_kernel<<<ceil_div((n + 1) / 2, kT), kT, 0, st>>>(x.get(), n,
+                                                                        ctx.serial_state);
+        HMB_CHECK_LAUNCH();
+    }
+    ctx.serial_state = lcg_skip_host(ctx.serial_state, 2ULL * (uint64_t)((n + 1) / 2));
+    {
+        LaunchScope ls(ctx, "norm_reduce");
+        set_scalar_kernel<<<1, 1, 0, st>>>(scal.get() + 1, theta);
+        sumsq_partial_kernel<<<kNormBlocks, kT, 0, st>>>(x.get(), n, partial.get());
+        norm_finalize_kernel<<<1, 32, 0, st>>>(partial.get(), kNormBlocks, scal.get(),
+                                               scal.get() + 1, -1.0);
+        HMB_CHECK_LAUNCH();
+    }
+    // x currently unnormalised; its scale is folded into the first product
+    // through alpha_scale = 1/||x||.
+    const double root = 1.0 / (double)k;
+    auto key = std::make_pair(0, 1);
+    auto it = A.plans.find(key);
+    if (it == A.plans.end()) {
+        PlanPtr p = build_plan(ctx, {JobSpec{&A, 0, false, 1}});
+        it = A.plans.emplace(key, std::shared_ptr<MatPlan>(p.release(), MatPlanDeleter())).first;
+    }
+    double* cur = x.get();
+    double* nxt = y.get();
+    for (int i = 0; i < k; ++i) {
+        JobArgs ja{cur, nxt, 1.0, 0.0, n, n, 1, 0, scal.get()};
+        execute_plan(ctx, *it->second, {ja});
+        LaunchScope ls(ctx, "norm_reduce");
+        sumsq_partial_kernel<<<kNormBlocks, kT, 0, st>>>(nxt, n, partial.get());
+        norm_finalize_kernel<<<1, 32, 0, st>>>(partial.get(), kNormBlocks, scal.get(),
+                                               scal.get() + 1, root);
+        HMB_CHECK_LAUNCH();
+        std::swap(cur, nxt);
+    }
+    double est = 0.0;
+    HMB_CUDA(cudaMemcpyAsync(&est, scal.get() + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+    HMB_CUDA(cudaStreamSynchronize(st));
+    return est;
+}
+
+// ---------------------------------------------------------------------------
+// SchulzInvert
+// ---------------------------------------------------------------------------
+SchulzResult schulz_invert(Context& ctx, HMatrix& A, int num_iterations, double theta,
+                           double confidence, double stop_tol) {
+    SchulzResult res;
+    bool stop = false;
+    if (num_iterations <= 0) {
+        num_iterations = 30;
+        stop = true;
+    }
+    const double est = estimate_two_norm(ctx, A, theta, confidence);
+    res.trace.push_back(est);
+    const double alpha = 2.0 / (est * est);
+    auto X = std::make_unique<HMatrix>();
+    hmat_transpose(ctx, A, *X);
+    hmat_scale(ctx, *X, alpha);
+    int k = 0;
+    for (; k < num_iterations; ++k) {
+        HMatrix Z;
+        hh_multiply(ctx, *X, A, -1.0, 0.0, Z, true);
+        if (stop) {
+            hmat_add_diagonal(ctx, Z, 1.0);
+            const double ez = estimate_two_norm(ctx, Z, theta, confidence);
+            res.trace.push_back(ez);
+            if (std::fabs(ez) < stop_tol) {
+                hmat_add_diagonal(ctx, Z, 1.0);
+                auto Xn = std::make_unique<HMatrix>();
+                hh_multiply(ctx, Z, *X, 1.0, 0.0, *Xn, true);
+                X = std::move(Xn);
+                ++k;
+                break;
+            }
+            hmat_add_diagonal(ctx, Z, 1.0);
+        } else {
+            hmat_add_diagonal(ctx, Z, 2.0);
+        }
+        auto Xn = std::make_unique<HMatrix>();
+        hh_multiply(ctx, Z, *X, 1.0, 0.0, *Xn, true);
+        X = std::move(Xn);
+    }
+    res.iterations = k;
+    // A := X (CopyFrom, Invert-incl.hpp:195): take over X's storage
+    A.rank = X->rank;
+    A.max_rank = X->max_rank;
+    A.off = X->off;
+    A.total = X->total;
+    A.data = std::move(X->data);
+    A.table = std::move(X->table);
+    A.plans.clear();
+    return res;
+}
+
+}  // namespace hmb

@@ -1,0 +1,18 @@
+// Schulz inversion and two-norm estimation (see schulz.cu).
+#pragma once
+#include <vector>
+
+#include "engine.h"
+
+namespace hmb {
+
+struct SchulzResult {
+    int iterations = 0;
+    std::vector<double> trace;   // [est ||A||, est ||I - X_k A|| per stop check]
+};
+
+double estimate_two_norm(Context& ctx, HMatrix& A, double theta, double confidence);
+SchulzResult schulz_invert(Context& ctx, HMatrix& A, int num_iterations, double theta,
+                           double confidence, double stop_tol);
+
+}  // namespace hmb

@@ -147,7 +147,7 @@ class _HMatBase:
             self._h = _handle
             return
         if S is None:
-            raise ValueError("an H-matrix is constructed from a Sparse matrix")
+            return       # empty H-matrix (HMat2d(), hmat2d.hpp:40), filled by CopyFrom etc.
         if len(sizes) != self.dim:
             raise ValueError(f"expected {self.dim} grid sizes")
         if S.symmetric:
@@ -280,8 +280,76 @@ class _HMatBase:
         """AdjointMultiply: equal to TransposeMultiply for real scalars."""
         return self.TransposeMultiply(alpha, B, beta, C)
 
-    def _multiply_hmat(self, alpha, B, beta, C):
-        raise _lib.HMError(4, "H*H multiply not available in this build")
+    def _multiply_hmat(self, alpha, B, beta, Cm):
+        """H*H (MultiplyHMat-incl.hpp:12-380).  Without beta: C = alpha A B,
+        rebuilt (a new H-matrix unless C is given); with beta: C :~= alpha A B
+        + beta C in place on C's structure."""
+        if beta is None:
+            out = _handle_of(Cm)
+            check(lib().hm_multiply_hmat(self._h, float(alpha), B.handle, C.byref(out)))
+            if Cm is not None:
+                Cm._h = out
+                return Cm
+            return type(self)(ctx=self.ctx, _handle=out)
+        if Cm is None or not Cm.handle:
+            raise _lib.HMError(1, "C is required with beta")
+        check(lib().hm_multiply_hmat_update(self._h, float(alpha), B.handle, float(beta),
+                                            Cm.handle))
+        return Cm
+
+    # -- structural / elementwise (HMat2d.cpp:331-744) ---------------------
+    def CopyFrom(self, B: "_HMatBase"):
+        """A := B (CopyFrom, HMat2d.cpp:331-391)."""
+        out = _handle_of(self)
+        check(lib().hm_copy(B.handle, C.byref(out)))
+        self._h = out
+        return self
+
+    def AdjointFrom(self, B: "_HMatBase"):
+        """A := B^H (= B^T for real scalars; AdjointFrom, HMat2d.cpp:545-614)."""
+        out = _handle_of(self)
+        check(lib().hm_transpose(B.handle, C.byref(out)))
+        self._h = out
+        return self
+
+    TransposeFrom = AdjointFrom
+
+    def Scale(self, alpha: float):
+        """A := alpha A (HMat2d.cpp:616-647)."""
+        check(lib().hm_scale(self._h, float(alpha)))
+
+    def AddConstantToDiagonal(self, alpha: float):
+        """A := A + alpha I (HMat2d.cpp:704-744)."""
+        check(lib().hm_add_constant_to_diagonal(self._h, float(alpha)))
+
+    def SchulzInvert(self, numIterations: int, theta: float = 1.5, confidence: float = 6.0,
+                     stopTol: float = 1e-4):
+        """A :~= inv(A) by Schulz iteration (src/HMat2d/Invert-incl.hpp:127-196).
+
+        Returns (iterations run, [estimate of ||A||, estimates of
+        ||I - X_k A|| at each stop check])."""
+        its = C.c_int()
+        cap = 64
+        trace = (C.c_double * cap)()
+        n = C.c_int()
+        check(lib().hm_schulz_invert(self._h, int(numIterations), float(theta),
+                                     float(confidence), float(stopTol), C.byref(its), trace,
+                                     cap, C.byref(n)))
+        return its.value, [trace[i] for i in range(min(n.value, cap))]
+
+
+def _handle_of(obj) -> C.c_void_p:
+    """A fresh c_void_p holding obj's handle (NULL for None or an empty object)."""
+    if obj is None or not obj.handle:
+        return C.c_void_p(None)
+    return C.c_void_p(obj.handle.value)
+
+
+def EstimateTwoNorm(A: _HMatBase, theta: float, confidence: float) -> float:
+    """hmat_tools::EstimateTwoNorm (include/dmhm/hmat_tools.hpp:1504-1548)."""
+    v = C.c_double()
+    check(lib().hm_estimate_two_norm(A.handle, float(theta), float(confidence), C.byref(v)))
+    return v.value
 
 
 class HMat2d(_HMatBase):

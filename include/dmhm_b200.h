@@ -108,6 +108,47 @@ HM_API int hm_multiply_dense_host(hm_matrix h, int transpose, double alpha,
                            const double* B, int ldb, double beta, double* C,
                            int ldc, int nrhs);
 
+/*
+ * H*H products with randomized low-rank compression.
+ * hm_multiply_hmat: C := alpha A B, C rebuilt (HMat2d::Multiply(alpha,
+ * const HMat2d& B, HMat2d& C), include/dmhm/hmat2d.hpp:260-263;
+ * src/HMat2d/MultiplyHMat-incl.hpp:12-187).  *C == NULL creates a new
+ * handle; otherwise its previous contents are replaced.
+ * hm_multiply_hmat_update: C :~= alpha A B + beta C on C's existing structure
+ * (hmat2d.hpp:265-268; MultiplyHMat-incl.hpp:189-380).
+ * Sampled products draw their Gaussian test matrices from the context's
+ * serial generator in the reference's recursion order; Oversample() extra
+ * samples (SampleRank, hmat2d.hpp:32-33).  C must differ from A and B.
+ */
+HM_API int hm_multiply_hmat(hm_matrix A, double alpha, hm_matrix B, hm_matrix* C);
+HM_API int hm_multiply_hmat_update(hm_matrix A, double alpha, hm_matrix B, double beta,
+                                   hm_matrix C);
+
+/* hmat_tools::EstimateTwoNorm (include/dmhm/hmat_tools.hpp:1504-1548). */
+HM_API int hm_estimate_two_norm(hm_matrix h, double theta, double confidence,
+                                double* estimate);
+
+/*
+ * SchulzInvert(numIterations, theta, confidence, stopTol)
+ * (include/dmhm/hmat2d.hpp:275-276, src/HMat2d/Invert-incl.hpp:127-196;
+ * HMat3d: pass stop_tol = 1e-4, src/HMat3d/Invert-incl.hpp:168).
+ * numIterations <= 0 runs up to 30 iterations with the stop test.  h is
+ * replaced by the approximate inverse.  Optional outputs: iterations run and
+ * the estimates [||A||, ||I - X_k A|| per stop check] (up to trace_cap).
+ */
+HM_API int hm_schulz_invert(hm_matrix h, int num_iterations, double theta,
+                            double confidence, double stop_tol, int* iterations,
+                            double* trace, int trace_cap, int* trace_len);
+
+/* CopyFrom (src/HMat2d/HMat2d.cpp:331-391); AdjointFrom / TransposeFrom for
+   real scalars (HMat2d.cpp:479-614); *dst == NULL creates a new handle. */
+HM_API int hm_copy(hm_matrix src, hm_matrix* dst);
+HM_API int hm_transpose(hm_matrix src, hm_matrix* dst);
+/* Scale (HMat2d.cpp:616-647; alpha = 0 drops every low-rank block to rank 0)
+   and AddConstantToDiagonal (HMat2d.cpp:704-744). */
+HM_API int hm_scale(hm_matrix h, double alpha);
+HM_API int hm_add_constant_to_diagonal(hm_matrix h, double alpha);
+
 /* Diagnostics (no reference counterpart): number of kernels this library has
    launched so far in the process, and per-kernel CUDA-event timing on the
    context stream.  hm_profile_enable resets the totals; hm_profile_read

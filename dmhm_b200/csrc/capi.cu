@@ -2,6 +2,7 @@
 // side of each entry point.
 #include <algorithm>
 #include <cstring>
+#include <set>
 #include <string>
 
 #include "engine.h"
@@ -9,13 +10,50 @@
 #include "rng.cuh"
 #include "schulz.h"
 
+struct hm_matrix_s;
+
 struct hm_context_s {
     hmb::Context c;
+    std::set<hm_matrix_s*> live;   // handles created on this context
 };
 
 struct hm_matrix_s {
     hmb::HMatrix h;
+    hm_context_s* owner = nullptr;
 };
+
+namespace {
+
+hm_matrix_s* new_handle(hm_context_s* ctx) {
+    auto* m = new hm_matrix_s;
+    m->owner = ctx;
+    m->h.ctx = &ctx->c;
+    ctx->live.insert(m);
+    return m;
+}
+
+// Releases the device storage of a handle (stream-ordered frees).
+void release_storage(hm_matrix_s* m) {
+    m->h.plans.clear();
+    m->h.data.reset();
+    m->h.table.reset();
+}
+
+void delete_handle(hm_matrix_s* m) {
+    if (m->owner) {
+        m->owner->live.erase(m);
+        release_storage(m);
+    }
+    delete m;
+}
+
+hm_context_s* owner_of(hm_matrix_s* m) {
+    HMB_REQUIRE(m->owner != nullptr, HM_ERR_ARGUMENT,
+                "the H-matrix's context was destroyed");
+    return m->owner;
+}
+
+}  // namespace
 
 namespace hmb {
 
@@ -179,6 +217,15 @@ int hm_context_create(int device, void* cuda_stream, hm_context* out) {
 int hm_context_destroy(hm_context ctx) {
     return guarded([&] {
         if (!ctx) return;
+        // H-matrices still alive lose their device storage and become
+        // unusable (every later call on them reports HM_ERR_ARGUMENT).
+        for (hm_matrix_s* m : ctx->live) {
+            release_storage(m);
+            m->owner = nullptr;
+            m->h.ctx = nullptr;
+        }
+        ctx->live.clear();
+        ctx->c.collect();
         cudaStreamSynchronize(ctx->c.stream);
         if (ctx->c.own_stream) cudaStreamDestroy(ctx->c.stream);
         delete ctx;
@@ -239,9 +286,8 @@ int hm_create_from_csr(hm_context ctx, int dim, const int* sizes, int num_levels
         HMB_REQUIRE(max_rank >= 0, HM_ERR_ARGUMENT, "max_rank must be >= 0");
         *out = nullptr;
         HMB_CUDA(cudaSetDevice(ctx->c.device));
-        auto* m = new hm_matrix_s;
+        auto* m = new_handle(ctx);
         try {
-            m->h.ctx = &ctx->c;
             m->h.S = build_structure(dim, sizes, num_levels, strongly_admissible != 0);
             m->h.max_rank = max_rank;
             const int64_t nnz = row_offsets[m->h.S->N];
@@ -249,7 +295,7 @@ int hm_create_from_csr(hm_context ctx, int dim, const int* sizes, int num_levels
                         "NULL CSR arrays");
             import_csr(m->h, row_offsets, col_indices, values);
         } catch (...) {
-            delete m;
+            delete_handle(m);
             throw;
         }
         *out = m;
@@ -259,7 +305,7 @@ int hm_create_from_csr(hm_context ctx, int dim, const int* sizes, int num_levels
 int hm_destroy(hm_matrix h) {
     return guarded([&] {
         if (!h) return;
-        delete h;
+        delete_handle(h);
     });
 }
 
@@ -267,6 +313,8 @@ int hm_info(hm_matrix h, int* height, int* width, int* num_levels, int* max_rank
             int64_t* counts, int64_t* bytes) {
     return guarded([&] {
         HMB_REQUIRE(h, HM_ERR_ARGUMENT, "h is NULL");
+        owner_of(h);
+        HMB_REQUIRE(h->h.S != nullptr, HM_ERR_ARGUMENT, "empty H-matrix");
         const Structure& S = *h->h.S;
         if (height) *height = S.N;
         if (width) *width = S.N;
@@ -287,7 +335,7 @@ int hm_info(hm_matrix h, int* height, int* width, int* num_levels, int* max_rank
 int hm_set_to_random(hm_matrix h) {
     return guarded([&] {
         HMB_REQUIRE(h, HM_ERR_ARGUMENT, "h is NULL");
-        launch_fill_random(*h->h.ctx, h->h);
+        launch_fill_random(owner_of(h)->c, h->h);
     });
 }
 
@@ -295,6 +343,7 @@ int hm_multiply_dense(hm_matrix h, int transpose, double alpha, const double* B,
                       double beta, double* C, int ldc, int nrhs) {
     return guarded([&] {
         HMB_REQUIRE(h && (nrhs == 0 || (B && C)), HM_ERR_ARGUMENT, "NULL argument");
+        owner_of(h);
         multiply_dense(h->h, transpose, alpha, B, ldb, beta, C, ldc, nrhs);
     });
 }
@@ -303,7 +352,7 @@ int hm_multiply_dense_host(hm_matrix h, int transpose, double alpha, const doubl
                            double beta, double* C, int ldc, int nrhs) {
     return guarded([&] {
         HMB_REQUIRE(h && (nrhs == 0 || (B && C)), HM_ERR_ARGUMENT, "NULL argument");
-        Context& ctx = *h->h.ctx;
+        Context& ctx = owner_of(h)->c;
         const int m = transpose ? h->h.width() : h->h.height();
         const int n = transpose ? h->h.height() : h->h.width();
         HMB_REQUIRE(ldb >= std::max(1, n) && ldc >= std::max(1, m), HM_ERR_ARGUMENT,
@@ -328,19 +377,21 @@ int hm_multiply_dense_host(hm_matrix h, int transpose, double alpha, const doubl
 int hm_multiply_hmat(hm_matrix A, double alpha, hm_matrix B, hm_matrix* C) {
     return guarded([&] {
         HMB_REQUIRE(A && B && C, HM_ERR_ARGUMENT, "NULL argument");
-        HMB_REQUIRE(A->h.ctx == B->h.ctx, HM_ERR_ARGUMENT, "factors live in different contexts");
+        hm_context_s* ctx = owner_of(A);
+        HMB_REQUIRE(owner_of(B) == ctx, HM_ERR_ARGUMENT, "factors live in different contexts");
+        HMB_REQUIRE(*C != A && *C != B, HM_ERR_ARGUMENT,
+                    "the product must not overwrite a factor");
+        if (*C) HMB_REQUIRE(owner_of(*C) == ctx, HM_ERR_ARGUMENT, "C lives in another context");
         bool created = false;
         if (*C == nullptr) {
-            *C = new hm_matrix_s;
+            *C = new_handle(ctx);
             created = true;
         }
         try {
-            HMB_REQUIRE(*C != A && *C != B, HM_ERR_ARGUMENT,
-                        "the product must not overwrite a factor");
-            hh_multiply(*A->h.ctx, A->h, B->h, alpha, 0.0, (*C)->h, true);
+            hh_multiply(ctx->c, A->h, B->h, alpha, 0.0, (*C)->h, true);
         } catch (...) {
             if (created) {
-                delete *C;
+                delete_handle(*C);
                 *C = nullptr;
             }
             throw;
@@ -352,15 +403,18 @@ int hm_multiply_hmat_update(hm_matrix A, double alpha, hm_matrix B, double beta,
     return guarded([&] {
         HMB_REQUIRE(A && B && C, HM_ERR_ARGUMENT, "NULL argument");
         HMB_REQUIRE(C != A && C != B, HM_ERR_ARGUMENT, "the product must not overwrite a factor");
+        hm_context_s* ctx = owner_of(A);
+        HMB_REQUIRE(owner_of(B) == ctx && owner_of(C) == ctx, HM_ERR_ARGUMENT,
+                    "operands live in different contexts");
         HMB_REQUIRE(C->h.S != nullptr, HM_ERR_ARGUMENT, "C is empty");
-        hh_multiply(*A->h.ctx, A->h, B->h, alpha, beta, C->h, false);
+        hh_multiply(ctx->c, A->h, B->h, alpha, beta, C->h, false);
     });
 }
 
 int hm_estimate_two_norm(hm_matrix h, double theta, double confidence, double* estimate) {
     return guarded([&] {
         HMB_REQUIRE(h && estimate, HM_ERR_ARGUMENT, "NULL argument");
-        *estimate = estimate_two_norm(*h->h.ctx, h->h, theta, confidence);
+        *estimate = estimate_two_norm(owner_of(h)->c, h->h, theta, confidence);
     });
 }
 
@@ -373,7 +427,7 @@ int hm_schulz_invert(hm_matrix h, int num_iterations, double theta, double confi
                     "Cannot invert non-square matrices");
         HMB_REQUIRE(theta > 1.0, HM_ERR_ARGUMENT, "Theta must be > 1");
         HMB_REQUIRE(confidence > 0.0, HM_ERR_ARGUMENT, "Confidence must be positive");
-        SchulzResult r = schulz_invert(*h->h.ctx, h->h, num_iterations, theta, confidence,
+        SchulzResult r = schulz_invert(owner_of(h)->c, h->h, num_iterations, theta, confidence,
                                        stop_tol);
         if (iterations) *iterations = r.iterations;
         if (trace_len) *trace_len = (int)r.trace.size();
@@ -386,8 +440,10 @@ int hm_copy(hm_matrix src, hm_matrix* dst) {
     return guarded([&] {
         HMB_REQUIRE(src && dst, HM_ERR_ARGUMENT, "NULL argument");
         HMB_REQUIRE(*dst != src, HM_ERR_ARGUMENT, "copy onto itself");
-        if (*dst == nullptr) *dst = new hm_matrix_s;
-        hmat_copy(*src->h.ctx, src->h, (*dst)->h);
+        hm_context_s* ctx = owner_of(src);
+        if (*dst == nullptr) *dst = new_handle(ctx);
+        HMB_REQUIRE(owner_of(*dst) == ctx, HM_ERR_ARGUMENT, "dst lives in another context");
+        hmat_copy(ctx->c, src->h, (*dst)->h);
     });
 }
 
@@ -395,22 +451,24 @@ int hm_transpose(hm_matrix src, hm_matrix* dst) {
     return guarded([&] {
         HMB_REQUIRE(src && dst, HM_ERR_ARGUMENT, "NULL argument");
         HMB_REQUIRE(*dst != src, HM_ERR_ARGUMENT, "transpose onto itself");
-        if (*dst == nullptr) *dst = new hm_matrix_s;
-        hmat_transpose(*src->h.ctx, src->h, (*dst)->h);
+        hm_context_s* ctx = owner_of(src);
+        if (*dst == nullptr) *dst = new_handle(ctx);
+        HMB_REQUIRE(owner_of(*dst) == ctx, HM_ERR_ARGUMENT, "dst lives in another context");
+        hmat_transpose(ctx->c, src->h, (*dst)->h);
     });
 }
 
 int hm_scale(hm_matrix h, double alpha) {
     return guarded([&] {
         HMB_REQUIRE(h, HM_ERR_ARGUMENT, "h is NULL");
-        hmat_scale(*h->h.ctx, h->h, alpha);
+        hmat_scale(owner_of(h)->c, h->h, alpha);
     });
 }
 
 int hm_add_constant_to_diagonal(hm_matrix h, double alpha) {
     return guarded([&] {
         HMB_REQUIRE(h, HM_ERR_ARGUMENT, "h is NULL");
-        hmat_add_diagonal(*h->h.ctx, h->h, alpha);
+        hmat_add_diagonal(owner_of(h)->c, h->h, alpha);
     });
 }
 

@@ -255,14 +255,15 @@ struct Arena {
 
 void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha, double beta,
                  HMatrix& C, bool fresh) {
-    HMB_REQUIRE(A.S == B.S, HM_ERR_ARGUMENT,
+    HMB_REQUIRE(A.S && B.S && (A.S == B.S || same_structure(*A.S, *B.S)), HM_ERR_ARGUMENT,
                 "H*H multiply needs both factors on the same block structure");
     HMB_REQUIRE(&C != &A && &C != &B, HM_ERR_ARGUMENT,
                 "the product must not overwrite a factor");
     const Structure& S = *A.S;
     cudaStream_t st = ctx.stream;
     if (!fresh) {
-        HMB_REQUIRE(C.S == A.S, HM_ERR_ARGUMENT, "C must share the factors' block structure");
+        HMB_REQUIRE(C.S && (C.S == A.S || same_structure(*C.S, *A.S)), HM_ERR_ARGUMENT,
+                    "C must share the factors' block structure");
     }
     const int maxRankC = fresh ? A.max_rank : C.max_rank;
 

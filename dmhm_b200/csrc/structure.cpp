@@ -4,6 +4,8 @@
 #include <algorithm>
 #include <cstdlib>
 #include <functional>
+#include <map>
+#include <mutex>
 
 #include "common.h"
 
@@ -63,8 +65,32 @@ bool Structure::in_subtree(int b, int root) const {
     return b == root;
 }
 
+bool same_structure(const Structure& a, const Structure& b) {
+    return a.dim == b.dim && a.num_levels == b.num_levels && a.strong == b.strong &&
+           a.sizes[0] == b.sizes[0] && a.sizes[1] == b.sizes[1] && a.sizes[2] == b.sizes[2];
+}
+
 std::shared_ptr<Structure> build_structure(int dim, const int* sizes,
                                            int num_levels, bool strong) {
+    // H-matrices over the same grid share one structure object.
+    static std::mutex mu;
+    static std::map<std::vector<int>, std::weak_ptr<Structure>> cache;
+    std::vector<int> key{dim, num_levels, strong ? 1 : 0};
+    for (int k = 0; k < dim; ++k) key.push_back(sizes[k]);
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = cache.find(key);
+        if (it != cache.end())
+            if (auto sp = it->second.lock()) return sp;
+    }
+    auto S = build_structure_uncached(dim, sizes, num_levels, strong);
+    std::lock_guard<std::mutex> lock(mu);
+    cache[key] = S;
+    return S;
+}
+
+std::shared_ptr<Structure> build_structure_uncached(int dim, const int* sizes,
+                                                    int num_levels, bool strong) {
     HMB_REQUIRE(dim == 2 || dim == 3, HM_ERR_ARGUMENT, "dim must be 2 or 3");
     HMB_REQUIRE(num_levels >= 1 && num_levels <= 16, HM_ERR_ARGUMENT,
                 "num_levels must be in [1, 16]");

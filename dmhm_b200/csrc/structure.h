@@ -55,9 +55,13 @@ struct Structure {
     bool in_subtree(int b, int root) const;  // b == root or a descendant
 };
 
-// Builds the structure; throws hmb::Error on bad arguments.
+// Builds the structure (shared by all H-matrices over the same grid and
+// parameters); throws hmb::Error on bad arguments.
 std::shared_ptr<Structure> build_structure(int dim, const int* sizes,
                                            int num_levels, bool strong);
+std::shared_ptr<Structure> build_structure_uncached(int dim, const int* sizes,
+                                                    int num_levels, bool strong);
+bool same_structure(const Structure& a, const Structure& b);
 
 // map[natural] = hierarchical index (x fastest in the natural order).
 void natural_to_hierarchical(int dim, const int* sizes, int num_levels,

@@ -49,5 +49,7 @@ def test_stop_tested_run_matches_reference():
     ref_trace = fx["schulz_stop_trace"]
     assert n == int(fx["schulz_stop_iterations"])
     assert len(trace) == len(ref_trace)
-    np.testing.assert_allclose(trace, ref_trace, rtol=1e-5)
+    # estimates of ||I - X_k A|| are compared absolutely (they measure a
+    # deviation from the identity, whose norm is 1)
+    np.testing.assert_allclose(trace, ref_trace, rtol=1e-5, atol=1e-7)
     assert relerr(A.Multiply(1.0, fx["probes"]), fx["schulz_stop"]) < 1e-6

@@ -19,12 +19,9 @@ __device__ __forceinline__ double ld_op(const double* X, int ld, bool trans, int
     return trans ? X[j + (long long)i * ld] : X[i + (long long)j * ld];
 }
 
-// One CTA per (op, 64x64 output tile).  k < 0 means C = alpha A + beta C.
-__global__ void __launch_bounds__(kT)
-gemm_ops_kernel(const GemmOp* __restrict__ ops, const int* __restrict__ tile_op,
-                const int* __restrict__ tile_id) {
-    const GemmOp op = ops[tile_op[blockIdx.x]];
-    const int tile = tile_id[blockIdx.x];
+// One 64x64 output tile of one op, computed by the whole CTA.  k < 0 means
+// C = alpha A + beta C.
+__device__ void gemm_tile(const GemmOp& op, int tile, double (*sA)[65], double (*sB)[65]) {
     const int tiles_m = (op.m + 63) / 64;
     const int i0 = (tile % tiles_m) * 64, j0 = (tile / tiles_m) * 64;
     const int tid = threadIdx.x;
@@ -39,8 +36,6 @@ gemm_ops_kernel(const GemmOp* __restrict__ ops, const int* __restrict__ tile_op,
         }
         return;
     }
-    __shared__ double sA[16][65];
-    __shared__ double sB[16][65];
     const int tr = (tid & 15) * 4, tc = (tid >> 4) * 4;
     double acc[4][4];
 #pragma unroll
@@ -92,6 +87,31 @@ gemm_ops_kernel(const GemmOp* __restrict__ ops, const int* __restrict__ tile_op,
     }
 }
 
+// One CTA per (op, 64x64 output tile).
+__global__ void __launch_bounds__(kT)
+gemm_ops_kernel(const GemmOp* __restrict__ ops, const int* __restrict__ tile_op,
+                const int* __restrict__ tile_id) {
+    __shared__ double sA[16][65];
+    __shared__ double sB[16][65];
+    const GemmOp op = ops[tile_op[blockIdx.x]];
+    gemm_tile(op, tile_id[blockIdx.x], sA, sB);
+}
+
+// One CTA per worker: ops [begin[w], begin[w+1]) in order, all tiles of each.
+__global__ void __launch_bounds__(kT)
+gemm_worker_kernel(const GemmOp* __restrict__ ops, const int* __restrict__ begin) {
+    __shared__ double sA[16][65];
+    __shared__ double sB[16][65];
+    for (int i = begin[blockIdx.x]; i < begin[blockIdx.x + 1]; ++i) {
+        const GemmOp op = ops[i];
+        const int tiles = ((op.m + 63) / 64) * ((op.n + 63) / 64);
+        for (int t = 0; t < tiles; ++t) {
+            gemm_tile(op, t, sA, sB);
+            __syncthreads();
+        }
+    }
+}
+
 }  // namespace
 
 void launch_gemm_ops(Context& ctx, const std::vector<GemmOp>& ops, const char* name) {
@@ -114,6 +134,18 @@ void launch_gemm_ops(Context& ctx, const std::vector<GemmOp>& ops, const char* n
     LaunchScope ls(ctx, name);
     gemm_ops_kernel<<<(unsigned)tile_op.size(), kT, 0, ctx.stream>>>(d_ops.get(), d_to.get(),
                                                                      d_ti.get());
+    HMB_CHECK_LAUNCH();
+}
+
+void launch_gemm_workers(Context& ctx, const std::vector<GemmOp>& ops,
+                         const std::vector<int>& begin, const char* name) {
+    if (ops.empty() || begin.size() < 2) return;
+    DeviceBuffer<GemmOp> d_ops;
+    DeviceBuffer<int> d_b;
+    d_ops.upload(ops, ctx.stream);
+    d_b.upload(begin, ctx.stream);
+    LaunchScope ls(ctx, name);
+    gemm_worker_kernel<<<(unsigned)(begin.size() - 1), kT, 0, ctx.stream>>>(d_ops.get(), d_b.get());
     HMB_CHECK_LAUNCH();
 }
 

@@ -19,4 +19,9 @@ struct GemmOp {
 // Launches all ops in one kernel; ops must write disjoint C matrices.
 void launch_gemm_ops(Context& ctx, const std::vector<GemmOp>& ops, const char* name);
 
+// One CTA per worker w running ops [begin[w], begin[w+1]) in order (ops of one
+// worker may update the same C); different workers write disjoint C.
+void launch_gemm_workers(Context& ctx, const std::vector<GemmOp>& ops,
+                         const std::vector<int>& begin, const char* name);
+
 }  // namespace hmb

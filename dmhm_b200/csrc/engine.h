@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <chrono>
 #include <map>
 #include <memory>
 #include <string>
@@ -40,6 +41,24 @@ struct Context {
     struct Totals { double ms = 0; long long launches = 0; };
     std::map<std::string, Totals> totals;
     void collect();   // synchronizes, folds pending event pairs into totals
+};
+
+// Host-side wall time of a phase, recorded under `name` when profiling.
+class HostScope {
+  public:
+    HostScope(Context& c, const char* name)
+        : c_(c), name_(name), t0_(std::chrono::steady_clock::now()) {}
+    ~HostScope() {
+        if (!c_.profiling) return;
+        auto dt = std::chrono::steady_clock::now() - t0_;
+        auto& t = c_.totals[std::string("host:") + name_];
+        t.ms += std::chrono::duration<double, std::milli>(dt).count();
+        t.launches += 1;
+    }
+  private:
+    Context& c_;
+    const char* name_;
+    std::chrono::steady_clock::time_point t0_;
 };
 
 // Counts every kernel launch of the library (all contexts).

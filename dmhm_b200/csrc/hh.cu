@@ -268,6 +268,7 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
     const int maxRankC = fresh ? A.max_rank : C.max_rank;
 
     // ---------------- symbolic phase ----------------
+    std::unique_ptr<HostScope> hs(new HostScope(ctx, "hh_symbolic"));
     Planner P(A, B, maxRankC, ctx.oversample, ctx.serial_state);
     if (fresh)
         P.fresh(0, 0, 0, alpha);
@@ -314,6 +315,7 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
         crank[c] = rank;
     }
 
+    hs.reset(new HostScope(ctx, "hh_sampling_lists"));
     // ---------------- allocation ----------------
     // keep the old C storage if C is updated in place
     DeviceBuffer<double> c_old_data;
@@ -483,6 +485,7 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
     }
     // HH products with rank 0 (empty blocks): nothing to compute.
 
+    hs.reset(new HostScope(ctx, "hh_leaf_lists"));
     // ---------------- leaf products ----------------
     {
         std::vector<GemmOp> g1, g2;
@@ -529,66 +532,61 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
         launch_gemm_ops(ctx, g2, "leaf_products");
     }
 
-    // ---------------- waves over the C blocks ----------------
-    // ping-pong state slots for low-rank blocks with more than one operation
-    Arena pa;
+    hs.reset(new HostScope(ctx, "hh_block_lists"));
+    // ---------------- per-block operation lists ----------------
+    // One worker (CTA) per C leaf block runs that block's operations in the
+    // reference's order; blocks proceed independently.  Low-rank states of a
+    // block with several operations alternate between two scratch slots; the
+    // last operation writes into C.
+    Arena pa, wk;
     std::vector<long long> slot0(S.blocks.size(), -1), slot1(S.blocks.size(), -1);
-    size_t max_ops = 0;
+    std::vector<long long> wslot(S.blocks.size(), -1);
     for (int c : S.leaves) {
         const Block& Cb = S.blocks[c];
-        if (Cb.kind == KIND_LOWRANK) {
-            max_ops = std::max(max_ops, P.lops[c].size());
-            int mr = 0;
-            for (size_t j = 0; j + 1 < state_rank[c].size(); ++j)
-                mr = std::max(mr, state_rank[c][j]);
-            if (P.lops[c].size() > 1) {
-                slot0[c] = pa.take((long long)(Cb.m + Cb.n) * mr);
-                slot1[c] = pa.take((long long)(Cb.m + Cb.n) * mr);
-            }
-        } else {
-            max_ops = std::max(max_ops, P.dops[c].size() + (fresh ? 0 : 1));
+        if (Cb.kind != KIND_LOWRANK || P.lops[c].empty()) continue;
+        int mr = 0;
+        for (size_t j = 0; j + 1 < state_rank[c].size(); ++j) mr = std::max(mr, state_rank[c][j]);
+        if (P.lops[c].size() > 1) {
+            slot0[c] = pa.take((long long)(Cb.m + Cb.n) * mr);
+            slot1[c] = pa.take((long long)(Cb.m + Cb.n) * mr);
         }
     }
     DeviceBuffer<double> parena;
     parena.allocate((size_t)std::max<long long>(pa.used, 2), st);
     double* P0 = parena.get();
-    // current state pointer of each low-rank C block
-    std::vector<const double*> cu(S.blocks.size(), nullptr), cv(S.blocks.size(), nullptr);
-    std::vector<int> cr(S.blocks.size(), 0);
-    if (!fresh) {
-        for (int c : S.leaves)
-            if (S.blocks[c].kind == KIND_LOWRANK) {
-                cu[c] = c_old_data.get() + c_old_off[c];
-                cv[c] = cu[c] + (long long)S.blocks[c].m * c_old_rank[c];
-                cr[c] = c_old_rank[c];
+    std::vector<RoundOp> rops;
+    std::vector<int> rbegin{0};
+    std::vector<long long> rwork;   // per op: offset into the work arena
+    std::vector<GemmOp> gops;
+    std::vector<int> gbegin{0};
+    for (int c : S.leaves) {
+        const Block& Cb = S.blocks[c];
+        if (Cb.kind == KIND_LOWRANK) {
+            const std::vector<LOp>& ops = P.lops[c];
+            if (ops.empty()) continue;
+            const double* cu = nullptr;
+            const double* cv = nullptr;
+            int cr = 0;
+            if (!fresh) {
+                cu = c_old_data.get() + c_old_off[c];
+                cv = cu + (long long)Cb.m * c_old_rank[c];
+                cr = c_old_rank[c];
             }
-    }
-    for (size_t wv = 0; wv < max_ops; ++wv) {
-        std::vector<RoundOp> rops;
-        Arena work;
-        std::vector<size_t> need_work;
-        std::vector<GemmOp> gops;
-        for (int c : S.leaves) {
-            const Block& Cb = S.blocks[c];
-            if (Cb.kind == KIND_LOWRANK) {
-                if (wv >= P.lops[c].size()) continue;
-                const LOp& op = P.lops[c][wv];
-                const int rnew = state_rank[c][wv];
+            long long wmax = 0;
+            const size_t first = rops.size();
+            for (size_t j = 0; j < ops.size(); ++j) {
+                const LOp& op = ops[j];
+                const int rnew = state_rank[c][j];
                 if (op.type == L_RESET) {
-                    cr[c] = 0;
+                    cr = 0;
                     continue;
                 }
-                const bool last = wv + 1 == P.lops[c].size();
-                double* ou;
-                if (last) {
-                    ou = C.U(c);
-                } else {
-                    ou = P0 + ((wv & 1) ? slot1[c] : slot0[c]);
-                }
+                double* ou = (j + 1 == ops.size()) ? C.U(c)
+                                                    : P0 + ((j & 1) ? slot1[c] : slot0[c]);
                 double* ov = ou + (long long)Cb.m * rnew;
                 const WTask& t = P.w[op.w];
                 RoundOp r{};
-                r.kind = op_kind[c][wv];
+                r.kind = op_kind[c][j];
                 r.m = Cb.m;
                 r.n = Cb.n;
                 r.alpha = 1.0;
@@ -606,34 +604,30 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
                     r.ldv1 = t.ldV;
                     r.r1 = t.r;
                 }
-                r.u2 = cu[c];
-                r.v2 = cv[c];
-                r.r2 = (op.type == L_SET) ? 0 : cr[c];
+                r.u2 = cu;
+                r.v2 = cv;
+                r.r2 = (op.type == L_SET || (op.type == L_DDC && op.beta == 0.0)) ? 0 : cr;
                 r.ldu2 = Cb.m;
                 r.ldv2 = Cb.n;
-                if (op.type == L_DDC && op.beta == 0.0) r.r2 = 0;
-                if (rnew == 0 || Cb.m == 0 || Cb.n == 0) {
-                    // nothing to compute: empty result
-                } else {
+                if (rnew > 0 && Cb.m > 0 && Cb.n > 0) {
                     rops.push_back(r);
-                    need_work.push_back(rops.size() - 1);
+                    wmax = std::max(wmax, round_work_size(r));
                 }
-                cu[c] = ou;
-                cv[c] = ov;
-                cr[c] = rnew;
-            } else {
-                // dense leaf: optional initial copy of the old block (update form)
-                size_t idx = wv;
-                if (!fresh) {
-                    if (wv == 0) {
-                        gops.push_back({c_old_data.get() + c_old_off[c], nullptr, C.D(c), 1.0, 0.0,
-                                        Cb.m, Cb.n, -1, Cb.m, 0, Cb.m, 0, 0});
-                        continue;
-                    }
-                    idx = wv - 1;
-                }
-                if (idx >= P.dops[c].size()) continue;
-                const DOp& op = P.dops[c][idx];
+                cu = ou;
+                cv = ov;
+                cr = rnew;
+            }
+            if (rops.size() > first) {
+                const long long w0 = wk.take(wmax);
+                for (size_t i = first; i < rops.size(); ++i) rwork.push_back(w0);
+                rbegin.push_back((int)rops.size());
+            }
+        } else {
+            const size_t first = gops.size();
+            if (!fresh)
+                gops.push_back({c_old_data.get() + c_old_off[c], nullptr, C.D(c), 1.0, 0.0, Cb.m,
+                                Cb.n, -1, Cb.m, 0, Cb.m, 0, 0});
+            for (const DOp& op : P.dops[c]) {
                 if (op.type == D_DD) {
                     const Block& Ba = S.blocks[op.a];
                     const Block& Bb = S.blocks[op.b];
@@ -641,28 +635,25 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
                                     Ba.n, Ba.m, Bb.m, Cb.m, 0, 0});
                 } else {
                     const WTask& t = P.w[op.w];
-                    if (t.r == 0) {
-                        // D := beta D (+ 0)
+                    if (t.r == 0)
                         gops.push_back({C.D(c), nullptr, C.D(c), op.beta, 0.0, Cb.m, Cb.n, -1,
                                         Cb.m, 0, Cb.m, 0, 0});
-                    } else {
+                    else
                         gops.push_back({t.U + op.row0, t.V + op.col0, C.D(c), 1.0, op.beta, Cb.m,
                                         Cb.n, t.r, t.ldU, t.ldV, Cb.m, 0, 1});
-                    }
                 }
             }
+            if (gops.size() > first && Cb.m > 0 && Cb.n > 0) gbegin.push_back((int)gops.size());
+            else gops.resize(first);
         }
-        // scratch for the rounding ops of this wave
-        std::vector<long long> woff(rops.size(), 0);
-        for (size_t i = 0; i < rops.size(); ++i) woff[i] = work.take(round_work_size(rops[i]));
-        DeviceBuffer<double> wbuf;
-        if (!rops.empty()) {
-            wbuf.allocate((size_t)std::max<long long>(work.used, 2), st);
-            for (size_t i = 0; i < rops.size(); ++i) rops[i].work = wbuf.get() + woff[i];
-        }
-        launch_round_ops(ctx, rops, "block_round");
-        launch_gemm_ops(ctx, gops, "dense_update");
     }
+    DeviceBuffer<double> wbuf;
+    if (!rops.empty()) {
+        wbuf.allocate((size_t)std::max<long long>(wk.used, 2), st);
+        for (size_t i = 0; i < rops.size(); ++i) rops[i].work = wbuf.get() + rwork[i];
+    }
+    launch_round_workers(ctx, rops, rbegin, "block_round");
+    launch_gemm_workers(ctx, gops, gbegin, "dense_update");
     // low-rank C blocks whose final rank is 0 or that received no operation
     // need nothing: their storage is empty.
     ctx.serial_state = serial_after;

@@ -202,14 +202,19 @@ __device__ void cta_order_columns(const double* M, int rows, int cols, double* n
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(kT)
-round_kernel(const RoundOp* __restrict__ ops, int smem_mj) {
-    extern __shared__ double dyn[];
-    __shared__ double red[kW + 1];
-    __shared__ double norms[kMaxK];
-    __shared__ int order[kMaxK];
-    __shared__ int flag;
-    const RoundOp op = ops[blockIdx.x];
+struct RoundShared {
+    double red[kW + 1];
+    double norms[kMaxK];
+    int order[kMaxK];
+    int flag;
+};
+
+// One rounding operation, executed by the whole CTA.  `dyn` holds the core
+// and the rotations when they fit in `smem_k` x `smem_k` each.
+__device__ void do_round(const RoundOp& op, double* dyn, int smem_k, RoundShared& sh) {
+    double* red = sh.red;
+    double* norms = sh.norms;
+    int* order = sh.order;
     const int m = op.m, n = op.n;
     const int tid = threadIdx.x;
 
@@ -257,9 +262,9 @@ round_kernel(const RoundOp* __restrict__ ops, int smem_mj) {
     const int kv = dense ? n : min(n, k);
     double* M;
     double* J;
-    if (smem_mj) {
+    if (ku <= smem_k && kv <= smem_k) {
         M = dyn;
-        J = dyn + (long long)kSmemK * kSmemK;
+        J = dyn + (long long)smem_k * smem_k;
     } else {
         M = w;
         J = w + (long long)ku * kv;
@@ -317,7 +322,7 @@ round_kernel(const RoundOp* __restrict__ ops, int smem_mj) {
     __syncthreads();
 
     // ---- SVD of the core ---------------------------------------------------
-    cta_jacobi(M, ku, kv, J, &flag);
+    cta_jacobi(M, ku, kv, J, &sh.flag);
     cta_order_columns(M, ku, kv, norms, order);
 
     // ---- outputs -------------------------------------------------------------
@@ -342,6 +347,20 @@ round_kernel(const RoundOp* __restrict__ ops, int smem_mj) {
     __syncthreads();
     if (!ortho) cta_apply_q(Ucat, m, min(m, k), m, tauU, op.uo, rout, m);
     if (!dense) cta_apply_q(Vcat, n, min(n, k), n, tauV, op.vo, rout, n);
+}
+
+// One CTA per worker; worker w runs ops [begin[w], begin[w+1]) in order (a
+// C block's whole operation list, each op reading the previous one's output).
+__global__ void __launch_bounds__(kT)
+round_worker_kernel(const RoundOp* __restrict__ ops, const int* __restrict__ begin, int smem_k) {
+    extern __shared__ double dyn[];
+    __shared__ RoundShared sh;
+    const int b0 = begin[blockIdx.x], b1 = begin[blockIdx.x + 1];
+    for (int i = b0; i < b1; ++i) {
+        const RoundOp op = ops[i];
+        do_round(op, dyn, smem_k, sh);
+        __syncthreads();
+    }
 }
 
 __global__ void __launch_bounds__(kT) qr_formq_kernel(const QrOp* __restrict__ ops) {
@@ -375,26 +394,40 @@ long long round_work_size(const RoundOp& op) {
 }
 
 void launch_round_ops(Context& ctx, std::vector<RoundOp>& ops, const char* name) {
-    if (ops.empty()) return;
+    std::vector<int> begin(ops.size() + 1);
+    for (size_t i = 0; i <= ops.size(); ++i) begin[i] = (int)i;
+    launch_round_workers(ctx, ops, begin, name);
+}
+
+void launch_round_workers(Context& ctx, const std::vector<RoundOp>& ops,
+                          const std::vector<int>& begin, const char* name) {
+    if (ops.empty() || begin.size() < 2) return;
     int kmax = 0;
     for (const RoundOp& op : ops) {
         int k = op.kind == ROUND_DENSE ? op.n : op.r1 + (op.kind == ROUND_GENERAL ? op.r2 : 0);
+        if (op.kind == ROUND_SET || op.kind == ROUND_CONCAT) k = 0;
         HMB_REQUIRE(k <= kMaxK, HM_ERR_UNSUPPORTED,
                     "low-rank rounding of more than 128 stacked columns");
         kmax = std::max(kmax, k);
     }
-    const int smem_mj = kmax <= kSmemK ? 1 : 0;
-    const size_t smem = smem_mj ? 2 * kSmemK * kSmemK * sizeof(double) : 0;
-    static bool attr_set = false;
-    if (!attr_set) {
-        HMB_CUDA(cudaFuncSetAttribute(round_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    const int smem_k = std::min(kmax, kSmemK);
+    const size_t smem = 2 * (size_t)smem_k * smem_k * sizeof(double);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static int attr_dev = -1;
+    if (attr_dev != dev) {
+        HMB_CUDA(cudaFuncSetAttribute(round_worker_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)(2 * kSmemK * kSmemK * sizeof(double))));
-        attr_set = true;
+        attr_dev = dev;
     }
     DeviceBuffer<RoundOp> d;
     d.upload(ops, ctx.stream);
+    DeviceBuffer<int> db;
+    db.upload(begin, ctx.stream);
     LaunchScope ls(ctx, name);
-    round_kernel<<<(unsigned)ops.size(), kT, smem, ctx.stream>>>(d.get(), smem_mj);
+    round_worker_kernel<<<(unsigned)(begin.size() - 1), kT, smem, ctx.stream>>>(d.get(), db.get(),
+                                                                              smem_k);
     HMB_CHECK_LAUNCH();
 }
 

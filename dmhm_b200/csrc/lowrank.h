@@ -33,6 +33,11 @@ long long round_work_size(const RoundOp& op);
 // Launches one CTA per op.  Ops must write disjoint outputs.
 void launch_round_ops(Context& ctx, std::vector<RoundOp>& ops, const char* name);
 
+// One CTA per worker w running ops [begin[w], begin[w+1]) in order; different
+// workers must write disjoint outputs.
+void launch_round_workers(Context& ctx, const std::vector<RoundOp>& ops,
+                          const std::vector<int>& begin, const char* name);
+
 // Orthonormal basis of the columns of Y (m x k, overwritten), written to Q
 // (m x min(m,k)): Householder QR, then Q = H_1 ... H_kk [I; 0].
 struct QrOp {

@@ -323,6 +323,7 @@ struct MatPlan {
 void MatPlanDeleter::operator()(MatPlan* p) const { delete p; }
 
 PlanPtr build_plan(Context& ctx, const std::vector<JobSpec>& jobs) {
+    HostScope hs(ctx, "hmm_plan");
     cudaStream_t st = ctx.stream;
     PlanPtr plan(new MatPlan);
     plan->njobs = (int)jobs.size();
@@ -394,13 +395,32 @@ PlanPtr build_plan(Context& ctx, const std::vector<JobSpec>& jobs) {
         const Box& outBox = S.boxes[J.trans ? R.src_box : R.tgt_box];
         const int outBase = J.trans ? R.col_off : R.row_off;
         if (J.k == 0) continue;
+        // bucket the subtree's leaf blocks by the output clusters they cover
+        const int c0 = outBox.leaf0, nc = outBox.leaf1 - outBox.leaf0;
+        std::vector<int> count(nc + 1, 0);
+        for (int b : sub_leaves[j]) {
+            const Block& B = S.blocks[b];
+            if (B.m == 0 || B.n == 0) continue;
+            const Box& ob = S.boxes[J.trans ? B.src_box : B.tgt_box];
+            for (int c = ob.leaf0; c < ob.leaf1; ++c) count[c - c0 + 1]++;
+        }
+        for (int c = 0; c < nc; ++c) count[c + 1] += count[c];
+        std::vector<int> bucket(count[nc]);
+        {
+            std::vector<int> fill(count.begin(), count.end() - 1);
+            for (int b : sub_leaves[j]) {
+                const Block& B = S.blocks[b];
+                if (B.m == 0 || B.n == 0) continue;
+                const Box& ob = S.boxes[J.trans ? B.src_box : B.tgt_box];
+                for (int c = ob.leaf0; c < ob.leaf1; ++c) bucket[fill[c - c0]++] = b;
+            }
+        }
         for (int c = outBox.leaf0; c < outBox.leaf1; ++c) {
             const Box& cl = S.boxes[S.leaf_box[c]];
             if (cl.count == 0) continue;
             int e0 = (int)ent.size();
-            const std::vector<int>& cover = J.trans ? S.col_cover[c] : S.row_cover[c];
-            for (int b : cover) {
-                if (!S.in_subtree(b, J.root)) continue;
+            for (int bi = count[c - c0]; bi < count[c - c0 + 1]; ++bi) {
+                const int b = bucket[bi];
                 const Block& B = S.blocks[b];
                 P2Entry e{};
                 if (B.kind == KIND_DENSE) {

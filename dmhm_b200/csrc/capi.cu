@@ -160,6 +160,9 @@ void import_csr(HMatrix& H, const int64_t* rows, const int32_t* cols,
     HMB_CUDA(cudaStreamSynchronize(H.ctx->stream));
 }
 
+void multiply_vector_noalloc(HMatrix& H, int transpose, double alpha, const double* x,
+                             double beta, double* y);
+
 void multiply_dense(HMatrix& H, int transpose, double alpha, const double* B,
                     int ldb, double beta, double* C, int ldc, int nrhs) {
     HMB_REQUIRE(nrhs >= 0, HM_ERR_ARGUMENT, "nrhs must be >= 0");
@@ -469,6 +472,16 @@ int hm_add_constant_to_diagonal(hm_matrix h, double alpha) {
     return guarded([&] {
         HMB_REQUIRE(h, HM_ERR_ARGUMENT, "h is NULL");
         hmat_add_diagonal(owner_of(h)->c, h->h, alpha);
+    });
+}
+
+int hm_multiply_vector_noalloc(hm_matrix h, int transpose, double alpha, const double* x,
+                               double beta, double* y) {
+    return guarded([&] {
+        HMB_REQUIRE(h, HM_ERR_ARGUMENT, "h is NULL");
+        owner_of(h);
+        HMB_REQUIRE(h->h.S != nullptr, HM_ERR_ARGUMENT, "empty H-matrix");
+        multiply_vector_noalloc(h->h, transpose != 0, alpha, x, beta, y);
     });
 }
 

@@ -149,6 +149,22 @@ HM_API int hm_transpose(hm_matrix src, hm_matrix* dst);
 HM_API int hm_scale(hm_matrix h, double alpha);
 HM_API int hm_add_constant_to_diagonal(hm_matrix h, double alpha);
 
+/*
+ * y := alpha op(H) x + beta y for one vector (DEVICE pointers, stream-ordered)
+ * without allocating any device memory.  No counterpart in the reference: it
+ * is for callers that cannot allocate device memory during the call (their
+ * memory manager already holds the GPU's memory, or a time-critical loop must
+ * not call the allocator).  Intermediates live in one static 4 MiB device
+ * array of the library, so the matrix may need at most 524288 entries of
+ * (blocks + sum of low-rank ranks); larger matrices return
+ * HM_ERR_UNSUPPORTED.  The first call on a device looks up the array's
+ * address; make that first call before any stream capture.  All calls share
+ * the array: calls that overlap on the GPU race and must not be issued.
+ * Results agree with hm_multiply_dense to rounding (atomic accumulation).
+ */
+HM_API int hm_multiply_vector_noalloc(hm_matrix h, int transpose, double alpha,
+                                      const double* x, double beta, double* y);
+
 /* Diagnostics (no reference counterpart): number of kernels this library has
    launched so far in the process, and per-kernel CUDA-event timing on the
    context stream.  hm_profile_enable resets the totals; hm_profile_read

@@ -34,7 +34,7 @@ hm_matrix_s* new_handle(hm_context_s* ctx) {
 
 // Releases the device storage of a handle (stream-ordered frees).
 void release_storage(hm_matrix_s* m) {
-    m->h.plans.clear();
+    m->h.templates.clear();
     m->h.data.reset();
     m->h.table.reset();
 }
@@ -171,13 +171,7 @@ void multiply_dense(HMatrix& H, int transpose, double alpha, const double* B,
     HMB_REQUIRE(ldb >= std::max(1, n) && ldc >= std::max(1, m), HM_ERR_ARGUMENT,
                 "leading dimension too small");
     if (nrhs == 0 || m == 0) return;
-    auto key = std::make_pair(transpose != 0 ? 1 : 0, nrhs);
-    auto it = H.plans.find(key);
-    if (it == H.plans.end()) {
-        PlanPtr p = build_plan(*H.ctx, {JobSpec{&H, 0, transpose != 0, nrhs}});
-        it = H.plans.emplace(key, std::shared_ptr<MatPlan>(p.release(), MatPlanDeleter())).first;
-    }
-    execute_plan(*H.ctx, *it->second, {JobArgs{B, C, alpha, beta, ldb, ldc, nrhs, 0}});
+    run_jobs(*H.ctx, {MatJob{&H, 0, transpose != 0, alpha, beta, B, ldb, C, ldc, nrhs}});
 }
 
 }  // namespace hmb

@@ -97,9 +97,9 @@ class HMatrix {
     long long total = 0;            // elements in `data`
     DeviceBuffer<double> data;
     DeviceBuffer<DevBlock> table;   // device copy of the per-block table
-    // Cached whole-matrix multiply plans keyed by (transpose, k); dropped
+    // Cached multiply work lists keyed by (subtree root, transpose); dropped
     // whenever the storage is re-laid out.
-    std::map<std::pair<int, int>, std::shared_ptr<struct MatPlan>> plans;
+    mutable std::map<std::pair<int, int>, std::shared_ptr<struct JobTemplate>> templates;
 
     int height() const { return S->N; }
     int width() const { return S->N; }
@@ -125,32 +125,13 @@ struct MatJob {
     double* out;
     int ldout;
     int k;
-};
-
-// The structural part of a batch of jobs (which H-matrix subtree, op, width)
-// and the per-call part (pointers, scalars).
-struct JobSpec {
-    const HMatrix* H;
-    int root;
-    bool trans;
-    int k;
-};
-struct JobArgs {
-    const double* in;
-    double* out;
-    double alpha, beta;
-    int ldin, ldout, k, pad;
     const double* alpha_scale = nullptr;   // if set, alpha is multiplied by *alpha_scale
 };
 
-// Work lists of a batch of jobs, resident on the device: build once, execute
-// many times with different pointers (the plan references the H-matrices'
-// storage, so it is invalid once they are re-laid out).
-struct MatPlan;
-struct MatPlanDeleter { void operator()(MatPlan* p) const; };
-using PlanPtr = std::unique_ptr<MatPlan, MatPlanDeleter>;
-PlanPtr build_plan(Context& ctx, const std::vector<JobSpec>& jobs);
-void execute_plan(Context& ctx, MatPlan& plan, const std::vector<JobArgs>& args);
+// Work lists of one subtree (root, op) of one H-matrix, kept on the device
+// (matmul.cu).  Cached per H-matrix; dropped when its storage is re-laid out.
+struct JobTemplate;
+std::shared_ptr<JobTemplate> get_template(Context& ctx, const HMatrix& H, int root, bool trans);
 
 // Runs a batch of jobs as two level-batched launches (low-rank inner products,
 // then one fused output pass per row tile).  Outputs of different jobs must

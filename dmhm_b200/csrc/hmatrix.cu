@@ -13,7 +13,7 @@ namespace hmb {
 
 void HMatrix::layout() {
     const Structure& St = *S;
-    plans.clear();
+    templates.clear();
     off.assign(St.blocks.size(), -1);
     long long cur = 0;
     for (int b : St.leaves) {

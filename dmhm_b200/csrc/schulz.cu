@@ -237,17 +237,11 @@ double estimate_two_norm(Context& ctx, HMatrix& A, double theta, double confiden
     // x currently unnormalised; its scale is folded into the first product
     // through alpha_scale = 1/||x||.
     const double root = 1.0 / (double)k;
-    auto key = std::make_pair(0, 1);
-    auto it = A.plans.find(key);
-    if (it == A.plans.end()) {
-        PlanPtr p = build_plan(ctx, {JobSpec{&A, 0, false, 1}});
-        it = A.plans.emplace(key, std::shared_ptr<MatPlan>(p.release(), MatPlanDeleter())).first;
-    }
     double* cur = x.get();
     double* nxt = y.get();
     for (int i = 0; i < k; ++i) {
-        JobArgs ja{cur, nxt, 1.0, 0.0, n, n, 1, 0, scal.get()};
-        execute_plan(ctx, *it->second, {ja});
+        MatJob job{&A, 0, false, 1.0, 0.0, cur, n, nxt, n, 1, scal.get()};
+        run_jobs(ctx, {job});
         LaunchScope ls(ctx, "norm_reduce");
         sumsq_partial_kernel<<<kNormBlocks, kT, 0, st>>>(nxt, n, partial.get());
         norm_finalize_kernel<<<1, 32, 0, st>>>(partial.get(), kNormBlocks, scal.get(),
@@ -310,7 +304,7 @@ SchulzResult schulz_invert(Context& ctx, HMatrix& A, int num_iterations, double 
     A.total = X->total;
     A.data = std::move(X->data);
     A.table = std::move(X->table);
-    A.plans.clear();
+    A.templates.clear();
     return res;
 }
 

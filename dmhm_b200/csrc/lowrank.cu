@@ -24,7 +24,6 @@ namespace {
 constexpr int kT = 256;
 constexpr int kW = kT / 32;
 constexpr int kMaxK = 128;         // largest stacked rank handled
-constexpr int kSmemK = 64;         // M and J in shared memory up to this k
 constexpr int kJacobiSweeps = 40;  // bounded; converges in ~6-12
 constexpr double kJacobiTol = 1e-15;
 
@@ -210,8 +209,9 @@ struct RoundShared {
 };
 
 // One rounding operation, executed by the whole CTA.  `dyn` holds the core
-// and the rotations when they fit in `smem_k` x `smem_k` each.
-__device__ void do_round(const RoundOp& op, double* dyn, int smem_k, RoundShared& sh) {
+// and the rotations in shared memory when they fit in `smem_doubles` doubles.
+__device__ void do_round(const RoundOp& op, double* dyn, long long smem_doubles,
+                         RoundShared& sh) {
     double* red = sh.red;
     double* norms = sh.norms;
     int* order = sh.order;
@@ -249,7 +249,15 @@ __device__ void do_round(const RoundOp& op, double* dyn, int smem_k, RoundShared
     const int k = dense ? n : op.r1 + (op.kind == ROUND_GENERAL ? op.r2 : 0);
     const int rout = op.rout;
     if (m == 0 || n == 0) return;
-    double* w = op.work;
+    const int ku = ortho ? op.r1 : min(m, k);
+    const int kv = dense ? n : min(n, k);
+    // Everything in shared memory when it fits (`smem_doubles`), else the
+    // core and rotations alone, else all in the global work area.
+    const long long need_f = (ortho ? 0LL : (long long)m * k) + (dense ? 0LL : (long long)n * k);
+    const long long need_mj = (long long)ku * kv + (long long)kv * kv;
+    const bool all_smem = need_f + 2 * k + need_mj <= smem_doubles;
+    const bool mj_smem = !all_smem && need_mj <= smem_doubles;
+    double* w = all_smem ? dyn : op.work;
     double* Ucat = w;
     if (!ortho) w += (long long)m * k;
     double* Vcat = w;
@@ -258,13 +266,11 @@ __device__ void do_round(const RoundOp& op, double* dyn, int smem_k, RoundShared
     w += k;
     double* tauV = w;
     w += k;
-    const int ku = ortho ? op.r1 : min(m, k);
-    const int kv = dense ? n : min(n, k);
     double* M;
     double* J;
-    if (ku <= smem_k && kv <= smem_k) {
+    if (mj_smem) {
         M = dyn;
-        J = dyn + (long long)smem_k * smem_k;
+        J = dyn + (long long)ku * kv;
     } else {
         M = w;
         J = w + (long long)ku * kv;
@@ -352,13 +358,15 @@ __device__ void do_round(const RoundOp& op, double* dyn, int smem_k, RoundShared
 // One CTA per worker; worker w runs ops [begin[w], begin[w+1]) in order (a
 // C block's whole operation list, each op reading the previous one's output).
 __global__ void __launch_bounds__(kT)
-round_worker_kernel(const RoundOp* __restrict__ ops, const int* __restrict__ begin, int smem_k) {
+round_worker_kernel(const RoundOp* __restrict__ ops, const int* __restrict__ begin,
+                    const int* __restrict__ workers, long long smem_doubles) {
     extern __shared__ double dyn[];
     __shared__ RoundShared sh;
-    const int b0 = begin[blockIdx.x], b1 = begin[blockIdx.x + 1];
+    const int w = workers[blockIdx.x];
+    const int b0 = begin[w], b1 = begin[w + 1];
     for (int i = b0; i < b1; ++i) {
         const RoundOp op = ops[i];
-        do_round(op, dyn, smem_k, sh);
+        do_round(op, dyn, smem_doubles, sh);
         __syncthreads();
     }
 }
@@ -399,36 +407,58 @@ void launch_round_ops(Context& ctx, std::vector<RoundOp>& ops, const char* name)
     launch_round_workers(ctx, ops, begin, name);
 }
 
+long long round_smem_need(const RoundOp& op) {
+    if (op.kind == ROUND_SET || op.kind == ROUND_CONCAT) return 0;
+    const bool ortho = op.kind == ROUND_ORTHO, dense = op.kind == ROUND_DENSE;
+    const long long k = dense ? op.n : op.r1 + (op.kind == ROUND_GENERAL ? op.r2 : 0);
+    const long long ku = ortho ? op.r1 : std::min<long long>(op.m, k);
+    const long long kv = dense ? op.n : std::min<long long>(op.n, k);
+    return (ortho ? 0 : op.m * k) + (dense ? 0 : op.n * k) + 2 * k + ku * kv + kv * kv;
+}
+
 void launch_round_workers(Context& ctx, const std::vector<RoundOp>& ops,
                           const std::vector<int>& begin, const char* name) {
     if (ops.empty() || begin.size() < 2) return;
-    int kmax = 0;
     for (const RoundOp& op : ops) {
         int k = op.kind == ROUND_DENSE ? op.n : op.r1 + (op.kind == ROUND_GENERAL ? op.r2 : 0);
         if (op.kind == ROUND_SET || op.kind == ROUND_CONCAT) k = 0;
         HMB_REQUIRE(k <= kMaxK, HM_ERR_UNSUPPORTED,
                     "low-rank rounding of more than 128 stacked columns");
-        kmax = std::max(kmax, k);
     }
-    const int smem_k = std::min(kmax, kSmemK);
-    const size_t smem = 2 * (size_t)smem_k * smem_k * sizeof(double);
+    // Workers grouped by the shared memory their largest op can use; each
+    // group is one launch sized for it.
+    const long long classes[4] = {2048, 6144, 16384, 26624};   // doubles: 16/48/128/208 KB
+    std::vector<std::vector<int>> group(4);
+    const int nw = (int)begin.size() - 1;
+    for (int w = 0; w < nw; ++w) {
+        long long need = 0;
+        for (int i = begin[w]; i < begin[w + 1]; ++i) need = std::max(need, round_smem_need(ops[i]));
+        int g = 0;
+        while (g < 3 && need > classes[g]) ++g;
+        group[g].push_back(w);
+    }
     int dev = 0;
     cudaGetDevice(&dev);
     static int attr_dev = -1;
     if (attr_dev != dev) {
         HMB_CUDA(cudaFuncSetAttribute(round_worker_kernel,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(2 * kSmemK * kSmemK * sizeof(double))));
+                                      (int)(classes[3] * sizeof(double))));
         attr_dev = dev;
     }
     DeviceBuffer<RoundOp> d;
     d.upload(ops, ctx.stream);
     DeviceBuffer<int> db;
     db.upload(begin, ctx.stream);
-    LaunchScope ls(ctx, name);
-    round_worker_kernel<<<(unsigned)(begin.size() - 1), kT, smem, ctx.stream>>>(d.get(), db.get(),
-                                                                              smem_k);
-    HMB_CHECK_LAUNCH();
+    for (int g = 0; g < 4; ++g) {
+        if (group[g].empty()) continue;
+        DeviceBuffer<int> dw;
+        dw.upload(group[g], ctx.stream);
+        LaunchScope ls(ctx, name);
+        round_worker_kernel<<<(unsigned)group[g].size(), kT, classes[g] * sizeof(double),
+                              ctx.stream>>>(d.get(), db.get(), dw.get(), classes[g]);
+        HMB_CHECK_LAUNCH();
+    }
 }
 
 void launch_qr_formq(Context& ctx, const std::vector<QrOp>& ops, const char* name) {

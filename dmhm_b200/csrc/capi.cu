@@ -197,6 +197,14 @@ int hm_context_create(int device, void* cuda_stream, hm_context* out) {
         c->c.serial_state = kLcgSeed;
         c->c.parallel_state = kLcgSeed;
         cudaDeviceGetAttribute(&c->c.num_sms, cudaDevAttrMultiProcessorCount, device);
+        // Keep freed stream-ordered memory in this process's pool across
+        // synchronizations instead of returning it at every sync (a process
+        // setting of the pool, not of the GPU).
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            uint64_t threshold = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+        }
         if (cuda_stream) {
             c->c.stream = (cudaStream_t)cuda_stream;
         } else {

@@ -78,6 +78,32 @@ struct DOp {
     int a, b;
 };
 
+// Operations grouped per C block: appended in recursion order, then grouped
+// by block with a stable counting sort (order inside a block is preserved).
+template <typename T>
+struct PerBlock {
+    std::vector<int> blk;
+    std::vector<T> raw;
+    std::vector<int> begin;
+    std::vector<T> ops;
+    void push(int c, const T& op) {
+        blk.push_back(c);
+        raw.push_back(op);
+    }
+    void finalize(size_t nblocks) {
+        begin.assign(nblocks + 1, 0);
+        for (int c : blk) begin[c + 1]++;
+        for (size_t c = 0; c < nblocks; ++c) begin[c + 1] += begin[c];
+        ops.resize(raw.size());
+        std::vector<int> fill(begin.begin(), begin.end() - 1);
+        for (size_t i = 0; i < raw.size(); ++i) ops[fill[blk[i]]++] = raw[i];
+        std::vector<int>().swap(blk);
+        std::vector<T>().swap(raw);
+    }
+    int size(int c) const { return begin[c + 1] - begin[c]; }
+    const T* of(int c) const { return ops.data() + begin[c]; }
+};
+
 struct Planner {
     const Structure& S;
     const HMatrix& A;
@@ -86,12 +112,11 @@ struct Planner {
     int oversample;
     uint64_t serial;
     std::vector<WTask> w;
-    std::vector<std::vector<LOp>> lops;
-    std::vector<std::vector<DOp>> dops;
+    PerBlock<LOp> lops;
+    PerBlock<DOp> dops;
 
     Planner(const HMatrix& a, const HMatrix& b, int maxRank, int over, uint64_t st)
-        : S(*a.S), A(a), B(b), maxRankC(maxRank), oversample(over), serial(st),
-          lops(a.S->blocks.size()), dops(a.S->blocks.size()) {}
+        : S(*a.S), A(a), B(b), maxRankC(maxRank), oversample(over), serial(st) {}
 
     int kind(int blk) const { return S.blocks[blk].kind; }
 
@@ -146,7 +171,7 @@ struct Planner {
         const int kc = kind(c);
         if (kc == KIND_LOWRANK) {
             int t = product(a, b, alpha);
-            lops[c].push_back({w[t].type == W_DD ? L_DDC : L_SET, t, 0, 0, 0.0});
+            lops.push(c, {w[t].type == W_DD ? L_DDC : L_SET, t, 0, 0, 0.0});
         } else if (kc == KIND_NODE) {
             HMB_REQUIRE(kind(a) != KIND_DENSE && kind(b) != KIND_DENSE, HM_ERR_UNSUPPORTED,
                         "invalid H-matrix combination");
@@ -172,7 +197,7 @@ struct Planner {
         const int kc = kind(c);
         if (kc == KIND_LOWRANK) {
             int t = product(a, b, alpha);
-            lops[c].push_back({w[t].type == W_DD ? L_DDC : L_RUPD, t, 0, 0, beta});
+            lops.push(c, {w[t].type == W_DD ? L_DDC : L_RUPD, t, 0, 0, beta});
         } else if (kc == KIND_NODE) {
             HMB_REQUIRE(kind(a) != KIND_DENSE && kind(b) != KIND_DENSE, HM_ERR_UNSUPPORTED,
                         "invalid H-matrix combination");
@@ -198,10 +223,10 @@ struct Planner {
         HMB_REQUIRE(kind(a) != KIND_NODE && kind(b) != KIND_NODE, HM_ERR_UNSUPPORTED,
                     "invalid H-matrix combination");
         if (kind(a) == KIND_DENSE && kind(b) == KIND_DENSE) {
-            dops[c].push_back({D_DD, -1, 0, 0, alpha, beta, a, b});
+            dops.push(c, {D_DD, -1, 0, 0, alpha, beta, a, b});
         } else {
             int t = product(a, b, alpha);
-            dops[c].push_back({D_LR, t, 0, 0, 1.0, beta, -1, -1});
+            dops.push(c, {D_LR, t, 0, 0, 1.0, beta, -1, -1});
         }
     }
 
@@ -209,7 +234,7 @@ struct Planner {
     void import_lowrank(int c, int t, int row0, int col0) {
         const Block& C = S.blocks[c];
         if (C.kind == KIND_LOWRANK) {
-            lops[c].push_back({L_SET, t, row0, col0, 0.0});
+            lops.push(c, {L_SET, t, row0, col0, 0.0});
         } else if (C.kind == KIND_NODE) {
             for (int ti = 0; ti < S.q; ++ti)
                 for (int si = 0; si < S.q; ++si) {
@@ -218,7 +243,7 @@ struct Planner {
                                    col0 + S.blocks[ch].col_off - C.col_off);
                 }
         } else {
-            dops[c].push_back({D_LR, t, row0, col0, 1.0, 0.0, -1, -1});
+            dops.push(c, {D_LR, t, row0, col0, 1.0, 0.0, -1, -1});
         }
     }
 
@@ -226,8 +251,8 @@ struct Planner {
     void update_with_lowrank(int c, int t, int row0, int col0, double beta) {
         const Block& C = S.blocks[c];
         if (C.kind == KIND_LOWRANK) {
-            if (beta == 0.0) lops[c].push_back({L_RESET, -1, 0, 0, 0.0});
-            lops[c].push_back({L_RUPD, t, row0, col0, beta == 0.0 ? 1.0 : beta});
+            if (beta == 0.0) lops.push(c, {L_RESET, -1, 0, 0, 0.0});
+            lops.push(c, {L_RUPD, t, row0, col0, beta == 0.0 ? 1.0 : beta});
         } else if (C.kind == KIND_NODE) {
             for (int ti = 0; ti < S.q; ++ti)
                 for (int si = 0; si < S.q; ++si) {
@@ -236,7 +261,7 @@ struct Planner {
                                         col0 + S.blocks[ch].col_off - C.col_off, beta);
                 }
         } else {
-            dops[c].push_back({D_LR, t, row0, col0, 1.0, beta, -1, -1});
+            dops.push(c, {D_LR, t, row0, col0, 1.0, beta, -1, -1});
         }
     }
 };
@@ -275,18 +300,24 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
     else
         P.update(0, 0, 0, alpha, beta);
     const uint64_t serial_after = P.serial;
+    P.lops.finalize(S.blocks.size());
+    P.dops.finalize(S.blocks.size());
 
     // final ranks of C
     std::vector<int> crank(S.blocks.size(), 0);
     std::vector<int> nops_lr(S.blocks.size(), 0);
-    std::vector<std::vector<int>> state_rank(S.blocks.size());   // rank after each op
-    std::vector<std::vector<int>> op_kind(S.blocks.size());      // RoundKind per op (-1 reset)
+    // rank after each operation and its rounding kind (-1: rank reset),
+    // parallel to P.lops.ops
+    std::vector<int> state_rank(P.lops.ops.size()), op_kind(P.lops.ops.size());
     for (int c : S.leaves) {
         const Block& Cb = S.blocks[c];
         if (Cb.kind != KIND_LOWRANK) continue;
         int rank = fresh ? 0 : C.rank[c];
         const int minDim = std::min(Cb.m, Cb.n);
-        for (const LOp& op : P.lops[c]) {
+        const int nops = P.lops.size(c);
+        const LOp* ops = P.lops.of(c);
+        for (int j = 0; j < nops; ++j) {
+            const LOp& op = ops[j];
             int kindr = -1;
             switch (op.type) {
                 case L_SET:
@@ -309,13 +340,12 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
                     kindr = ROUND_DENSE;
                     break;
             }
-            state_rank[c].push_back(rank);
-            op_kind[c].push_back(kindr);
+            state_rank[P.lops.begin[c] + j] = rank;
+            op_kind[P.lops.begin[c] + j] = kindr;
         }
         crank[c] = rank;
     }
 
-    hs.reset(new HostScope(ctx, "hh_sampling_lists"));
     // ---------------- allocation ----------------
     // keep the old C storage if C is updated in place
     DeviceBuffer<double> c_old_data;
@@ -543,10 +573,11 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
     std::vector<long long> wslot(S.blocks.size(), -1);
     for (int c : S.leaves) {
         const Block& Cb = S.blocks[c];
-        if (Cb.kind != KIND_LOWRANK || P.lops[c].empty()) continue;
+        const int nops = P.lops.size(c);
+        if (Cb.kind != KIND_LOWRANK || nops == 0) continue;
         int mr = 0;
-        for (size_t j = 0; j + 1 < state_rank[c].size(); ++j) mr = std::max(mr, state_rank[c][j]);
-        if (P.lops[c].size() > 1) {
+        for (int j = 0; j + 1 < nops; ++j) mr = std::max(mr, state_rank[P.lops.begin[c] + j]);
+        if (nops > 1) {
             slot0[c] = pa.take((long long)(Cb.m + Cb.n) * mr);
             slot1[c] = pa.take((long long)(Cb.m + Cb.n) * mr);
         }
@@ -562,8 +593,10 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
     for (int c : S.leaves) {
         const Block& Cb = S.blocks[c];
         if (Cb.kind == KIND_LOWRANK) {
-            const std::vector<LOp>& ops = P.lops[c];
-            if (ops.empty()) continue;
+            const int nops = P.lops.size(c);
+            const LOp* ops = P.lops.of(c);
+            const int obase = P.lops.begin[c];
+            if (nops == 0) continue;
             const double* cu = nullptr;
             const double* cv = nullptr;
             int cr = 0;
@@ -574,19 +607,19 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
             }
             long long wmax = 0;
             const size_t first = rops.size();
-            for (size_t j = 0; j < ops.size(); ++j) {
+            for (int j = 0; j < nops; ++j) {
                 const LOp& op = ops[j];
-                const int rnew = state_rank[c][j];
+                const int rnew = state_rank[obase + j];
                 if (op.type == L_RESET) {
                     cr = 0;
                     continue;
                 }
-                double* ou = (j + 1 == ops.size()) ? C.U(c)
+                double* ou = (j + 1 == nops) ? C.U(c)
                                                     : P0 + ((j & 1) ? slot1[c] : slot0[c]);
                 double* ov = ou + (long long)Cb.m * rnew;
                 const WTask& t = P.w[op.w];
                 RoundOp r{};
-                r.kind = op_kind[c][j];
+                r.kind = op_kind[obase + j];
                 r.m = Cb.m;
                 r.n = Cb.n;
                 r.alpha = 1.0;
@@ -627,7 +660,8 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
             if (!fresh)
                 gops.push_back({c_old_data.get() + c_old_off[c], nullptr, C.D(c), 1.0, 0.0, Cb.m,
                                 Cb.n, -1, Cb.m, 0, Cb.m, 0, 0});
-            for (const DOp& op : P.dops[c]) {
+            for (int j = 0; j < P.dops.size(c); ++j) {
+                const DOp& op = P.dops.of(c)[j];
                 if (op.type == D_DD) {
                     const Block& Ba = S.blocks[op.a];
                     const Block& Bb = S.blocks[op.b];

@@ -24,6 +24,7 @@ namespace {
 constexpr int kT = 256;
 constexpr int kW = kT / 32;
 constexpr int kMaxK = 128;         // largest stacked rank handled
+constexpr long long kSmemDoubles = 8192;   // 64 KB: M and J up to 64 x 64
 constexpr int kJacobiSweeps = 40;  // bounded; converges in ~6-12
 constexpr double kJacobiTol = 1e-15;
 
@@ -251,13 +252,11 @@ __device__ void do_round(const RoundOp& op, double* dyn, long long smem_doubles,
     if (m == 0 || n == 0) return;
     const int ku = ortho ? op.r1 : min(m, k);
     const int kv = dense ? n : min(n, k);
-    // Everything in shared memory when it fits (`smem_doubles`), else the
-    // core and rotations alone, else all in the global work area.
-    const long long need_f = (ortho ? 0LL : (long long)m * k) + (dense ? 0LL : (long long)n * k);
+    // The core and the rotations live in shared memory when they fit in
+    // `smem_doubles`; the stacked factors in the (L1-cached) work area.
     const long long need_mj = (long long)ku * kv + (long long)kv * kv;
-    const bool all_smem = need_f + 2 * k + need_mj <= smem_doubles;
-    const bool mj_smem = !all_smem && need_mj <= smem_doubles;
-    double* w = all_smem ? dyn : op.work;
+    const bool mj_smem = need_mj <= smem_doubles;
+    double* w = op.work;
     double* Ucat = w;
     if (!ortho) w += (long long)m * k;
     double* Vcat = w;
@@ -425,40 +424,30 @@ void launch_round_workers(Context& ctx, const std::vector<RoundOp>& ops,
         HMB_REQUIRE(k <= kMaxK, HM_ERR_UNSUPPORTED,
                     "low-rank rounding of more than 128 stacked columns");
     }
-    // Workers grouped by the shared memory their largest op can use; each
-    // group is one launch sized for it.
-    const long long classes[4] = {2048, 6144, 16384, 26624};   // doubles: 16/48/128/208 KB
-    std::vector<std::vector<int>> group(4);
+    // One launch; ops whose core and rotations fit use `kSmemDoubles` of
+    // shared memory for them, the stacked factors stay in the (L1-cached)
+    // global work area.
     const int nw = (int)begin.size() - 1;
-    for (int w = 0; w < nw; ++w) {
-        long long need = 0;
-        for (int i = begin[w]; i < begin[w + 1]; ++i) need = std::max(need, round_smem_need(ops[i]));
-        int g = 0;
-        while (g < 3 && need > classes[g]) ++g;
-        group[g].push_back(w);
-    }
+    std::vector<int> workers(nw);
+    for (int w = 0; w < nw; ++w) workers[w] = w;
     int dev = 0;
     cudaGetDevice(&dev);
     static int attr_dev = -1;
     if (attr_dev != dev) {
         HMB_CUDA(cudaFuncSetAttribute(round_worker_kernel,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(classes[3] * sizeof(double))));
+                                      (int)(kSmemDoubles * sizeof(double))));
         attr_dev = dev;
     }
     DeviceBuffer<RoundOp> d;
     d.upload(ops, ctx.stream);
-    DeviceBuffer<int> db;
+    DeviceBuffer<int> db, dw;
     db.upload(begin, ctx.stream);
-    for (int g = 0; g < 4; ++g) {
-        if (group[g].empty()) continue;
-        DeviceBuffer<int> dw;
-        dw.upload(group[g], ctx.stream);
-        LaunchScope ls(ctx, name);
-        round_worker_kernel<<<(unsigned)group[g].size(), kT, classes[g] * sizeof(double),
-                              ctx.stream>>>(d.get(), db.get(), dw.get(), classes[g]);
-        HMB_CHECK_LAUNCH();
-    }
+    dw.upload(workers, ctx.stream);
+    LaunchScope ls(ctx, name);
+    round_worker_kernel<<<(unsigned)nw, kT, kSmemDoubles * sizeof(double), ctx.stream>>>(
+        d.get(), db.get(), dw.get(), kSmemDoubles);
+    HMB_CHECK_LAUNCH();
 }
 
 void launch_qr_formq(Context& ctx, const std::vector<QrOp>& ops, const char* name) {

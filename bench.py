@@ -293,6 +293,8 @@ def gpu_arm(args):
                         for k, v in prof.items()}}
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(coef, Xh, nbytes)
+    if not args.no_schulz:
+        line["schulz"] = schulz_leg(local, rank == 0 and not args.no_cpu_baseline)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
@@ -327,6 +329,65 @@ def read_profile(ctx):
     return out
 
 
+SCHULZ = dict(sizes=(32, 32), levels=4, rank=8, oversample=4, seed=1, stop_tol=1e-8)
+
+
+def schulz_leg(device, with_reference):
+    """The Schulz half of the metric: SchulzInvert(-1, 1.5, 6, stopTol 1e-8)
+    on the 32 x 32 five-point operator (N = 1024, 16-point leaves, maxRank 8,
+    oversample 4), timed end to end on the GPU (host wall clock around the
+    synchronous call: the iteration reads one norm estimate back per step),
+    beside the reference build timed on one core for a 3-iteration sample
+    (its per-iteration cost extrapolated to the iterations the GPU ran)."""
+    import torch
+    import dmhm_b200 as D
+    sz, L, r = SCHULZ["sizes"], SCHULZ["levels"], SCHULZ["rank"]
+    coef = D.operators.uniform_coefficients(sz, SCHULZ["seed"])
+    S = D.operators.stencil(sz, coef, L)
+    ctx = D.Context(device)
+    ctx.set_oversample(SCHULZ["oversample"])
+    # warm-up on a throwaway copy (code paths, pool), then a fresh context
+    Hw = D.HMat2d(S, L, r, True, *sz, ctx=ctx)
+    Hw.SchulzInvert(2, 1.5, 6.0, SCHULZ["stop_tol"])
+    ctx.synchronize()
+    ctx2 = D.Context(device)
+    ctx2.set_oversample(SCHULZ["oversample"])
+    H = D.HMat2d(S, L, r, True, *sz, ctx=ctx2)
+    ctx2.synchronize()
+    t0 = time.perf_counter()
+    its, trace = H.SchulzInvert(-1, 1.5, 6.0, SCHULZ["stop_tol"])
+    ctx2.synchronize()
+    gpu_s = time.perf_counter() - t0
+    # attained residual ||I - X A|| on probe vectors
+    A = D.HMat2d(S, L, r, True, *sz, ctx=ctx2)
+    P = np.random.default_rng(5).standard_normal((A.Width(), 8))
+    res = np.linalg.norm(H.Multiply(1.0, A.Multiply(1.0, P)) - P) / np.linalg.norm(P)
+    out = {"workload": "SchulzInvert(-1, theta 1.5, confidence 6, stopTol 1e-8), HMat2d<double> "
+                       "32x32 five-point operator, numLevels 4, maxRank 8, oversample 4",
+           "gpu_seconds": gpu_s, "iterations": its, "final_norm_estimate": trace[-1],
+           "relative_residual_XAp_minus_p": float(res), "dtype": "f64"}
+    if with_reference and os.path.exists(REF_DRIVER):
+        with tempfile.TemporaryDirectory() as tmp:
+            cp, pp = os.path.join(tmp, "c.bin"), os.path.join(tmp, "p.bin")
+            coef.tofile(cp)
+            np.zeros(A.Width()).tofile(pp)
+            env = {**os.environ, "OPENBLAS_NUM_THREADS": "1"}
+            cmd = [REF_DRIVER, "schulz_trace", "--dim", "2", "--nx", str(sz[0]), "--ny", str(sz[1]),
+                   "--levels", str(L), "--rank", str(r), "--oversample", str(SCHULZ["oversample"]),
+                   "--coef", cp, "--x", pp, "--nrhs", "1", "--iters", "3"]
+            rr = subprocess.run(cmd, capture_output=True, text=True, env=env, check=True)
+            info = json.loads(rr.stdout.strip().splitlines()[-1])
+        per_it = float(info["seconds"]) / 3.0
+        out["cpu_reference"] = {"seconds_per_iteration": per_it,
+                                "extrapolated_seconds": per_it * its, "cores": 1,
+                                "kind": "reference",
+                                "sample": "3 fixed Schulz iterations (plus the initial norm "
+                                          "estimate) of the same operator, extrapolated to "
+                                          f"{its} iterations"}
+        out["speedup_vs_cpu_reference"] = per_it * its / gpu_s
+    return out
+
+
 def cpu_baseline(coef, X, nbytes):
     if not os.path.exists(REF_DRIVER):
         return {"value": None, "unit": "GB/s", "cores": 1, "kind": "reference",
@@ -345,6 +406,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-schulz", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)

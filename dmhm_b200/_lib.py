@@ -66,6 +66,7 @@ SIGNATURES = {
     "hm_scale": [_P, _D],
     "hm_add_constant_to_diagonal": [_P, _D],
     "hm_multiply_vector_noalloc": [_P, _I, _D, _P, _D, _P],
+    "hm_multiply_dense_tf32": [_P, _D, _P, _I, _D, _P, _I, _I],
     "hm_kernel_launches": [],
     "hm_profile_enable": [_P, _I],
     "hm_profile_read": [_P, _I, C.c_char_p, _I, _PD, _PI64],

@@ -35,6 +35,7 @@ hm_matrix_s* new_handle(hm_context_s* ctx) {
 // Releases the device storage of a handle (stream-ordered frees).
 void release_storage(hm_matrix_s* m) {
     m->h.templates.clear();
+    m->h.data32.reset();
     m->h.data.reset();
     m->h.table.reset();
 }
@@ -474,6 +475,16 @@ int hm_add_constant_to_diagonal(hm_matrix h, double alpha) {
     return guarded([&] {
         HMB_REQUIRE(h, HM_ERR_ARGUMENT, "h is NULL");
         hmat_add_diagonal(owner_of(h)->c, h->h, alpha);
+    });
+}
+
+int hm_multiply_dense_tf32(hm_matrix h, double alpha, const double* B, int ldb, double beta,
+                           double* C, int ldc, int nrhs) {
+    return guarded([&] {
+        HMB_REQUIRE(h && (nrhs == 0 || (B && C)), HM_ERR_ARGUMENT, "NULL argument");
+        owner_of(h);
+        HMB_REQUIRE(h->h.S != nullptr, HM_ERR_ARGUMENT, "empty H-matrix");
+        multiply_dense_tf32(h->h, alpha, B, ldb, beta, C, ldc, nrhs);
     });
 }
 

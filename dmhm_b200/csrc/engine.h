@@ -97,6 +97,10 @@ class HMatrix {
     long long total = 0;            // elements in `data`
     DeviceBuffer<double> data;
     DeviceBuffer<DevBlock> table;   // device copy of the per-block table
+    // FP32 copy (rounded to TF32) of `data` for the tensor-core products;
+    // made on first use, dropped whenever `data` changes.
+    DeviceBuffer<float> data32;
+    bool shadow_valid = false;
     // Cached multiply work lists keyed by (subtree root, transpose); dropped
     // whenever the storage is re-laid out.
     mutable std::map<std::pair<int, int>, std::shared_ptr<struct JobTemplate>> templates;
@@ -137,6 +141,11 @@ std::shared_ptr<JobTemplate> get_template(Context& ctx, const HMatrix& H, int ro
 // then one fused output pass per row tile).  Outputs of different jobs must
 // not overlap; inputs may alias each other but not outputs.
 void run_jobs(Context& ctx, const std::vector<MatJob>& jobs);
+
+// Tensor-core (TF32, FP32 accumulation) H-matrix x dense, device pointers;
+// at most 64 right-hand sides; synchronizes (checks the kernels' error word).
+void multiply_dense_tf32(HMatrix& H, double alpha, const double* B, int ldb, double beta,
+                         double* C, int ldc, int nrhs);
 
 // Device kernels driven from the host side (launchers).
 void launch_fill_random(Context& ctx, HMatrix& H);

@@ -14,6 +14,7 @@ namespace hmb {
 void HMatrix::layout() {
     const Structure& St = *S;
     templates.clear();
+    shadow_valid = false;
     off.assign(St.blocks.size(), -1);
     long long cur = 0;
     for (int b : St.leaves) {

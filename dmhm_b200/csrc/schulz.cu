@@ -166,6 +166,7 @@ void hmat_transpose(Context& ctx, const HMatrix& src, HMatrix& dst) {
 
 void hmat_scale(Context& ctx, HMatrix& H, double alpha) {
     const Structure& S = *H.S;
+    H.shadow_valid = false;
     if (alpha == 0.0) {
         // Scale(0, LowRank) drops the rank (hmat_tools.hpp, Scale); dense -> 0
         bool any = false;
@@ -190,6 +191,7 @@ void hmat_scale(Context& ctx, HMatrix& H, double alpha) {
 
 void hmat_add_diagonal(Context& ctx, HMatrix& H, double alpha) {
     const Structure& S = *H.S;
+    H.shadow_valid = false;
     std::vector<DiagTask> tasks;
     for (int b : S.leaves) {
         const Block& B = S.blocks[b];
@@ -303,6 +305,7 @@ SchulzResult schulz_invert(Context& ctx, HMatrix& A, int num_iterations, double 
     A.off = X->off;
     A.total = X->total;
     A.data = std::move(X->data);
+    A.shadow_valid = false;
     A.table = std::move(X->table);
     A.templates.clear();
     return res;

@@ -109,6 +109,17 @@ HM_API int hm_multiply_dense_host(hm_matrix h, int transpose, double alpha,
                            int ldc, int nrhs);
 
 /*
+ * Mixed-precision form of hm_multiply_dense (no transpose): block data read
+ * from an FP32 copy rounded to TF32 (made on first use), products on the
+ * tensor cores (tcgen05.mma kind::tf32) with FP32 accumulation, C in FP64.
+ * DEVICE pointers; nrhs <= 64 per call; synchronizes the stream.  Relative
+ * error against the FP64 product is about 1e-3 (TF32 has an 11-bit
+ * significand).  The reference computes only in the matrix's own precision.
+ */
+HM_API int hm_multiply_dense_tf32(hm_matrix h, double alpha, const double* B, int ldb,
+                                  double beta, double* C, int ldc, int nrhs);
+
+/*
  * H*H products with randomized low-rank compression.
  * hm_multiply_hmat: C := alpha A B, C rebuilt (HMat2d::Multiply(alpha,
  * const HMat2d& B, HMat2d& C), include/dmhm/hmat2d.hpp:260-263;

@@ -10,9 +10,9 @@
 //            sum_e A_e^T B_e^T over the tile's dense leaves (X rows, D rows)
 //            and low-rank blocks (T_b, U_b rows),
 // with the right-hand sides as the MMA's M dimension (M = 64), the tile rows
-// or the rank as N, and the block's inner dimension as K.  Operands are
-// staged in shared memory in the canonical no-swizzle layouts (K-major for
-// X and T, MN-major for the U / D rows); one thread issues the MMAs and
+// or the rank as N, and the block's inner dimension as K.  Both operands are
+// staged in shared memory in the canonical no-swizzle K-major layout (core
+// matrices of 8 rows x 16 bytes); one thread issues the MMAs and
 // commits them to an mbarrier; every wait on it is bounded and reports
 // through an error word instead of hanging.
 //
@@ -122,12 +122,6 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 __device__ __forceinline__ int kmaj_off(int r, int k) {
     return (r >> 3) * ((kKC / 4) * 128) + (k >> 2) * 128 + (r & 7) * 16 + (k & 3) * 4;
 }
-// MN-major (N x KC): core matrices of 4 N x 8 K; N-direction step 128 B,
-// K-direction step (N/4)*128 B.
-__device__ __forceinline__ int mnmaj_off(int n, int k, int N) {
-    return (n & 3) * 4 + (k & 7) * 16 + (n >> 2) * 128 + (k >> 3) * ((N / 4) * 128);
-}
-
 struct TcArgs {
     const double* base64;    // H-matrix FP64 storage (template pointers live here)
     const float* base32;     // its TF32-rounded FP32 copy
@@ -260,12 +254,12 @@ __global__ void __launch_bounds__(kTcThreads) tc_row_tiles_kernel(const TcArgs a
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_base;
-    const uint32_t idesc = idesc_tf32(kM, N, 0, 1);
+    const uint32_t idesc = idesc_tf32(kM, N, 0, 0);
     uint32_t phase = 0;
     bool ok = true, any = false;
     for (int ei = it.e0; ei < it.e1 && ok; ++ei) {
         const P2Entry e = a.ent[ei];
-        const float* Bsrc = to32(a, e.A);      // rows of U or D (MN-major)
+        const float* Bsrc = to32(a, e.A);      // rows of U or D (staged K-major)
         const float* Asrc;                     // T_b^T or X rows
         int lda_src;
         if (e.b_from_t) { Asrc = a.T + e.b_off * a.k; lda_src = e.ldt; }
@@ -287,7 +281,7 @@ __global__ void __launch_bounds__(kTcThreads) tc_row_tiles_kernel(const TcArgs a
                 float v = 0.f;
                 if (i < it.rows && p < inner && kk < kc)
                     v = Bsrc[(it.r0 + i) + (long long)p * e.lda];
-                sB[mnmaj_off(i, kk, N) >> 2] = v;
+                sB[kmaj_off(i, kk) >> 2] = v;
             }
             fence_async_smem();
             __syncthreads();
@@ -296,7 +290,7 @@ __global__ void __launch_bounds__(kTcThreads) tc_row_tiles_kernel(const TcArgs a
                 const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
                 for (int s = 0; s < kc / 8; ++s) {
                     const uint64_t ad = smem_desc(a0 + s * 256, 128, (kKC / 4) * 128);
-                    const uint64_t bd = smem_desc(b0 + s * ((N / 4) * 128), (N / 4) * 128, 128);
+                    const uint64_t bd = smem_desc(b0 + s * 256, 128, (kKC / 4) * 128);
                     mma_tf32(tmem, ad, bd, idesc, (any || s > 0) ? 1u : 0u);
                 }
                 mma_commit(&bar);

@@ -172,8 +172,12 @@ __device__ __forceinline__ void store_out(const JobExec& J, const P2T& it, int i
     *y = J.beta == 0.0 ? al * v : al * v + J.beta * *y;
 }
 
-// Narrow: columns <= NC, rows <= 64.  Lanes map to (row, inner sub-lane);
-// warps split the inner dimension; partial sums reduced through shared memory.
+// Narrow: columns <= NC, rows <= 64, a streaming (HBM-bound) kernel.  The
+// tile's entries are concatenated along the inner dimension (entry e covers
+// columns [cbeg, cbeg + inner)), and the columns are split evenly among
+// "column workers" (sub-groups of lanes; lanes within a worker own rows).
+// Each worker keeps four columns of loads in flight; partial sums are
+// reduced over workers through shuffles and shared memory.
 template <int NC>
 __global__ void __launch_bounds__(kThreads)
 p2_narrow_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0) {
@@ -185,7 +189,7 @@ p2_narrow_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0
     const int cols = min(NC, J.k - c0);
     __shared__ double red[kWarps][64][NC];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // rows-per-pass RL (power of two <= 32), inner sub-lanes 32/RL
+    // rows-per-pass RL (power of two <= 32), column sub-groups 32/RL per warp
     int RL = 1;
     while (RL < it.rows && RL < 32) RL <<= 1;
     const int sub = lane / RL, rl = lane % RL, nsub = 32 / RL;
@@ -195,29 +199,64 @@ p2_narrow_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0
     for (int a = 0; a < 2; ++a)
 #pragma unroll
         for (int c = 0; c < NC; ++c) acc[a][c] = 0.0;
-    for (int ei = it.e0; ei < it.e1; ++ei) {
-        const P2Entry e = J.ent[ei];
-        const double* EB;
-        int ldb;
-        entry_b(e, J, EB, ldb);
-        const int stride = kWarps * nsub;
-        for (int p = warp * nsub + sub; p < e.inner; p += stride) {
-            double b[NC];
+    if (it.e1 > it.e0) {
+        const P2Entry last = J.ent[it.e1 - 1];
+        const int total = last.cbeg + last.inner;
+        const int nworkers = kWarps * nsub;
+        const int worker = warp * nsub + sub;
+        const int chunk = (total + nworkers - 1) / nworkers;
+        int p = worker * chunk;
+        const int pend = min(total, p + chunk);
+        int ei = it.e0;
+        while (ei + 1 < it.e1 && J.ent[ei + 1].cbeg <= p) ++ei;
+        while (p < pend) {
+            const P2Entry e = J.ent[ei];
+            const double* EB;
+            int ldb;
+            entry_b(e, J, EB, ldb);
+            const int stop = min(pend, e.cbeg + e.inner);
+            int q = p - e.cbeg;                 // column within the entry
+            const int qstop = stop - e.cbeg;
+            for (; q + 3 < qstop; q += 4) {
+                double av[2][4], bv[4][NC];
 #pragma unroll
-            for (int c = 0; c < NC; ++c)
-                b[c] = (c < cols) ? __ldg(EB + p + (long long)(c0 + c) * ldb) : 0.0;
+                for (int u = 0; u < 4; ++u) {
 #pragma unroll
-            for (int a = 0; a < 2; ++a) {
-                int i = rl + a * RL;
-                if (a < rpt && i < it.rows) {
-                    double av = load_a(e, it.r0 + i, p);
+                    for (int c = 0; c < NC; ++c)
+                        bv[u][c] = (c < cols) ? __ldg(EB + (q + u) + (long long)(c0 + c) * ldb) : 0.0;
 #pragma unroll
-                    for (int c = 0; c < NC; ++c) acc[a][c] = fma(av, b[c], acc[a][c]);
+                    for (int a = 0; a < 2; ++a) {
+                        const int i = rl + a * RL;
+                        av[a][u] = (a < rpt && i < it.rows) ? load_a(e, it.r0 + i, q + u) : 0.0;
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+#pragma unroll
+                    for (int a = 0; a < 2; ++a)
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) acc[a][c] = fma(av[a][u], bv[u][c], acc[a][c]);
+            }
+            for (; q < qstop; ++q) {
+                double b[NC];
+#pragma unroll
+                for (int c = 0; c < NC; ++c)
+                    b[c] = (c < cols) ? __ldg(EB + q + (long long)(c0 + c) * ldb) : 0.0;
+#pragma unroll
+                for (int a = 0; a < 2; ++a) {
+                    const int i = rl + a * RL;
+                    if (a < rpt && i < it.rows) {
+                        const double av = load_a(e, it.r0 + i, q);
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) acc[a][c] = fma(av, b[c], acc[a][c]);
+                    }
                 }
             }
+            p = stop;
+            ++ei;
         }
     }
-    // reduce over sub-lanes within the warp (lanes with equal rl)
+    // reduce over the column sub-groups within the warp (lanes with equal rl)
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
@@ -389,6 +428,7 @@ std::shared_ptr<JobTemplate> build_template(Context& ctx, const HMatrix& H, int 
         const Box& cl = S.boxes[S.leaf_box[c]];
         if (cl.count == 0) continue;
         const int e0 = (int)ent.size();
+        int cbeg = 0;
         for (int bi = count[c - c0]; bi < count[c - c0 + 1]; ++bi) {
             const int li = bucket[bi];
             const int b = leaves[li];
@@ -424,6 +464,8 @@ std::shared_ptr<JobTemplate> build_template(Context& ctx, const HMatrix& H, int 
                 e.b_off = t_rel[li];
                 e.ldt = H.rank[b];
             }
+            e.cbeg = cbeg;
+            cbeg += e.inner;
             ent.push_back(e);
         }
         const int e1 = (int)ent.size();

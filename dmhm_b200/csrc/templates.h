@@ -21,7 +21,8 @@ struct P2T {
 struct P2Entry {
     const double* A;   // element (i,p) = transA ? A[p + i*lda] : A[i + p*lda]
     long long b_off;   // b_from_t ? T + b_off * k (ld ldt) : job input + b_off
-    int lda, inner, transA, b_from_t, ldt, pad;
+    int lda, inner, transA, b_from_t, ldt;
+    int cbeg;          // first column of this entry in its tile's concatenation
 };
 
 struct JobTemplate {

@@ -8,6 +8,7 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "common.h"
@@ -103,7 +104,7 @@ class HMatrix {
     bool shadow_valid = false;
     // Cached multiply work lists keyed by (subtree root, transpose); dropped
     // whenever the storage is re-laid out.
-    mutable std::map<std::pair<int, int>, std::shared_ptr<struct JobTemplate>> templates;
+    mutable std::map<std::tuple<int, int, int>, std::shared_ptr<struct JobTemplate>> templates;
 
     int height() const { return S->N; }
     int width() const { return S->N; }
@@ -135,7 +136,9 @@ struct MatJob {
 // Work lists of one subtree (root, op) of one H-matrix, kept on the device
 // (matmul.cu).  Cached per H-matrix; dropped when its storage is re-laid out.
 struct JobTemplate;
-std::shared_ptr<JobTemplate> get_template(Context& ctx, const HMatrix& H, int root, bool trans);
+// Row tiles of the output hold at most `row_tile` rows (<= 64).
+std::shared_ptr<JobTemplate> get_template(Context& ctx, const HMatrix& H, int root, bool trans,
+                                          int row_tile = 64);
 
 // Runs a batch of jobs as two level-batched launches (low-rank inner products,
 // then one fused output pass per row tile).  Outputs of different jobs must

@@ -75,17 +75,16 @@ p1_narrow_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0
 #pragma unroll
         for (int c = 0; c < NC; ++c) acc[c] = 0.0;
         int p = lane;
-        for (; p + 96 < it.nin; p += 128) {
-            double w0 = __ldg(w + p), w1 = __ldg(w + p + 32);
-            double w2 = __ldg(w + p + 64), w3 = __ldg(w + p + 96);
+        for (; p + 224 < it.nin; p += 256) {   // eight loads of W in flight per lane
+            double wv[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) wv[u] = __ldg(w + p + 32 * u);
 #pragma unroll
             for (int c = 0; c < NC; ++c) {
                 if (c < K) {
                     const double* x = in + (long long)c * ldin + p;
-                    acc[c] = fma(w0, __ldg(x), acc[c]);
-                    acc[c] = fma(w1, __ldg(x + 32), acc[c]);
-                    acc[c] = fma(w2, __ldg(x + 64), acc[c]);
-                    acc[c] = fma(w3, __ldg(x + 96), acc[c]);
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) acc[c] = fma(wv[u], __ldg(x + 32 * u), acc[c]);
                 }
             }
         }
@@ -176,7 +175,7 @@ __device__ __forceinline__ void store_out(const JobExec& J, const P2T& it, int i
 // tile's entries are concatenated along the inner dimension (entry e covers
 // columns [cbeg, cbeg + inner)), and the columns are split evenly among
 // "column workers" (sub-groups of lanes; lanes within a worker own rows).
-// Each worker keeps four columns of loads in flight; partial sums are
+// Each worker keeps eight columns of loads in flight; partial sums are
 // reduced over workers through shuffles and shared memory.
 template <int NC>
 __global__ void __launch_bounds__(kThreads)
@@ -217,10 +216,10 @@ p2_narrow_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0
             const int stop = min(pend, e.cbeg + e.inner);
             int q = p - e.cbeg;                 // column within the entry
             const int qstop = stop - e.cbeg;
-            for (; q + 3 < qstop; q += 4) {
-                double av[2][4], bv[4][NC];
+            for (; q + 7 < qstop; q += 8) {
+                double av[2][8], bv[8][NC];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
+                for (int u = 0; u < 8; ++u) {
 #pragma unroll
                     for (int c = 0; c < NC; ++c)
                         bv[u][c] = (c < cols) ? __ldg(EB + (q + u) + (long long)(c0 + c) * ldb) : 0.0;
@@ -231,7 +230,7 @@ p2_narrow_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0
                     }
                 }
 #pragma unroll
-                for (int u = 0; u < 4; ++u)
+                for (int u = 0; u < 8; ++u)
 #pragma unroll
                     for (int a = 0; a < 2; ++a)
 #pragma unroll
@@ -352,11 +351,9 @@ p2_wide_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0) 
     }
 }
 
-constexpr int kRowTile = 64;
-
 // Work lists of one subtree of one H-matrix.
 std::shared_ptr<JobTemplate> build_template(Context& ctx, const HMatrix& H, int root,
-                                            bool trans) {
+                                            bool trans, int row_tile) {
     HostScope hs(ctx, "hmm_template");
     const Structure& S = *H.S;
     const Block& R = S.blocks[root];
@@ -469,11 +466,11 @@ std::shared_ptr<JobTemplate> build_template(Context& ctx, const HMatrix& H, int 
             ent.push_back(e);
         }
         const int e1 = (int)ent.size();
-        for (int r0 = 0; r0 < cl.count; r0 += kRowTile) {
+        for (int r0 = 0; r0 < cl.count; r0 += row_tile) {
             P2T it{};
             it.out_off = cl.offset - outBase;
             it.r0 = r0;
-            it.rows = std::min(kRowTile, cl.count - r0);
+            it.rows = std::min(row_tile, cl.count - r0);
             it.e0 = e0;
             it.e1 = e1;
             p2.push_back(it);
@@ -490,11 +487,13 @@ std::shared_ptr<JobTemplate> build_template(Context& ctx, const HMatrix& H, int 
 
 }  // namespace
 
-std::shared_ptr<JobTemplate> get_template(Context& ctx, const HMatrix& H, int root, bool trans) {
-    auto key = std::make_pair(root, trans ? 1 : 0);
+std::shared_ptr<JobTemplate> get_template(Context& ctx, const HMatrix& H, int root, bool trans,
+                                          int row_tile) {
+    HMB_REQUIRE(row_tile >= 1 && row_tile <= 64, HM_ERR_INTERNAL, "row tile out of range");
+    auto key = std::make_tuple(root, trans ? 1 : 0, row_tile);
     auto it = H.templates.find(key);
     if (it != H.templates.end()) return it->second;
-    auto T = build_template(ctx, H, root, trans);
+    auto T = build_template(ctx, H, root, trans, row_tile);
     H.templates.emplace(key, T);
     return T;
 }
@@ -508,8 +507,10 @@ void run_jobs(Context& ctx, const std::vector<MatJob>& jobs) {
     for (const MatJob& J : jobs) {
         HMB_REQUIRE(J.k >= 0, HM_ERR_ARGUMENT, "negative column count");
         kmax = std::max(kmax, J.k);
-        tmpl.push_back(get_template(ctx, *J.H, J.root, J.trans));
     }
+    // streaming (few right-hand sides): 32-row tiles for more CTAs in flight
+    const int row_tile = kmax <= 8 ? 32 : 64;
+    for (const MatJob& J : jobs) tmpl.push_back(get_template(ctx, *J.H, J.root, J.trans, row_tile));
     const bool wide = kmax > 8;
     const int NC2 = kmax <= 1 ? 1 : kmax <= 4 ? 4 : kmax <= 8 ? 8 : 64;
     long long t_total = 0;

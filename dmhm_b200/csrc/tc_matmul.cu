@@ -232,18 +232,27 @@ __global__ void __launch_bounds__(kTcThreads) tc_lowrank_inner_kernel(const TcAr
 // ---------------------------------------------------------------------------
 // Phase 2: Y_tile^T (k x rows) = sum_e A_e^T B_e^T, one CTA per row tile.
 // ---------------------------------------------------------------------------
+// Each template row tile (<= 64 rows) is split over gridDim.y CTAs of
+// kTileRows rows: more CTAs in flight per SM, the small A operands (T_b, X
+// rows) re-read from L2.
+constexpr int kTileRows = 16;
+
 __global__ void __launch_bounds__(kTcThreads) tc_row_tiles_kernel(const TcArgs a) {
-    constexpr int N = 64;                      // tile rows (zero-padded)
+    constexpr int N = kTileRows;               // MMA N: tile rows (zero-padded)
+    constexpr int kCols = 32;                  // TMEM columns allocated (minimum 32)
     __shared__ __align__(128) float sA[kM * kKC];
     __shared__ __align__(128) float sB[N * kKC];
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t tmem_base;
-    const P2T it = a.p2[blockIdx.x];
+    P2T it = a.p2[blockIdx.x];
+    it.r0 += kTileRows * blockIdx.y;
+    it.rows = min(kTileRows, it.rows - kTileRows * (int)blockIdx.y);
+    if (it.rows <= 0) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_u32(&tmem_base)),
-                     "r"(N));
+                     "r"(kCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (threadIdx.x == 0) {
@@ -321,7 +330,8 @@ __global__ void __launch_bounds__(kTcThreads) tc_row_tiles_kernel(const TcArgs a
     tc_fence_before();
     __syncthreads();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(N));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(kCols));
 }
 
 __global__ void to_tf32_kernel(const double* __restrict__ src, float* __restrict__ dst,
@@ -405,7 +415,7 @@ void multiply_dense_tf32(HMatrix& H, double alpha, const double* B, int ldb, dou
     }
     if (T->n2 > 0) {
         LaunchScope ls(ctx, "tc_row_tiles");
-        tc_row_tiles_kernel<<<T->n2, kTcThreads, 0, st>>>(a);
+        tc_row_tiles_kernel<<<dim3(T->n2, 64 / kTileRows), kTcThreads, 0, st>>>(a);
         HMB_CHECK_LAUNCH();
     }
     int h_err = 0;

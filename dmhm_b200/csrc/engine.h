@@ -42,6 +42,12 @@ struct Context {
     struct Totals { double ms = 0; long long launches = 0; };
     std::map<std::string, Totals> totals;
     void collect();   // synchronizes, folds pending event pairs into totals
+
+    // Completion counters of the split-work kernels: all zero between
+    // launches (each user resets what it counted).  Returns >= n of them.
+    int* zeroed_counters(long long n);
+    DeviceBuffer<int> counters;
+    long long counters_cap = 0;
 };
 
 // Host-side wall time of a phase, recorded under `name` when profiling.

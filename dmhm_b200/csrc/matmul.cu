@@ -9,7 +9,9 @@
 // input.  Each (H-matrix, root, op) has a template -- its work lists, built
 // once and kept on the device -- and a batch of jobs runs as two launches:
 //   phase 1: T_b = W_b^T X_b for every low-rank block b of every job
-//            (W = V, or U for the transpose), one CTA per block;
+//            (W = V, or U for the transpose): for few columns one warp per
+//            row segment of a block, whole blocks per CTA; otherwise one
+//            CTA per block and 32-column tile;
 //   phase 2: for every output row tile of every job, Y_tile = alpha * (sum
 //            over the dense leaves and low-rank blocks covering the tile of
 //            A_e(tile rows) * B_e) + beta * Y_tile, one CTA per tile, so each
@@ -18,6 +20,8 @@
 // its job by binary search over the jobs' first work-item indices.
 #include <algorithm>
 #include <cstring>
+#include <map>
+#include <mutex>
 
 #include "engine.h"
 #include "templates.h"
@@ -32,9 +36,11 @@ struct JobExec {
     const double* in;
     double* out;
     double* T;
+    int* cnt1;           // per item: pieces finished (zero between launches)
+    int* cnt2;           // per row tile: pieces finished
     const double* alpha_scale;
     double alpha, beta;
-    long long p1_begin, p2_begin;   // first global work item of this job
+    long long p1_begin, p2_begin;   // first global work item (row / column) of this job
     int n1, n2, ldin, ldout, k, ct1, ct2, pad;   // ct*: column tiles per item
 };
 
@@ -58,49 +64,136 @@ __device__ __forceinline__ int find_job(const JobExec* jobs, int njobs, long lon
 // ---------------------------------------------------------------------------
 // Phase 1: T = W^T in
 // ---------------------------------------------------------------------------
-// Narrow: k <= NC.  Warps take columns of W; lanes stride over rows.
+// Sum of v[f] over the 32 lanes for 16 values at once (a transposing
+// butterfly: 16 shuffles instead of 80).  Lanes 2f and 2f+1 end up holding
+// the total of value f in v[0].
+__device__ __forceinline__ void warp_transpose_sum16(double (&v)[16], int lane) {
+#pragma unroll
+    for (int h = 8, o = 16; h >= 1; h >>= 1, o >>= 1) {
+        const bool up = (lane & o) != 0;
+#pragma unroll
+        for (int i = 0; i < h; ++i) {
+            const double send = up ? v[i] : v[i + h];
+            const double keep = up ? v[i + h] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+    }
+    v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
+}
+
+// Even split of a concatenation of C work items (rows of the phase-1 items,
+// columns of the phase-2 tiles, over all jobs) among GW <= C warps: warp w
+// takes [w C / GW, (w+1) C / GW), never empty.  An item or tile cut between
+// warps wa..wb is summed by the piece that finishes last (a counter per item
+// or tile, reset by that piece), over the warps in order; warp w leaves the
+// partial sum of its first piece in scratch slot 2w, of its last in 2w + 1.
+__device__ __forceinline__ long long split_start(long long w, long long GW, long long C) {
+    return w * C / GW;
+}
+__device__ __forceinline__ long long split_owner(long long g, long long GW, long long C) {
+    return ((g + 1) * GW + C - 1) / C - 1;
+}
+__device__ __forceinline__ long long piece_slot(long long q, long long wa, bool wa_starts_here) {
+    return 2 * q + ((q == wa && !wa_starts_here) ? 1 : 0);
+}
+
+// Narrow: k <= NC.  Persistent warps stream their share of the items' rows.
+// A lane owns rows p and p + 32 of a 64-row step and loads JC = 16/NC columns
+// of W for both (2 JC loads in flight); the 16 partial sums of a column chunk
+// are reduced across the warp by a transposing butterfly.
 template <int NC>
-__global__ void __launch_bounds__(kThreads)
-p1_narrow_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0) {
-    const long long gi = blockIdx.x;
-    const JobExec& J = jobs ? jobs[find_job(jobs, njobs, gi, false)] : job0;
-    const P1T it = J.p1[gi - J.p1_begin];
-    const double* in = J.in + it.in_off;
-    double* T = J.T + it.t_rel * J.k;
-    const int K = J.k, ldin = J.ldin;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int j = warp; j < it.r; j += kWarps) {
-        const double* w = it.W + (long long)j * it.ldw;
-        double acc[NC];
-#pragma unroll
-        for (int c = 0; c < NC; ++c) acc[c] = 0.0;
-        int p = lane;
-        for (; p + 224 < it.nin; p += 256) {   // eight loads of W in flight per lane
-            double wv[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u) wv[u] = __ldg(w + p + 32 * u);
-#pragma unroll
-            for (int c = 0; c < NC; ++c) {
-                if (c < K) {
-                    const double* x = in + (long long)c * ldin + p;
-#pragma unroll
-                    for (int u = 0; u < 8; ++u) acc[c] = fma(wv[u], __ldg(x + 32 * u), acc[c]);
-                }
+__global__ void __launch_bounds__(kThreads, 2)
+p1_stream_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0, long long C,
+                 long long GW, double* __restrict__ S, int rmax,
+                 const int* __restrict__ start) {
+    constexpr int JC = 16 / NC;
+    const int lane = threadIdx.x & 31;
+    const long long w = (long long)blockIdx.x * kWarps + (threadIdx.x >> 5);
+    if (w >= GW) return;
+    const long long slot_len = (long long)rmax * NC;
+    long long g = split_start(w, GW, C);
+    const long long gend = split_start(w + 1, GW, C);
+    bool first = true;
+    // one job with precomputed starts: items follow one another
+    const bool seq = jobs == nullptr && start != nullptr;
+    int item = seq ? start[w] - 1 : 0;
+    while (g < gend) {
+        const JobExec& J = jobs ? jobs[find_job(jobs, njobs, g, false)] : job0;
+        const long long local = g - J.p1_begin;
+        if (seq) {
+            ++item;
+        } else {
+            item = 0;
+            int hi = J.n1 - 1;
+            while (item < hi) {
+                const int mid = (item + hi + 1) >> 1;
+                if (J.p1[mid].c0 <= local) item = mid;
+                else hi = mid - 1;
             }
         }
-        for (; p < it.nin; p += 32) {
-            double w0 = __ldg(w + p);
+        const P1T it = J.p1[item];
+        if (item + 1 < J.n1) asm volatile("prefetch.global.L1 [%0];" ::"l"(J.p1 + item + 1));
+        const int K = J.k, ldin = J.ldin, r = it.r;
+        const int p0 = (int)(local - it.c0);
+        const int p1 = (int)min((long long)it.nin, gend - J.p1_begin - it.c0);
+        const bool whole = p0 == 0 && p1 == it.nin;
+        double* dst = whole ? J.T + it.t_rel * K : S + (2 * w + (first ? 0 : 1)) * slot_len;
+        const double* in = J.in + it.in_off;
+        for (int j0 = 0; j0 < r; j0 += JC) {
+            double v[16];
 #pragma unroll
-            for (int c = 0; c < NC; ++c)
-                if (c < K) acc[c] = fma(w0, __ldg(in + (long long)c * ldin + p), acc[c]);
+            for (int f = 0; f < 16; ++f) v[f] = 0.0;
+            const double* wp = it.W + (long long)j0 * it.ldw;
+            for (int pa = p0 + lane; pa < p1; pa += 64) {
+                const int pb = pa + 32;
+                const bool okb = pb < p1;
+                double wa[JC], wb[JC], xa[NC], xb[NC];
+#pragma unroll
+                for (int jj = 0; jj < JC; ++jj) {
+                    const bool cj = j0 + jj < r;
+                    wa[jj] = cj ? __ldg(wp + pa + (long long)jj * it.ldw) : 0.0;
+                    wb[jj] = (okb && cj) ? __ldg(wp + pb + (long long)jj * it.ldw) : 0.0;
+                }
+#pragma unroll
+                for (int c = 0; c < NC; ++c) {
+                    xa[c] = (c < K) ? __ldg(in + pa + (long long)c * ldin) : 0.0;
+                    xb[c] = (okb && c < K) ? __ldg(in + pb + (long long)c * ldin) : 0.0;
+                }
+#pragma unroll
+                for (int jj = 0; jj < JC; ++jj)
+#pragma unroll
+                    for (int c = 0; c < NC; ++c)
+                        v[jj * NC + c] = fma(wb[jj], xb[c], fma(wa[jj], xa[c], v[jj * NC + c]));
+            }
+            warp_transpose_sum16(v, lane);
+            if ((lane & 1) == 0) {
+                const int f = lane >> 1, jj = f / NC, c = f % NC;
+                if (j0 + jj < r && c < K) dst[(j0 + jj) + (long long)c * r] = v[0];
+            }
         }
-#pragma unroll
-        for (int c = 0; c < NC; ++c) {
-            double v = acc[c];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0 && c < K) T[j + (long long)c * it.r] = v;
+        if (!whole) {
+            __threadfence();
+            __syncwarp();
+            const long long G0 = J.p1_begin + it.c0;
+            const long long wa = split_owner(G0, GW, C), wb = split_owner(G0 + it.nin - 1, GW, C);
+            int last = 0;
+            if (lane == 0) last = atomicAdd(J.cnt1 + item, 1) == (int)(wb - wa);
+            last = __shfl_sync(0xffffffffu, last, 0);
+            if (last) {
+                __threadfence();
+                const bool wa_here = split_start(wa, GW, C) == G0;
+                double* T = J.T + it.t_rel * K;
+                for (int o = lane; o < r * K; o += 32) {
+                    double t = 0.0;
+                    for (long long q = wa; q <= wb; ++q)
+                        t += __ldcg(S + piece_slot(q, wa, wa_here) * slot_len + o);
+                    T[o] = t;
+                }
+                if (lane == 0) J.cnt1[item] = 0;
+            }
         }
+        g = J.p1_begin + it.c0 + p1;
+        first = false;
     }
 }
 
@@ -171,115 +264,161 @@ __device__ __forceinline__ void store_out(const JobExec& J, const P2T& it, int i
     *y = J.beta == 0.0 ? al * v : al * v + J.beta * *y;
 }
 
-// Narrow: columns <= NC, rows <= 64, a streaming (HBM-bound) kernel.  The
-// tile's entries are concatenated along the inner dimension (entry e covers
-// columns [cbeg, cbeg + inner)), and the columns are split evenly among
-// "column workers" (sub-groups of lanes; lanes within a worker own rows).
-// Each worker keeps eight columns of loads in flight; partial sums are
-// reduced over workers through shuffles and shared memory.
+// Narrow: columns <= NC, rows <= 32, a streaming (HBM-bound) kernel.
+// Persistent warps stream their share of the tiles' concatenated inner
+// dimensions (entry e of a tile covers [cbeg, cbeg + inner)).  Within a
+// warp, "column workers" (sub-groups of lanes, one lane per row) split the
+// piece evenly and keep U columns of loads in flight.
 template <int NC>
-__global__ void __launch_bounds__(kThreads)
-p2_narrow_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0) {
-    const long long gi = blockIdx.x;
-    const JobExec& J = jobs ? jobs[find_job(jobs, njobs, gi, true)] : job0;
-    const long long local = gi - J.p2_begin;
-    const P2T it = J.p2[local / J.ct2];
-    const int c0 = (int)(local % J.ct2) * NC;
-    const int cols = min(NC, J.k - c0);
-    __shared__ double red[kWarps][64][NC];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // rows-per-pass RL (power of two <= 32), column sub-groups 32/RL per warp
-    int RL = 1;
-    while (RL < it.rows && RL < 32) RL <<= 1;
-    const int sub = lane / RL, rl = lane % RL, nsub = 32 / RL;
-    const int rpt = (it.rows + RL - 1) / RL;   // rows per thread (<= 2)
-    double acc[2][NC];
+__global__ void __launch_bounds__(kThreads, 2)
+p2_stream_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0, long long C,
+                 long long GW, double* __restrict__ S, const int2* __restrict__ start) {
+    constexpr int U = NC == 1 ? 16 : 4;
+    const int lane = threadIdx.x & 31;
+    const long long w = (long long)blockIdx.x * kWarps + (threadIdx.x >> 5);
+    if (w >= GW) return;
+    constexpr long long slot_len = 32LL * NC;
+    long long g = split_start(w, GW, C);
+    const long long gend = split_start(w + 1, GW, C);
+    bool first = true;
+    // one job with precomputed starts: tiles follow one another
+    const bool seq = jobs == nullptr && start != nullptr;
+    int tile = 0, ent_first = -1;
+    if (seq) {
+        const int2 s0 = start[w];
+        tile = s0.x;
+        ent_first = s0.y;
+    }
+    while (g < gend) {
+        const JobExec& J = jobs ? jobs[find_job(jobs, njobs, g, true)] : job0;
+        const long long local = g - J.p2_begin;
+        P2T it;
+        if (seq) {
+            if (!first) {
+                do { it = J.p2[++tile]; } while (it.width == 0);
+            } else {
+                it = J.p2[tile];
+            }
+        } else {
+            tile = 0;
+            int hi = J.n2 - 1;
+            while (tile < hi) {
+                const int mid = (tile + hi + 1) >> 1;
+                if (J.p2[mid].c0 <= local) tile = mid;
+                else hi = mid - 1;
+            }
+            it = J.p2[tile];
+        }
+        const int cols = J.k;
+        const int q0 = (int)(local - it.c0);
+        const int q1 = (int)min((long long)it.width, gend - J.p2_begin - it.c0);
+        const bool whole = q0 == 0 && q1 == it.width;
+        // rows-per-pass RL (power of two <= 32), column sub-groups 32/RL
+        int RL = 1;
+        while (RL < it.rows && RL < 32) RL <<= 1;
+        const int sub = lane / RL, rl = lane % RL, nsub = 32 / RL;
+        const bool row_ok = rl < it.rows;
+        const int row = it.r0 + rl;
+        double acc[NC];
 #pragma unroll
-    for (int a = 0; a < 2; ++a)
+        for (int c = 0; c < NC; ++c) acc[c] = 0.0;
+        {
+            const int chunk = (q1 - q0 + nsub - 1) / nsub;
+            int p = q0 + sub * chunk;
+            const int pend = min(q1, p + chunk);
+            int ei = it.e0;
+            if (seq && nsub == 1) {
+                if (first) ei = ent_first;
+            } else {
+                int hi = it.e1 - 1;
+                while (ei < hi) {
+                    const int mid = (ei + hi + 1) >> 1;
+                    if (J.ent[mid].cbeg <= p) ei = mid;
+                    else hi = mid - 1;
+                }
+            }
+            while (p < pend) {
+                const P2Entry e = J.ent[ei];
+                if (ei + 1 < it.e1) asm volatile("prefetch.global.L1 [%0];" ::"l"(J.ent + ei + 1));
+                const double* EB;
+                int ldb;
+                entry_b(e, J, EB, ldb);
+                const int stop = min(pend, e.cbeg + e.inner);
+                int q = p - e.cbeg;                 // column within the entry
+                const int qstop = stop - e.cbeg;
+                for (; q + U - 1 < qstop; q += U) {
+                    double av[U], bv[U][NC];
 #pragma unroll
-        for (int c = 0; c < NC; ++c) acc[a][c] = 0.0;
-    if (it.e1 > it.e0) {
-        const P2Entry last = J.ent[it.e1 - 1];
-        const int total = last.cbeg + last.inner;
-        const int nworkers = kWarps * nsub;
-        const int worker = warp * nsub + sub;
-        const int chunk = (total + nworkers - 1) / nworkers;
-        int p = worker * chunk;
-        const int pend = min(total, p + chunk);
-        int ei = it.e0;
-        while (ei + 1 < it.e1 && J.ent[ei + 1].cbeg <= p) ++ei;
-        while (p < pend) {
-            const P2Entry e = J.ent[ei];
-            const double* EB;
-            int ldb;
-            entry_b(e, J, EB, ldb);
-            const int stop = min(pend, e.cbeg + e.inner);
-            int q = p - e.cbeg;                 // column within the entry
-            const int qstop = stop - e.cbeg;
-            for (; q + 7 < qstop; q += 8) {
-                double av[2][8], bv[8][NC];
+                    for (int u = 0; u < U; ++u) {
 #pragma unroll
-                for (int u = 0; u < 8; ++u) {
+                        for (int c = 0; c < NC; ++c)
+                            bv[u][c] = (c < cols) ? __ldg(EB + (q + u) + (long long)c * ldb) : 0.0;
+                        av[u] = row_ok ? load_a(e, row, q + u) : 0.0;
+                    }
+#pragma unroll
+                    for (int u = 0; u < U; ++u)
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) acc[c] = fma(av[u], bv[u][c], acc[c]);
+                }
+                for (; q < qstop; ++q) {
+                    const double av = row_ok ? load_a(e, row, q) : 0.0;
 #pragma unroll
                     for (int c = 0; c < NC; ++c)
-                        bv[u][c] = (c < cols) ? __ldg(EB + (q + u) + (long long)(c0 + c) * ldb) : 0.0;
-#pragma unroll
-                    for (int a = 0; a < 2; ++a) {
-                        const int i = rl + a * RL;
-                        av[a][u] = (a < rpt && i < it.rows) ? load_a(e, it.r0 + i, q + u) : 0.0;
-                    }
+                        if (c < cols) acc[c] = fma(av, __ldg(EB + q + (long long)c * ldb), acc[c]);
                 }
-#pragma unroll
-                for (int u = 0; u < 8; ++u)
-#pragma unroll
-                    for (int a = 0; a < 2; ++a)
-#pragma unroll
-                        for (int c = 0; c < NC; ++c) acc[a][c] = fma(av[a][u], bv[u][c], acc[a][c]);
+                p = stop;
+                ++ei;
             }
-            for (; q < qstop; ++q) {
-                double b[NC];
-#pragma unroll
-                for (int c = 0; c < NC; ++c)
-                    b[c] = (c < cols) ? __ldg(EB + q + (long long)(c0 + c) * ldb) : 0.0;
-#pragma unroll
-                for (int a = 0; a < 2; ++a) {
-                    const int i = rl + a * RL;
-                    if (a < rpt && i < it.rows) {
-                        const double av = load_a(e, it.r0 + i, q);
-#pragma unroll
-                        for (int c = 0; c < NC; ++c) acc[a][c] = fma(av, b[c], acc[a][c]);
-                    }
-                }
-            }
-            p = stop;
-            ++ei;
         }
-    }
-    // reduce over the column sub-groups within the warp (lanes with equal rl)
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
+        // reduce over the column sub-groups (lanes with equal rl)
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
-            double v = acc[a][c];
+            double v = acc[c];
             for (int o = 16; o >= RL; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            acc[a][c] = v;
+            acc[c] = v;
         }
-    if (sub == 0) {
+        if (whole) {
+            if (sub == 0 && row_ok)
 #pragma unroll
-        for (int a = 0; a < 2; ++a) {
-            int i = rl + a * RL;
-            if (a < rpt && i < it.rows)
+                for (int c = 0; c < NC; ++c)
+                    if (c < cols) store_out(J, it, rl, c, acc[c]);
+        } else {
+            double* P = S + (2 * w + (first ? 0 : 1)) * slot_len;   // 32 x NC, ld 32
+            if (sub == 0 && row_ok)
 #pragma unroll
-                for (int c = 0; c < NC; ++c) red[warp][i][c] = acc[a][c];
+                for (int c = 0; c < NC; ++c)
+                    if (c < cols) P[rl + 32 * c] = acc[c];
+            __threadfence();
+            __syncwarp();
+            const long long G0 = J.p2_begin + it.c0;
+            const long long wa = split_owner(G0, GW, C), wb = split_owner(G0 + it.width - 1, GW, C);
+            int last = 0;
+            if (lane == 0) last = atomicAdd(J.cnt2 + tile, 1) == (int)(wb - wa);
+            last = __shfl_sync(0xffffffffu, last, 0);
+            if (last) {
+                __threadfence();
+                const bool wa_here = split_start(wa, GW, C) == G0;
+                for (int o = lane; o < it.rows * cols; o += 32) {
+                    const int i = o % it.rows, c = o / it.rows;
+                    double t = 0.0;
+                    for (long long q = wa; q <= wb; ++q)
+                        t += __ldcg(S + piece_slot(q, wa, wa_here) * slot_len + i + 32 * c);
+                    store_out(J, it, i, c, t);
+                }
+                if (lane == 0) J.cnt2[tile] = 0;
+            }
         }
+        g = J.p2_begin + it.c0 + q1;
+        first = false;
     }
-    __syncthreads();
-    for (int o = threadIdx.x; o < it.rows * cols; o += kThreads) {
-        int i = o % it.rows, c = o / it.rows;
-        double v = 0.0;
-#pragma unroll
-        for (int w = 0; w < kWarps; ++w) v += red[w][i][c];
-        store_out(J, it, i, c0 + c, v);
+}
+
+// Row tiles without entries: output = beta * output (alpha times an empty sum).
+__global__ void p2_zero_kernel(const JobExec J, const int* __restrict__ tiles, int n) {
+    for (int t = blockIdx.x; t < n; t += gridDim.x) {
+        const P2T it = J.p2[tiles[t]];
+        for (int o = threadIdx.x; o < it.rows * J.k; o += blockDim.x)
+            store_out(J, it, o % it.rows, o / it.rows, 0.0);
     }
 }
 
@@ -399,6 +538,13 @@ std::shared_ptr<JobTemplate> build_template(Context& ctx, const HMatrix& H, int 
         t_rows += it.r;
         p1.push_back(it);
     }
+    long long c1 = 0;
+    int rmax = 0;
+    for (P1T& it : p1) {
+        it.c0 = c1;
+        c1 += it.nin;
+        rmax = std::max(rmax, it.r);
+    }
     // phase 2: bucket the leaves by the output clusters they cover
     const Box& outBox = S.boxes[trans ? R.src_box : R.tgt_box];
     const int outBase = trans ? R.col_off : R.row_off;
@@ -421,6 +567,8 @@ std::shared_ptr<JobTemplate> build_template(Context& ctx, const HMatrix& H, int 
     }
     std::vector<P2T> p2;
     std::vector<P2Entry> ent;
+    std::vector<int> zero;
+    long long c2 = 0;
     for (int c = outBox.leaf0; c < outBox.leaf1; ++c) {
         const Box& cl = S.boxes[S.leaf_box[c]];
         if (cl.count == 0) continue;
@@ -473,15 +621,27 @@ std::shared_ptr<JobTemplate> build_template(Context& ctx, const HMatrix& H, int 
             it.rows = std::min(row_tile, cl.count - r0);
             it.e0 = e0;
             it.e1 = e1;
+            it.c0 = c2;
+            it.width = cbeg;
+            c2 += cbeg;
+            if (cbeg == 0) zero.push_back((int)p2.size());
             p2.push_back(it);
         }
     }
     T->n1 = (int)p1.size();
     T->n2 = (int)p2.size();
     T->t_rows = t_rows;
+    T->nz = (int)zero.size();
+    T->c1 = c1;
+    T->c2 = c2;
+    T->rmax = rmax;
     T->p1.upload(p1, ctx.stream);
     T->p2.upload(p2, ctx.stream);
     T->ent.upload(ent, ctx.stream);
+    T->zero_tiles.upload(zero, ctx.stream);
+    T->hp1 = std::move(p1);
+    T->hp2 = std::move(p2);
+    T->hent = std::move(ent);
     return T;
 }
 
@@ -494,8 +654,104 @@ std::shared_ptr<JobTemplate> get_template(Context& ctx, const HMatrix& H, int ro
     auto it = H.templates.find(key);
     if (it != H.templates.end()) return it->second;
     auto T = build_template(ctx, H, root, trans, row_tile);
+    HMB_REQUIRE((T->n1 == 0 || T->p1.get()) && (T->n2 == 0 || (T->p2.get() && T->ent.get())) &&
+                    (T->nz == 0 || T->zero_tiles.get()),
+                HM_ERR_INTERNAL, "work lists missing on the device");
     H.templates.emplace(key, T);
     return T;
+}
+
+namespace {
+
+// Resident CTAs of a persistent kernel (occupancy x SMs), cached per kernel.
+template <typename K>
+int persistent_grid(const Context& ctx, K kernel) {
+    static std::mutex mu;
+    static std::map<const void*, int> per_sm;
+    std::lock_guard<std::mutex> lock(mu);
+    int& n = per_sm[(const void*)kernel];
+    if (n == 0) {
+        HMB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, kThreads, 0));
+        n = std::max(1, n);
+    }
+    return n * ctx.num_sms;
+}
+
+// First item of every warp of the narrow phase-1 kernel for split width GW.
+const int* warp_starts1(Context& ctx, JobTemplate& T, long long GW) {
+    auto f = T.start1.find(GW);
+    if (f != T.start1.end()) return f->second.get();
+    std::vector<int> st((size_t)GW);
+    int item = 0;
+    for (long long w = 0; w < GW; ++w) {
+        const long long g = w * T.c1 / GW;
+        while (item + 1 < (int)T.hp1.size() && T.hp1[item + 1].c0 <= g) ++item;
+        st[(size_t)w] = item;
+    }
+    DeviceBuffer<int>& d = T.start1[GW];
+    d.upload(st, ctx.stream);
+    return d.get();
+}
+
+// First (tile, entry) of every warp of the narrow phase-2 kernel.
+const int2* warp_starts2(Context& ctx, JobTemplate& T, long long GW) {
+    auto f = T.start2.find(GW);
+    if (f != T.start2.end()) return f->second.get();
+    std::vector<int2> st((size_t)GW);
+    int tile = 0;
+    for (long long w = 0; w < GW; ++w) {
+        const long long g = w * T.c2 / GW;
+        while (tile + 1 < (int)T.hp2.size() && T.hp2[tile + 1].c0 <= g) ++tile;
+        const P2T& it = T.hp2[tile];
+        int e = it.e0;
+        while (e + 1 < it.e1 && T.hent[e + 1].cbeg <= g - it.c0) ++e;
+        st[(size_t)w] = make_int2(tile, e);
+    }
+    DeviceBuffer<int2>& d = T.start2[GW];
+    d.upload(st, ctx.stream);
+    return d.get();
+}
+
+template <int NC>
+void launch_narrow(Context& ctx, const JobExec* jobs_d, int nj, const JobExec& job0,
+                   long long c1, long long c2, int rmax, JobTemplate* single) {
+    cudaStream_t st = ctx.stream;
+    if (c1 > 0) {
+        const long long g = std::min<long long>(ceil_div(c1, kWarps),
+                                                persistent_grid(ctx, p1_stream_kernel<NC>));
+        const long long GW = std::min<long long>(g * kWarps, c1);
+        const int* starts = single ? warp_starts1(ctx, *single, GW) : nullptr;
+        DeviceBuffer<double> S;
+        S.allocate((size_t)(2 * GW * rmax * NC), st);
+        LaunchScope ls(ctx, "hmm_lowrank_inner");
+        p1_stream_kernel<NC><<<(unsigned)g, kThreads, 0, st>>>(jobs_d, nj, job0, c1, GW, S.get(),
+                                                               rmax, starts);
+        HMB_CHECK_LAUNCH();
+    }
+    if (c2 > 0) {
+        const long long g = std::min<long long>(ceil_div(c2, kWarps),
+                                                persistent_grid(ctx, p2_stream_kernel<NC>));
+        const long long GW = std::min<long long>(g * kWarps, c2);
+        const int2* starts = single ? warp_starts2(ctx, *single, GW) : nullptr;
+        DeviceBuffer<double> S;
+        S.allocate((size_t)(2 * GW * 32 * NC), st);
+        LaunchScope ls(ctx, "hmm_row_tiles");
+        p2_stream_kernel<NC><<<(unsigned)g, kThreads, 0, st>>>(jobs_d, nj, job0, c2, GW, S.get(),
+                                                               starts);
+        HMB_CHECK_LAUNCH();
+    }
+}
+
+}  // namespace
+
+int* Context::zeroed_counters(long long n) {
+    if (n > counters_cap) {
+        const long long cap = std::max<long long>(n, 2 * counters_cap);
+        counters.allocate((size_t)cap, stream);
+        HMB_CUDA(cudaMemsetAsync(counters.get(), 0, (size_t)cap * sizeof(int), stream));
+        counters_cap = cap;
+    }
+    return counters.get();
 }
 
 void run_jobs(Context& ctx, const std::vector<MatJob>& jobs) {
@@ -508,25 +764,35 @@ void run_jobs(Context& ctx, const std::vector<MatJob>& jobs) {
         HMB_REQUIRE(J.k >= 0, HM_ERR_ARGUMENT, "negative column count");
         kmax = std::max(kmax, J.k);
     }
-    // streaming (few right-hand sides): 32-row tiles for more CTAs in flight
-    const int row_tile = kmax <= 8 ? 32 : 64;
-    for (const MatJob& J : jobs) tmpl.push_back(get_template(ctx, *J.H, J.root, J.trans, row_tile));
+    // streaming (few right-hand sides): 32-row tiles, work split evenly
+    // over all resident warps
     const bool wide = kmax > 8;
+    const int row_tile = wide ? 64 : 32;
+    for (const MatJob& J : jobs) tmpl.push_back(get_template(ctx, *J.H, J.root, J.trans, row_tile));
     const int NC2 = kmax <= 1 ? 1 : kmax <= 4 ? 4 : kmax <= 8 ? 8 : 64;
-    long long t_total = 0;
-    std::vector<long long> t_off(jobs.size());
+    long long t_total = 0, c_total = 0;
+    std::vector<long long> t_off(jobs.size()), c1_off(jobs.size()), c2_off(jobs.size());
     for (size_t j = 0; j < jobs.size(); ++j) {
+        const JobTemplate& T = *tmpl[j];
         t_off[j] = t_total;
-        t_total += tmpl[j]->t_rows * jobs[j].k;
+        t_total += T.t_rows * jobs[j].k;
+        c1_off[j] = c_total;
+        c_total += T.n1;
+        c2_off[j] = c_total;
+        c_total += T.n2;
     }
     DeviceBuffer<double> tbuf;
     tbuf.allocate((size_t)std::max<long long>(t_total, 1), st);
+    int* cnt = wide ? nullptr : ctx.zeroed_counters(std::max<long long>(c_total, 1));
     std::vector<JobExec> ex;
     ex.reserve(jobs.size());
     long long n1 = 0, n2 = 0;
+    int rmax = 0;
+    size_t first_job = 0;
     for (size_t j = 0; j < jobs.size(); ++j) {
         const MatJob& J = jobs[j];
         if (J.k == 0) continue;
+        if (ex.empty()) first_job = j;
         const JobTemplate& T = *tmpl[j];
         JobExec e{};
         e.p1 = T.p1.get();
@@ -535,6 +801,10 @@ void run_jobs(Context& ctx, const std::vector<MatJob>& jobs) {
         e.in = J.in;
         e.out = J.out;
         e.T = tbuf.get() + t_off[j];
+        if (!wide) {
+            e.cnt1 = cnt + c1_off[j];
+            e.cnt2 = cnt + c2_off[j];
+        }
         e.alpha_scale = J.alpha_scale;
         e.alpha = J.alpha;
         e.beta = J.beta;
@@ -544,15 +814,15 @@ void run_jobs(Context& ctx, const std::vector<MatJob>& jobs) {
         e.n1 = T.n1;
         e.n2 = T.n2;
         e.ct1 = wide ? ceil_div(J.k, 32) : 1;
-        e.ct2 = ceil_div(J.k, NC2);
+        e.ct2 = wide ? ceil_div(J.k, NC2) : 1;
         e.p1_begin = n1;
         e.p2_begin = n2;
-        n1 += (long long)T.n1 * e.ct1;
-        n2 += (long long)T.n2 * e.ct2;
+        n1 += wide ? (long long)T.n1 * e.ct1 : T.c1;
+        n2 += wide ? (long long)T.n2 * e.ct2 : T.c2;
+        rmax = std::max(rmax, T.rmax);
         ex.push_back(e);
     }
     if (ex.empty()) return;
-    HMB_REQUIRE(n1 < (1LL << 31) && n2 < (1LL << 31), HM_ERR_UNSUPPORTED, "batch too large");
     DeviceBuffer<JobExec> dex;
     const JobExec* jobs_d = nullptr;
     if (ex.size() > 1) {
@@ -561,22 +831,34 @@ void run_jobs(Context& ctx, const std::vector<MatJob>& jobs) {
     }
     const JobExec job0 = ex[0];
     const int nj = (int)ex.size();
+    if (!wide) {
+        JobTemplate* single = nj == 1 ? tmpl[first_job].get() : nullptr;
+        if (kmax <= 1) launch_narrow<1>(ctx, jobs_d, nj, job0, n1, n2, rmax, single);
+        else if (kmax <= 4) launch_narrow<4>(ctx, jobs_d, nj, job0, n1, n2, rmax, single);
+        else launch_narrow<8>(ctx, jobs_d, nj, job0, n1, n2, rmax, single);
+        size_t j = 0;
+        for (size_t i = 0; i < jobs.size(); ++i) {
+            if (jobs[i].k == 0) continue;
+            const JobTemplate& T = *tmpl[i];
+            if (T.nz > 0) {
+                LaunchScope ls(ctx, "hmm_zero_tiles");
+                p2_zero_kernel<<<std::min(T.nz, 4 * ctx.num_sms), 256, 0, st>>>(
+                    ex[j], T.zero_tiles.get(), T.nz);
+                HMB_CHECK_LAUNCH();
+            }
+            ++j;
+        }
+        return;
+    }
+    HMB_REQUIRE(n1 < (1LL << 31) && n2 < (1LL << 31), HM_ERR_UNSUPPORTED, "batch too large");
     if (n1 > 0) {
         LaunchScope ls(ctx, "hmm_lowrank_inner");
-        const unsigned g = (unsigned)n1;
-        if (kmax <= 1) p1_narrow_kernel<1><<<g, kThreads, 0, st>>>(jobs_d, nj, job0);
-        else if (kmax <= 4) p1_narrow_kernel<4><<<g, kThreads, 0, st>>>(jobs_d, nj, job0);
-        else if (kmax <= 8) p1_narrow_kernel<8><<<g, kThreads, 0, st>>>(jobs_d, nj, job0);
-        else p1_wide_kernel<<<g, kThreads, 0, st>>>(jobs_d, nj, job0);
+        p1_wide_kernel<<<(unsigned)n1, kThreads, 0, st>>>(jobs_d, nj, job0);
         HMB_CHECK_LAUNCH();
     }
     if (n2 > 0) {
         LaunchScope ls(ctx, "hmm_row_tiles");
-        const unsigned g = (unsigned)n2;
-        if (kmax <= 1) p2_narrow_kernel<1><<<g, kThreads, 0, st>>>(jobs_d, nj, job0);
-        else if (kmax <= 4) p2_narrow_kernel<4><<<g, kThreads, 0, st>>>(jobs_d, nj, job0);
-        else if (kmax <= 8) p2_narrow_kernel<8><<<g, kThreads, 0, st>>>(jobs_d, nj, job0);
-        else p2_wide_kernel<<<g, kThreads, 0, st>>>(jobs_d, nj, job0);
+        p2_wide_kernel<<<(unsigned)n2, kThreads, 0, st>>>(jobs_d, nj, job0);
         HMB_CHECK_LAUNCH();
     }
 }

@@ -1,6 +1,9 @@
 // Device work lists of one subtree of one H-matrix (see matmul.cu), shared
 // by the FP64 and the tensor-core H-matrix x dense products.
 #pragma once
+#include <map>
+#include <vector>
+
 #include "engine.h"
 
 namespace hmb {
@@ -10,12 +13,16 @@ struct P1T {
     const double* W;   // nin x r, ld ldw
     long long in_off;  // row offset into the job input
     long long t_rel;   // T_b = T + t_rel * k (r x k, ld r)
+    long long c0;      // first row of this item in the concatenation of all items' rows
     int nin, r, ldw, pad;
 };
 
 struct P2T {
     long long out_off;  // row offset of the tile's first row in the job output
+    long long c0;       // first column of this tile in the concatenation of all tiles
     int r0, rows, e0, e1;
+    int width;          // columns of the tile's concatenation (sum of its entries' inner)
+    int pad;
 };
 
 struct P2Entry {
@@ -29,7 +36,17 @@ struct JobTemplate {
     DeviceBuffer<P1T> p1;
     DeviceBuffer<P2T> p2;
     DeviceBuffer<P2Entry> ent;
-    int n1 = 0, n2 = 0;
+    DeviceBuffer<int> zero_tiles;   // tiles without entries (output = beta * output)
+    // Host copies, and per split width GW the first item / (tile, entry) of
+    // every warp of the narrow kernels (built on first use).
+    std::vector<P1T> hp1;
+    std::vector<P2T> hp2;
+    std::vector<P2Entry> hent;
+    std::map<long long, DeviceBuffer<int>> start1;
+    std::map<long long, DeviceBuffer<int2>> start2;
+    int n1 = 0, n2 = 0, nz = 0;
+    long long c1 = 0, c2 = 0;       // rows of all items, columns of all tiles
+    int rmax = 0;                   // largest rank among the items
     long long t_rows = 0;   // sum of the ranks: T holds t_rows * k entries
 };
 

@@ -233,6 +233,7 @@ int hm_context_destroy(hm_context ctx) {
         ctx->live.clear();
         ctx->c.collect();
         ctx->c.counters.reset();
+        ctx->c.errword.reset();
         cudaStreamSynchronize(ctx->c.stream);
         if (ctx->c.own_stream) cudaStreamDestroy(ctx->c.stream);
         delete ctx;

@@ -48,6 +48,9 @@ struct Context {
     int* zeroed_counters(long long n);
     DeviceBuffer<int> counters;
     long long counters_cap = 0;
+    // Device word set by kernels whose bounded waits gave up (zero = fine).
+    int* error_word();
+    DeviceBuffer<int> errword;
 };
 
 // Host-side wall time of a phase, recorded under `name` when profiling.
@@ -150,6 +153,9 @@ std::shared_ptr<JobTemplate> get_template(Context& ctx, const HMatrix& H, int ro
 // then one fused output pass per row tile).  Outputs of different jobs must
 // not overlap; inputs may alias each other but not outputs.
 void run_jobs(Context& ctx, const std::vector<MatJob>& jobs);
+// One-vector product of one job streamed block by block (matvec.cu); false
+// when the matrix does not fit that kernel (the caller uses run_jobs' lists).
+bool multiply_vector_streamed(Context& ctx, const MatJob& job);
 
 // Tensor-core (TF32, FP32 accumulation) H-matrix x dense, device pointers;
 // at most 64 right-hand sides; synchronizes (checks the kernels' error word).

@@ -568,6 +568,7 @@ std::shared_ptr<JobTemplate> build_template(Context& ctx, const HMatrix& H, int 
     std::vector<P2T> p2;
     std::vector<P2Entry> ent;
     std::vector<int> zero;
+    std::vector<int> ent_block;
     long long c2 = 0;
     for (int c = outBox.leaf0; c < outBox.leaf1; ++c) {
         const Box& cl = S.boxes[S.leaf_box[c]];
@@ -612,6 +613,7 @@ std::shared_ptr<JobTemplate> build_template(Context& ctx, const HMatrix& H, int 
             e.cbeg = cbeg;
             cbeg += e.inner;
             ent.push_back(e);
+            ent_block.push_back(b);
         }
         const int e1 = (int)ent.size();
         for (int r0 = 0; r0 < cl.count; r0 += row_tile) {
@@ -642,6 +644,7 @@ std::shared_ptr<JobTemplate> build_template(Context& ctx, const HMatrix& H, int 
     T->hp1 = std::move(p1);
     T->hp2 = std::move(p2);
     T->hent = std::move(ent);
+    T->hent_block = std::move(ent_block);
     return T;
 }
 
@@ -744,6 +747,14 @@ void launch_narrow(Context& ctx, const JobExec* jobs_d, int nj, const JobExec& j
 
 }  // namespace
 
+int* Context::error_word() {
+    if (!errword.get()) {
+        errword.allocate(1, stream);
+        HMB_CUDA(cudaMemsetAsync(errword.get(), 0, sizeof(int), stream));
+    }
+    return errword.get();
+}
+
 int* Context::zeroed_counters(long long n) {
     if (n > counters_cap) {
         const long long cap = std::max<long long>(n, 2 * counters_cap);
@@ -764,6 +775,8 @@ void run_jobs(Context& ctx, const std::vector<MatJob>& jobs) {
         HMB_REQUIRE(J.k >= 0, HM_ERR_ARGUMENT, "negative column count");
         kmax = std::max(kmax, J.k);
     }
+    // one vector, one job: stream the blocks (matvec.cu)
+    if (jobs.size() == 1 && jobs[0].k == 1 && multiply_vector_streamed(ctx, jobs[0])) return;
     // streaming (few right-hand sides): 32-row tiles, work split evenly
     // over all resident warps
     const bool wide = kmax > 8;

@@ -2,6 +2,7 @@
 // by the FP64 and the tensor-core H-matrix x dense products.
 #pragma once
 #include <map>
+#include <memory>
 #include <vector>
 
 #include "engine.h"
@@ -42,6 +43,11 @@ struct JobTemplate {
     std::vector<P1T> hp1;
     std::vector<P2T> hp2;
     std::vector<P2Entry> hent;
+    std::vector<int> hent_block;    // leaf block of every entry
+    // Block-streamed one-vector product plan (matvec.cu); null when the
+    // blocks do not fit its limits.
+    std::shared_ptr<struct MvPlan> mv;
+    bool mv_tried = false;
     std::map<long long, DeviceBuffer<int>> start1;
     std::map<long long, DeviceBuffer<int2>> start2;
     int n1 = 0, n2 = 0, nz = 0;

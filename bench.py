@@ -291,6 +291,8 @@ def gpu_arm(args):
             "wall_ms_per_step": wall * 1e3 / args.steps,
             "kernels": {k: {"ms_per_launch": v["ms"] / v["launches"], "launches": v["launches"]}
                         for k, v in prof.items()}}
+    line["matvec"] = matvec_leg(ctx, H, stream, census, hbm_peak, peak_kind, args)
+    line["tf32"] = tf32_leg(ctx, H, stream, X, Y, NRHS, nbytes, args)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(coef, Xh, nbytes)
     if not args.no_schulz:
@@ -300,6 +302,95 @@ def gpu_arm(args):
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def _time_steps(stream, fn, steps):
+    import torch
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        fn()
+    ev1.record(stream)
+    ev1.synchronize()
+    return ev0.elapsed_time(ev1) / steps
+
+
+def matvec_leg(ctx, H, stream, census, hbm_peak, peak_kind, args):
+    """One-vector product y = H x (FP64), the HBM-bound form of the hot
+    path: GB/s of algorithmic bytes (every stored block once, x and y), the
+    dominant kernel's roofline from per-launch CUDA events, and the relative
+    difference of H^T applied through the same kernels against a dense-free
+    check (x^T (H y) = (H^T x)^T y)."""
+    import ctypes as C
+    import torch
+    from dmhm_b200 import _lib
+    lib = _lib.lib()
+    N = H.Height()
+    x = torch.tensor(np.random.default_rng(SEED + 3).standard_normal(N), device="cuda")
+    y = torch.empty(N, dtype=torch.float64, device="cuda")
+
+    def mv(trans=0, src=x, dst=y):
+        _lib.check(lib.hm_multiply_dense(H.handle, trans, 1.0, C.c_void_p(src.data_ptr()), N, 0.0,
+                                         C.c_void_p(dst.data_ptr()), N, 1))
+
+    for _ in range(max(3, args.warmup)):
+        mv()
+    ctx.synchronize()
+    steps = max(20, args.steps)
+    ms = _time_steps(stream, mv, steps)
+    nbytes = census["bytes"] + 2 * N * 8
+    _lib.check(lib.hm_profile_enable(ctx.handle, 1))
+    for _ in range(steps):
+        mv()
+    prof = read_profile(ctx)
+    _lib.check(lib.hm_profile_enable(ctx.handle, 0))
+    kname, kv = max(prof.items(), key=lambda kv: kv[1]["ms"])
+    kms = kv["ms"] / kv["launches"]
+    kbytes = census["bytes"] + N * 8
+    # adjoint identity as a size-independent check of the streamed kernels
+    z = torch.tensor(np.random.default_rng(SEED + 4).standard_normal(N), device="cuda")
+    w = torch.empty_like(z)
+    mv(0, x, y)
+    mv(1, z, w)
+    ctx.synchronize()
+    lhs, rhs = float(torch.dot(z, y)), float(torch.dot(w, x))
+    return {"metric": "H-matvec GB/s (FP64, one vector)", "value": nbytes / (ms * 1e-3) / 1e9,
+            "unit": "GB/s", "ms_per_step": ms, "steps": steps,
+            "frac_of_hbm": nbytes / (ms * 1e-3) / 1e9 / hbm_peak,
+            "roofline": {"bound": "hbm", "kernel": kname,
+                         "achieved": kbytes / (kms * 1e-3) / 1e9, "peak": hbm_peak,
+                         "unit": "GB/s", "frac": kbytes / (kms * 1e-3) / 1e9 / hbm_peak,
+                         "peak_source": peak_kind, "algorithmic_bytes_per_launch": kbytes},
+            "adjoint_identity_rel_diff": abs(lhs - rhs) / max(abs(lhs), 1e-300),
+            "kernels": {k: {"ms_per_launch": v["ms"] / v["launches"], "launches": v["launches"]}
+                        for k, v in prof.items()}}
+
+
+def tf32_leg(ctx, H, stream, X, Y, nrhs, nbytes, args):
+    """The same 64-right-hand-side product on the tensor cores (TF32 inputs,
+    FP32 accumulation): GB/s of the FP64 algorithmic bytes and the relative
+    error against the FP64 product."""
+    import ctypes as C
+    import torch
+    from dmhm_b200 import _lib
+    lib = _lib.lib()
+    N = H.Height()
+    Y2 = torch.empty_like(Y)
+
+    def mm():
+        _lib.check(lib.hm_multiply_dense_tf32(H.handle, 1.0, C.c_void_p(X.data_ptr()), N, 0.0,
+                                              C.c_void_p(Y2.data_ptr()), N, nrhs))
+
+    for _ in range(max(3, args.warmup)):
+        mm()
+    ctx.synchronize()
+    ms = _time_steps(stream, mm, max(5, args.steps))
+    _lib.check(lib.hm_multiply_dense(H.handle, 0, 1.0, C.c_void_p(X.data_ptr()), N, 0.0,
+                                     C.c_void_p(Y.data_ptr()), N, nrhs))
+    ctx.synchronize()
+    err = float((Y2 - Y).norm() / Y.norm())
+    return {"value": nbytes / (ms * 1e-3) / 1e9, "unit": "GB/s", "ms_per_step": ms,
+            "rel_err_vs_fp64": err, "dtype": "tf32 inputs, f32 accumulation"}
 
 
 def kernel_bytes(name, census, N, nrhs, H):

@@ -31,6 +31,8 @@ namespace hmb {
 // What a CTA needs to run its share of one job.
 struct JobExec {
     const P1T* p1;
+    const W1Tile* w1;
+    double* part;        // wide phase-2 partials of split tiles
     const P2T* p2;
     const P2Entry* ent;
     const double* in;
@@ -194,51 +196,6 @@ p1_stream_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0
         }
         g = J.p1_begin + it.c0 + p1;
         first = false;
-    }
-}
-
-// Wide: any k.  Output tile 32 (r) x 32 (k) per CTA column-tile; inner dim
-// staged through shared memory in chunks of 32.
-__global__ void __launch_bounds__(kThreads)
-p1_wide_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0) {
-    const long long gi = blockIdx.x;
-    const JobExec& J = jobs ? jobs[find_job(jobs, njobs, gi, false)] : job0;
-    const long long local = gi - J.p1_begin;
-    const P1T it = J.p1[local / J.ct1];
-    const int c0 = (int)(local % J.ct1) * 32;
-    const double* in = J.in + it.in_off;
-    double* T = J.T + it.t_rel * J.k;
-    const int K = J.k, ldin = J.ldin;
-    if (c0 >= K) return;
-    __shared__ double sW[32][33];
-    __shared__ double sX[32][33];
-    const int tid = threadIdx.x;
-    const int tj = tid & 31;          // output row within tile
-    const int tc = (tid >> 5) * 4;    // 4 consecutive output columns
-    for (int j0 = 0; j0 < it.r; j0 += 32) {
-        double acc[4] = {0, 0, 0, 0};
-        for (int p0 = 0; p0 < it.nin; p0 += 32) {
-            for (int e = tid; e < 32 * 32; e += kThreads) {
-                int pp = e & 31, jj = e >> 5;
-                int p = p0 + pp, j = j0 + jj, c = c0 + jj;
-                sW[jj][pp] = (p < it.nin && j < it.r) ? it.W[p + (long long)j * it.ldw] : 0.0;
-                sX[jj][pp] = (p < it.nin && c < K) ? in[p + (long long)c * ldin] : 0.0;
-            }
-            __syncthreads();
-#pragma unroll 8
-            for (int pp = 0; pp < 32; ++pp) {
-                double w = sW[tj][pp];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) acc[u] = fma(w, sX[tc + u][pp], acc[u]);
-            }
-            __syncthreads();
-        }
-        int j = j0 + tj;
-        if (j < it.r)
-            for (int u = 0; u < 4; ++u) {
-                int c = c0 + tc + u;
-                if (c < K) T[j + (long long)c * it.r] = acc[u];
-            }
     }
 }
 
@@ -422,72 +379,224 @@ __global__ void p2_zero_kernel(const JobExec J, const int* __restrict__ tiles, i
     }
 }
 
-// Wide: tile 64 rows x 64 cols, inner staged in chunks of 16; each thread
-// owns a 4x4 register tile.
-__global__ void __launch_bounds__(kThreads)
-p2_wide_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0) {
+// ---------------------------------------------------------------------------
+// Wide (many columns): FP64 64 x 64 output tiles, 128 threads, 8 x 4 outputs
+// a thread; operands staged through shared memory in chunks of KC inner
+// indices by cp.async, two stages (the next chunk loads while this one is
+// multiplied).
+// ---------------------------------------------------------------------------
+constexpr int WT = kWideTile;   // tile rows = tile columns
+constexpr int KC = 16;          // inner chunk
+constexpr int WTHREADS = 128;   // 8 row groups x 16 column lanes
+constexpr int SP = WT + 1;      // padded smem row (conflict-free transposing stores)
+
+struct WideSmem {
+    double a[2][KC][SP];   // a[buf][p][i] = A(i, p)
+    double b[2][KC][SP];   // b[buf][p][c] = B(p, c)
+};
+
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src),
+                 "r"(valid ? 8 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// acc[a][b] += sum_p A(tr*8+a, p) B(p, tc+16b) over one staged chunk.
+__device__ __forceinline__ void wide_mma(const WideSmem& sm, int buf, int tr, int tc,
+                                         double (&acc)[8][4]) {
+#pragma unroll 4
+    for (int p = 0; p < KC; ++p) {
+        double av[8], bv[4];
+#pragma unroll
+        for (int a = 0; a < 8; ++a) av[a] = sm.a[buf][p][tr * 8 + a];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) bv[b] = sm.b[buf][p][tc + 16 * b];
+#pragma unroll
+        for (int a = 0; a < 8; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+    }
+}
+
+// B chunk: B(p, c) = Bp[p + c * ldb] for p < len, c < cols (p fastest).
+__device__ __forceinline__ void load_b_chunk(WideSmem& sm, int buf, const double* Bp, int ldb,
+                                             int len, int cols, int tid) {
+#pragma unroll
+    for (int e = tid; e < KC * WT; e += WTHREADS) {
+        const int p = e % KC, c = e / KC;
+        const bool v = p < len && c < cols;
+        cp_async8(&sm.b[buf][p][c], v ? Bp + p + (long long)c * ldb : Bp, v);
+    }
+}
+
+__global__ void __launch_bounds__(WTHREADS)
+w1_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0) {
+    __shared__ WideSmem sm;
+    __shared__ const double* wcol[WT];
+    const long long gi = blockIdx.x;
+    const JobExec& J = jobs ? jobs[find_job(jobs, njobs, gi, false)] : job0;
+    const W1Tile* tile = J.w1 + (gi - J.p1_begin);
+    const int tid = threadIdx.x, tr = tid >> 4, tc = tid & 15;
+    const int c0 = blockIdx.y * WT;
+    const int cols = min(WT, J.k - c0);
+    if (cols <= 0) return;
+    const int rows = tile->rows, K = tile->nin;
+    for (int i = tid; i < WT; i += WTHREADS) wcol[i] = i < rows ? tile->wcol[i] : tile->wcol[0];
+    __syncthreads();
+    const double* X = J.in + tile->in_off + (long long)c0 * J.ldin;
+    auto load = [&](int q, int buf) {
+        const int p0 = q * KC, len = min(KC, K - p0);
+#pragma unroll
+        for (int e = tid; e < WT * KC; e += WTHREADS) {
+            const int p = e % KC, i = e / KC;   // p fastest: W columns are contiguous
+            const bool v = p < len && i < rows;
+            cp_async8(&sm.a[buf][p][i], v ? wcol[i] + p0 + p : wcol[0], v);
+        }
+        load_b_chunk(sm, buf, X + p0, J.ldin, len, cols, tid);
+        cp_async_commit();
+    };
+    double acc[8][4];
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+    const int nq = (K + KC - 1) / KC;
+    if (nq > 0) load(0, 0);
+    for (int q = 0; q < nq; ++q) {
+        if (q + 1 < nq) {
+            load(q + 1, (q + 1) & 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        wide_mma(sm, q & 1, tr, tc, acc);
+        __syncthreads();
+    }
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        const int i = tr * 8 + a;
+        if (i >= rows) continue;
+        double* t = J.T + tile->trel[i] * J.k + tile->tj[i];
+        const int st = tile->tr[i];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int c = tc + 16 * b;
+            if (c < cols) t[(long long)(c0 + c) * st] = acc[a][b];
+        }
+    }
+}
+
+// Phase-2 tile of the wide path: Y_tile = alpha sum_e A_e B_e + beta Y_tile,
+// the tile's concatenated inner dimension cut into `S` pieces (one CTA each);
+// with S > 1 every piece leaves a 64 x 64 partial and the last piece of the
+// tile adds them up in piece order (a counter per tile and column tile).
+__global__ void __launch_bounds__(WTHREADS)
+w2_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0, int S) {
+    __shared__ WideSmem sm;
+    __shared__ int last_flag;
     const long long gi = blockIdx.x;
     const JobExec& J = jobs ? jobs[find_job(jobs, njobs, gi, true)] : job0;
     const long long local = gi - J.p2_begin;
-    const P2T it = J.p2[local / J.ct2];
-    const int c0 = (int)(local % J.ct2) * 64;
-    const int cols = min(64, J.k - c0);
-    __shared__ double sA[16][64 + 1];
-    __shared__ double sB[16][64 + 1];
-    const int tid = threadIdx.x;
-    const int tr = (tid & 15) * 4;   // rows tr..tr+3
-    const int tc = (tid >> 4) * 4;   // cols tc..tc+3
-    double acc[4][4];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-    for (int ei = it.e0; ei < it.e1; ++ei) {
+    const int tile = (int)(local / S), s = (int)(local % S);
+    const P2T it = J.p2[tile];
+    const int tid = threadIdx.x, tr = tid >> 4, tc = tid & 15;
+    const int c0 = blockIdx.y * WT;
+    const int cols = min(WT, J.k - c0);
+    if (cols <= 0) return;
+    const int q0 = (int)((long long)it.width * s / S), q1 = (int)((long long)it.width * (s + 1) / S);
+    // chunk cursor: entry ei, position pos (concatenation index)
+    int ei = it.e0;
+    while (ei + 1 < it.e1 && J.ent[ei + 1].cbeg <= q0) ++ei;
+    int pos = q0;
+    auto load = [&](int buf) {
         const P2Entry e = J.ent[ei];
+        const int pin = pos - e.cbeg;   // position within the entry
+        const int len = min(KC, min(e.cbeg + e.inner, q1) - pos);
+        if (!e.transA) {
+            const double* A = e.A + it.r0 + (long long)pin * e.lda;
+#pragma unroll
+            for (int x = tid; x < WT * KC; x += WTHREADS) {
+                const int i = x % WT, p = x / WT;   // rows contiguous
+                const bool v = p < len && i < it.rows;
+                cp_async8(&sm.a[buf][p][i], v ? A + i + (long long)p * e.lda : e.A, v);
+            }
+        } else {
+            const double* A = e.A + pin + (long long)it.r0 * e.lda;
+#pragma unroll
+            for (int x = tid; x < WT * KC; x += WTHREADS) {
+                const int p = x % KC, i = x / KC;   // inner index contiguous
+                const bool v = p < len && i < it.rows;
+                cp_async8(&sm.a[buf][p][i], v ? A + p + (long long)i * e.lda : e.A, v);
+            }
+        }
         const double* EB;
         int ldb;
         entry_b(e, J, EB, ldb);
-        for (int p0 = 0; p0 < e.inner; p0 += 16) {
-            for (int x = tid; x < 16 * 64; x += kThreads) {
-                int i, pp;
-                if (e.transA) { pp = x & 15; i = x >> 4; }
-                else { i = x & 63; pp = x >> 6; }
-                int p = p0 + pp;
-                sA[pp][i] = (i < it.rows && p < e.inner) ? load_a(e, it.r0 + i, p) : 0.0;
-            }
-            for (int x = tid; x < 16 * 64; x += kThreads) {
-                int pp = x & 15, c = x >> 4;
-                int p = p0 + pp;
-                sB[pp][c] = (c < cols && p < e.inner)
-                                ? __ldg(EB + p + (long long)(c0 + c) * ldb) : 0.0;
-            }
-            __syncthreads();
-#pragma unroll 4
-            for (int pp = 0; pp < 16; ++pp) {
-                double av[4], bv[4];
+        load_b_chunk(sm, buf, EB + pin + (long long)c0 * ldb, ldb, len, cols, tid);
+        cp_async_commit();
+        pos += len;
+        if (pos >= e.cbeg + e.inner) ++ei;
+    };
+    double acc[8][4];
 #pragma unroll
-                for (int a = 0; a < 4; ++a) av[a] = sA[pp][tr + a];
+    for (int a = 0; a < 8; ++a)
 #pragma unroll
-                for (int b = 0; b < 4; ++b) bv[b] = sB[pp][tc + b];
-#pragma unroll
-                for (int a = 0; a < 4; ++a)
-#pragma unroll
-                    for (int b = 0; b < 4; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
-            }
-            __syncthreads();
+        for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+    const bool any = q1 > q0;
+    if (any) load(0);
+    for (int buf = 0; any; buf ^= 1) {
+        const bool more = pos < q1;
+        if (more) {
+            load(buf ^ 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
         }
+        __syncthreads();
+        wide_mma(sm, buf, tr, tc, acc);
+        __syncthreads();
+        if (!more) break;
     }
+    if (S == 1) {
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
-        int i = tr + a;
-        if (i >= it.rows) continue;
+        for (int a = 0; a < 8; ++a) {
+            const int i = tr * 8 + a;
+            if (i >= it.rows) continue;
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            int c = tc + b;
-            if (c >= cols) continue;
-            store_out(J, it, i, c0 + c, acc[a][b]);
+            for (int b = 0; b < 4; ++b) {
+                const int c = tc + 16 * b;
+                if (c < cols) store_out(J, it, i, c0 + c, acc[a][b]);
+            }
         }
+        return;
     }
+    // partial of this piece: part[((tile * ct + y) * S + s) * 4096 + i + 64 c]
+    const long long slot = ((long long)(tile * gridDim.y + blockIdx.y) * S + s) * (WT * WT);
+    double* mine = J.part + slot;
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) mine[(tr * 8 + a) + WT * (tc + 16 * b)] = acc[a][b];
+    __threadfence();
+    __syncthreads();
+    if (tid == 0)
+        last_flag = atomicAdd(J.cnt2 + tile * gridDim.y + blockIdx.y, 1) == S - 1;
+    __syncthreads();
+    if (!last_flag) return;
+    __threadfence();
+    const double* base = J.part + slot - (long long)s * (WT * WT);
+    for (int x = tid; x < it.rows * cols; x += WTHREADS) {
+        const int i = x % it.rows, c = x / it.rows;
+        double v = 0.0;
+        for (int q = 0; q < S; ++q) v += __ldcg(base + (long long)q * (WT * WT) + i + WT * c);
+        store_out(J, it, i, c0 + c, v);
+    }
+    if (tid == 0) J.cnt2[tile * gridDim.y + blockIdx.y] = 0;
 }
 
 // Work lists of one subtree of one H-matrix.
@@ -544,6 +653,36 @@ std::shared_ptr<JobTemplate> build_template(Context& ctx, const HMatrix& H, int 
         it.c0 = c1;
         c1 += it.nin;
         rmax = std::max(rmax, it.r);
+    }
+    // wide phase-1 tiles: the columns of the W's that share a source box
+    // (one input slice), 64 to a tile
+    std::vector<W1Tile> w1;
+    if (row_tile > 32) {
+        std::map<std::pair<long long, int>, std::vector<int>> groups;
+        for (int i = 0; i < (int)p1.size(); ++i) groups[{p1[i].in_off, p1[i].nin}].push_back(i);
+        for (auto& g : groups) {
+            W1Tile cur{};
+            cur.in_off = g.first.first;
+            cur.nin = g.first.second;
+            for (int i : g.second) {
+                for (int j = 0; j < p1[i].r; ++j) {
+                    if (cur.rows == kWideTile) {
+                        w1.push_back(cur);
+                        const long long io = cur.in_off;
+                        const int ni = cur.nin;
+                        cur = W1Tile{};
+                        cur.in_off = io;
+                        cur.nin = ni;
+                    }
+                    cur.wcol[cur.rows] = p1[i].W + (long long)j * p1[i].ldw;
+                    cur.trel[cur.rows] = p1[i].t_rel;
+                    cur.tj[cur.rows] = j;
+                    cur.tr[cur.rows] = p1[i].r;
+                    ++cur.rows;
+                }
+            }
+            if (cur.rows > 0) w1.push_back(cur);
+        }
     }
     // phase 2: bucket the leaves by the output clusters they cover
     const Box& outBox = S.boxes[trans ? R.src_box : R.tgt_box];
@@ -641,6 +780,8 @@ std::shared_ptr<JobTemplate> build_template(Context& ctx, const HMatrix& H, int 
     T->p2.upload(p2, ctx.stream);
     T->ent.upload(ent, ctx.stream);
     T->zero_tiles.upload(zero, ctx.stream);
+    T->nw1 = (int)w1.size();
+    T->w1.upload(w1, ctx.stream);
     T->hp1 = std::move(p1);
     T->hp2 = std::move(p2);
     T->hent = std::move(ent);
@@ -658,7 +799,7 @@ std::shared_ptr<JobTemplate> get_template(Context& ctx, const HMatrix& H, int ro
     if (it != H.templates.end()) return it->second;
     auto T = build_template(ctx, H, root, trans, row_tile);
     HMB_REQUIRE((T->n1 == 0 || T->p1.get()) && (T->n2 == 0 || (T->p2.get() && T->ent.get())) &&
-                    (T->nz == 0 || T->zero_tiles.get()),
+                    (T->nz == 0 || T->zero_tiles.get()) && (T->nw1 == 0 || T->w1.get()),
                 HM_ERR_INTERNAL, "work lists missing on the device");
     H.templates.emplace(key, T);
     return T;
@@ -777,26 +918,38 @@ void run_jobs(Context& ctx, const std::vector<MatJob>& jobs) {
     }
     // one vector, one job: stream the blocks (matvec.cu)
     if (jobs.size() == 1 && jobs[0].k == 1 && multiply_vector_streamed(ctx, jobs[0])) return;
-    // streaming (few right-hand sides): 32-row tiles, work split evenly
-    // over all resident warps
+    // few columns: 32-row tiles, work split evenly over all resident warps;
+    // many columns: 64 x 64 FP64 tiles
     const bool wide = kmax > 8;
     const int row_tile = wide ? 64 : 32;
     for (const MatJob& J : jobs) tmpl.push_back(get_template(ctx, *J.H, J.root, J.trans, row_tile));
-    const int NC2 = kmax <= 1 ? 1 : kmax <= 4 ? 4 : kmax <= 8 ? 8 : 64;
-    long long t_total = 0, c_total = 0;
-    std::vector<long long> t_off(jobs.size()), c1_off(jobs.size()), c2_off(jobs.size());
+    const int ct = ceil_div(std::max(kmax, 1), kWideTile);   // wide column tiles
+    // wide: cut every row tile's inner dimension into S pieces when there are
+    // too few tiles to fill the GPU
+    int S = 1;
+    if (wide) {
+        long long tiles = 0;
+        for (size_t j = 0; j < jobs.size(); ++j)
+            if (jobs[j].k > 0) tiles += (long long)tmpl[j]->n2 * ct;
+        if (tiles > 0) S = (int)std::min<long long>(8, std::max<long long>(1, (4LL * ctx.num_sms + tiles - 1) / tiles));
+    }
+    long long t_total = 0, c_total = 0, p_total = 0;
+    std::vector<long long> t_off(jobs.size()), c1_off(jobs.size()), c2_off(jobs.size()),
+        p_off(jobs.size());
     for (size_t j = 0; j < jobs.size(); ++j) {
         const JobTemplate& T = *tmpl[j];
         t_off[j] = t_total;
         t_total += T.t_rows * jobs[j].k;
         c1_off[j] = c_total;
-        c_total += T.n1;
+        c_total += wide ? 0 : T.n1;
         c2_off[j] = c_total;
-        c_total += T.n2;
+        c_total += wide ? (long long)T.n2 * ct : T.n2;
+        p_off[j] = p_total;
+        if (wide && S > 1) p_total += (long long)T.n2 * ct * S * kWideTile * kWideTile;
     }
     DeviceBuffer<double> tbuf;
-    tbuf.allocate((size_t)std::max<long long>(t_total, 1), st);
-    int* cnt = wide ? nullptr : ctx.zeroed_counters(std::max<long long>(c_total, 1));
+    tbuf.allocate((size_t)std::max<long long>(t_total + p_total, 1), st);
+    int* cnt = (wide && S == 1) ? nullptr : ctx.zeroed_counters(std::max<long long>(c_total, 1));
     std::vector<JobExec> ex;
     ex.reserve(jobs.size());
     long long n1 = 0, n2 = 0;
@@ -809,12 +962,14 @@ void run_jobs(Context& ctx, const std::vector<MatJob>& jobs) {
         const JobTemplate& T = *tmpl[j];
         JobExec e{};
         e.p1 = T.p1.get();
+        e.w1 = T.w1.get();
         e.p2 = T.p2.get();
         e.ent = T.ent.get();
         e.in = J.in;
         e.out = J.out;
         e.T = tbuf.get() + t_off[j];
-        if (!wide) {
+        e.part = tbuf.get() + t_total + p_off[j];
+        if (cnt) {
             e.cnt1 = cnt + c1_off[j];
             e.cnt2 = cnt + c2_off[j];
         }
@@ -826,12 +981,12 @@ void run_jobs(Context& ctx, const std::vector<MatJob>& jobs) {
         e.k = J.k;
         e.n1 = T.n1;
         e.n2 = T.n2;
-        e.ct1 = wide ? ceil_div(J.k, 32) : 1;
-        e.ct2 = wide ? ceil_div(J.k, NC2) : 1;
+        e.ct1 = 1;
+        e.ct2 = 1;
         e.p1_begin = n1;
         e.p2_begin = n2;
-        n1 += wide ? (long long)T.n1 * e.ct1 : T.c1;
-        n2 += wide ? (long long)T.n2 * e.ct2 : T.c2;
+        n1 += wide ? (long long)T.nw1 : T.c1;
+        n2 += wide ? (long long)T.n2 * S : T.c2;
         rmax = std::max(rmax, T.rmax);
         ex.push_back(e);
     }
@@ -863,15 +1018,16 @@ void run_jobs(Context& ctx, const std::vector<MatJob>& jobs) {
         }
         return;
     }
-    HMB_REQUIRE(n1 < (1LL << 31) && n2 < (1LL << 31), HM_ERR_UNSUPPORTED, "batch too large");
+    HMB_REQUIRE(n1 < (1LL << 31) && n2 < (1LL << 31) && ct < 65536, HM_ERR_UNSUPPORTED,
+                "batch too large");
     if (n1 > 0) {
         LaunchScope ls(ctx, "hmm_lowrank_inner");
-        p1_wide_kernel<<<(unsigned)n1, kThreads, 0, st>>>(jobs_d, nj, job0);
+        w1_kernel<<<dim3((unsigned)n1, (unsigned)ct), WTHREADS, 0, st>>>(jobs_d, nj, job0);
         HMB_CHECK_LAUNCH();
     }
     if (n2 > 0) {
         LaunchScope ls(ctx, "hmm_row_tiles");
-        p2_wide_kernel<<<(unsigned)n2, kThreads, 0, st>>>(jobs_d, nj, job0);
+        w2_kernel<<<dim3((unsigned)n2, (unsigned)ct), WTHREADS, 0, st>>>(jobs_d, nj, job0, S);
         HMB_CHECK_LAUNCH();
     }
 }

@@ -33,11 +33,27 @@ struct P2Entry {
     int cbeg;          // first column of this entry in its tile's concatenation
 };
 
+// Phase-1 tile of the wide (many-column) product: 64 rows of T gathered from
+// the low-rank blocks that share one source box (so one input slice, rows
+// [in_off, in_off + nin)).  Row i is column wcol[i] of some W; its results
+// go to T[trel[i] * k + tj[i] + c * tr[i]].
+constexpr int kWideTile = 64;
+struct W1Tile {
+    long long in_off;
+    int nin, rows;
+    const double* wcol[kWideTile];
+    long long trel[kWideTile];
+    int tj[kWideTile];
+    int tr[kWideTile];
+};
+
 struct JobTemplate {
     DeviceBuffer<P1T> p1;
     DeviceBuffer<P2T> p2;
     DeviceBuffer<P2Entry> ent;
     DeviceBuffer<int> zero_tiles;   // tiles without entries (output = beta * output)
+    DeviceBuffer<W1Tile> w1;        // wide phase-1 tiles
+    int nw1 = 0;
     // Host copies, and per split width GW the first item / (tile, entry) of
     // every warp of the narrow kernels (built on first use).
     std::vector<P1T> hp1;

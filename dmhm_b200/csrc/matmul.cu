@@ -380,15 +380,16 @@ __global__ void p2_zero_kernel(const JobExec J, const int* __restrict__ tiles, i
 }
 
 // ---------------------------------------------------------------------------
-// Wide (many columns): FP64 64 x 64 output tiles, 128 threads, 8 x 4 outputs
-// a thread; operands staged through shared memory in chunks of KC inner
-// indices by cp.async, two stages (the next chunk loads while this one is
-// multiplied).
+// Wide (many columns): FP64 64 x 64 output tiles on the FP64 tensor cores
+// (mma.m8n8k4.f64), 4 warps of 32 x 32 each (4 x 4 MMA blocks, 32
+// accumulators a thread); operands staged through shared memory in chunks
+// of KC inner indices by cp.async, two stages (the next chunk loads while
+// this one is multiplied).
 // ---------------------------------------------------------------------------
 constexpr int WT = kWideTile;   // tile rows = tile columns
 constexpr int KC = 16;          // inner chunk
-constexpr int WTHREADS = 128;   // 8 row groups x 16 column lanes
-constexpr int SP = WT + 1;      // padded smem row (conflict-free transposing stores)
+constexpr int WTHREADS = 128;   // 2 x 2 warps of 32 x 32
+constexpr int SP = WT + 8;      // smem row: fragment loads hit 32 distinct banks
 
 struct WideSmem {
     double a[2][KC][SP];   // a[buf][p][i] = A(i, p)
@@ -405,20 +406,41 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-// acc[a][b] += sum_p A(tr*8+a, p) B(p, tc+16b) over one staged chunk.
-__device__ __forceinline__ void wide_mma(const WideSmem& sm, int buf, int tr, int tc,
-                                         double (&acc)[8][4]) {
-#pragma unroll 4
-    for (int p = 0; p < KC; ++p) {
-        double av[8], bv[4];
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
+// Accumulator slot s = (mb * 4 + nb) * 2 + h of a thread holds tile element
+// (row_of(s), col_of(s)) (the m8n8k4 C fragment: row lane/4, columns
+// 2 (lane%4) + h of MMA block (mb, nb) of the warp's 32 x 32 quarter).
+__device__ __forceinline__ int acc_row(int s, int warp, int lane) {
+    return (warp & 1) * 32 + (s >> 3) * 8 + (lane >> 2);
+}
+__device__ __forceinline__ int acc_col(int s, int warp, int lane) {
+    return (warp >> 1) * 32 + ((s >> 1) & 3) * 8 + 2 * (lane & 3) + (s & 1);
+}
+
+// acc += A(warp rows, chunk) B(chunk, warp columns) over one staged chunk.
+__device__ __forceinline__ void wide_mma(const WideSmem& sm, int buf, int warp, int lane,
+                                         double (&acc)[32]) {
+    const int r0 = (warp & 1) * 32 + (lane >> 2), c0 = (warp >> 1) * 32 + (lane >> 2);
 #pragma unroll
-        for (int a = 0; a < 8; ++a) av[a] = sm.a[buf][p][tr * 8 + a];
+    for (int ks = 0; ks < KC / 4; ++ks) {
+        const int p = ks * 4 + (lane & 3);
+        double a[4], b[4];
 #pragma unroll
-        for (int b = 0; b < 4; ++b) bv[b] = sm.b[buf][p][tc + 16 * b];
+        for (int mb = 0; mb < 4; ++mb) a[mb] = sm.a[buf][p][r0 + mb * 8];
 #pragma unroll
-        for (int a = 0; a < 8; ++a)
+        for (int nb = 0; nb < 4; ++nb) b[nb] = sm.b[buf][p][c0 + nb * 8];
 #pragma unroll
-            for (int b = 0; b < 4; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+        for (int mb = 0; mb < 4; ++mb)
+#pragma unroll
+            for (int nb = 0; nb < 4; ++nb) {
+                double (&d)[2] = *reinterpret_cast<double(*)[2]>(&acc[(mb * 4 + nb) * 2]);
+                dmma(d, a[mb], b[nb]);
+            }
     }
 }
 
@@ -440,7 +462,7 @@ w1_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0) {
     const long long gi = blockIdx.x;
     const JobExec& J = jobs ? jobs[find_job(jobs, njobs, gi, false)] : job0;
     const W1Tile* tile = J.w1 + (gi - J.p1_begin);
-    const int tid = threadIdx.x, tr = tid >> 4, tc = tid & 15;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int c0 = blockIdx.y * WT;
     const int cols = min(WT, J.k - c0);
     if (cols <= 0) return;
@@ -459,11 +481,9 @@ w1_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0) {
         load_b_chunk(sm, buf, X + p0, J.ldin, len, cols, tid);
         cp_async_commit();
     };
-    double acc[8][4];
+    double acc[32];
 #pragma unroll
-    for (int a = 0; a < 8; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+    for (int q = 0; q < 32; ++q) acc[q] = 0.0;
     const int nq = (K + KC - 1) / KC;
     if (nq > 0) load(0, 0);
     for (int q = 0; q < nq; ++q) {
@@ -474,20 +494,14 @@ w1_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0) {
             cp_async_wait<0>();
         }
         __syncthreads();
-        wide_mma(sm, q & 1, tr, tc, acc);
+        wide_mma(sm, q & 1, warp, lane, acc);
         __syncthreads();
     }
 #pragma unroll
-    for (int a = 0; a < 8; ++a) {
-        const int i = tr * 8 + a;
-        if (i >= rows) continue;
-        double* t = J.T + tile->trel[i] * J.k + tile->tj[i];
-        const int st = tile->tr[i];
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            const int c = tc + 16 * b;
-            if (c < cols) t[(long long)(c0 + c) * st] = acc[a][b];
-        }
+    for (int q = 0; q < 32; ++q) {
+        const int i = acc_row(q, warp, lane), c = acc_col(q, warp, lane);
+        if (i < rows && c < cols)
+            J.T[tile->trel[i] * J.k + tile->tj[i] + (long long)(c0 + c) * tile->tr[i]] = acc[q];
     }
 }
 
@@ -504,7 +518,7 @@ w2_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0, int S
     const long long local = gi - J.p2_begin;
     const int tile = (int)(local / S), s = (int)(local % S);
     const P2T it = J.p2[tile];
-    const int tid = threadIdx.x, tr = tid >> 4, tc = tid & 15;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int c0 = blockIdx.y * WT;
     const int cols = min(WT, J.k - c0);
     if (cols <= 0) return;
@@ -542,11 +556,9 @@ w2_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0, int S
         pos += len;
         if (pos >= e.cbeg + e.inner) ++ei;
     };
-    double acc[8][4];
+    double acc[32];
 #pragma unroll
-    for (int a = 0; a < 8; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+    for (int q = 0; q < 32; ++q) acc[q] = 0.0;
     const bool any = q1 > q0;
     if (any) load(0);
     for (int buf = 0; any; buf ^= 1) {
@@ -558,20 +570,15 @@ w2_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0, int S
             cp_async_wait<0>();
         }
         __syncthreads();
-        wide_mma(sm, buf, tr, tc, acc);
+        wide_mma(sm, buf, warp, lane, acc);
         __syncthreads();
         if (!more) break;
     }
     if (S == 1) {
 #pragma unroll
-        for (int a = 0; a < 8; ++a) {
-            const int i = tr * 8 + a;
-            if (i >= it.rows) continue;
-#pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                const int c = tc + 16 * b;
-                if (c < cols) store_out(J, it, i, c0 + c, acc[a][b]);
-            }
+        for (int q = 0; q < 32; ++q) {
+            const int i = acc_row(q, warp, lane), c = acc_col(q, warp, lane);
+            if (i < it.rows && c < cols) store_out(J, it, i, c0 + c, acc[q]);
         }
         return;
     }
@@ -579,9 +586,7 @@ w2_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0, int S
     const long long slot = ((long long)(tile * gridDim.y + blockIdx.y) * S + s) * (WT * WT);
     double* mine = J.part + slot;
 #pragma unroll
-    for (int a = 0; a < 8; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) mine[(tr * 8 + a) + WT * (tc + 16 * b)] = acc[a][b];
+    for (int q = 0; q < 32; ++q) mine[acc_row(q, warp, lane) + WT * acc_col(q, warp, lane)] = acc[q];
     __threadfence();
     __syncthreads();
     if (tid == 0)

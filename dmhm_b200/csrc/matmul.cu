@@ -32,7 +32,10 @@ namespace hmb {
 struct JobExec {
     const P1T* p1;
     const W1Tile* w1;
-    double* part;        // wide phase-2 partials of split tiles
+    const int* w1cp;     // wide: chunk prefix over the W1 tiles (n_w1 + 1)
+    const int* tcp;      // wide: chunk prefix over the row tiles (n2 + 1)
+    const int* ekc;      // wide: first chunk of each entry within its tile
+    double* part;        // wide: partials of tiles cut between CTAs (shared by all jobs)
     const P2T* p2;
     const P2Entry* ent;
     const double* in;
@@ -391,9 +394,10 @@ constexpr int KC = 16;          // inner chunk
 constexpr int WTHREADS = 128;   // 2 x 2 warps of 32 x 32
 constexpr int SP = WT + 8;      // smem row: fragment loads hit 32 distinct banks
 
+constexpr int NSTAGE = 2;       // chunk buffers per CTA
 struct WideSmem {
-    double a[2][KC][SP];   // a[buf][p][i] = A(i, p)
-    double b[2][KC][SP];   // b[buf][p][c] = B(p, c)
+    double a[NSTAGE][KC][SP];   // a[buf][p][i] = A(i, p)
+    double b[NSTAGE][KC][SP];   // b[buf][p][c] = B(p, c)
 };
 
 __device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
@@ -455,153 +459,229 @@ __device__ __forceinline__ void load_b_chunk(WideSmem& sm, int buf, const double
     }
 }
 
-__global__ void __launch_bounds__(WTHREADS)
-w1_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0) {
-    __shared__ WideSmem sm;
-    __shared__ const double* wcol[WT];
-    const long long gi = blockIdx.x;
-    const JobExec& J = jobs ? jobs[find_job(jobs, njobs, gi, false)] : job0;
-    const W1Tile* tile = J.w1 + (gi - J.p1_begin);
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int c0 = blockIdx.y * WT;
-    const int cols = min(WT, J.k - c0);
-    if (cols <= 0) return;
-    const int rows = tile->rows, K = tile->nin;
-    for (int i = tid; i < WT; i += WTHREADS) wcol[i] = i < rows ? tile->wcol[i] : tile->wcol[0];
-    __syncthreads();
-    const double* X = J.in + tile->in_off + (long long)c0 * J.ldin;
-    auto load = [&](int q, int buf) {
-        const int p0 = q * KC, len = min(KC, K - p0);
-#pragma unroll
-        for (int e = tid; e < WT * KC; e += WTHREADS) {
-            const int p = e % KC, i = e / KC;   // p fastest: W columns are contiguous
-            const bool v = p < len && i < rows;
-            cp_async8(&sm.a[buf][p][i], v ? wcol[i] + p0 + p : wcol[0], v);
-        }
-        load_b_chunk(sm, buf, X + p0, J.ldin, len, cols, tid);
-        cp_async_commit();
-    };
-    double acc[32];
-#pragma unroll
-    for (int q = 0; q < 32; ++q) acc[q] = 0.0;
-    const int nq = (K + KC - 1) / KC;
-    if (nq > 0) load(0, 0);
-    for (int q = 0; q < nq; ++q) {
-        if (q + 1 < nq) {
-            load(q + 1, (q + 1) & 1);
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
-        __syncthreads();
-        wide_mma(sm, q & 1, warp, lane, acc);
-        __syncthreads();
-    }
-#pragma unroll
-    for (int q = 0; q < 32; ++q) {
-        const int i = acc_row(q, warp, lane), c = acc_col(q, warp, lane);
-        if (i < rows && c < cols)
-            J.T[tile->trel[i] * J.k + tile->tj[i] + (long long)(c0 + c) * tile->tr[i]] = acc[q];
-    }
-}
+// The wide kernels stream a sequence of KC-chunks: phase 1 the chunks of
+// every W1 tile (its nin input rows), phase 2 the chunks of every row tile's
+// entries (no chunk spans two entries), over all jobs.  A persistent CTA takes
+// an even share [b C / G, (b+1) C / G) of the sequence; the next chunk (of the
+// same or the next tile) loads while the current one is multiplied.  A tile
+// whose chunks a CTA holds completely is written directly; a tile cut between
+// CTAs b_a..b_b leaves 64 x 64 partials (slot 2b for a CTA's first piece,
+// 2b + 1 for its last) that the piece finishing last adds up in CTA order.
+struct ChunkPos {
+    int job, tile, ei, pos;   // phase 1: ei unused, pos = row offset in the tile's input
+};
 
-// Phase-2 tile of the wide path: Y_tile = alpha sum_e A_e B_e + beta Y_tile,
-// the tile's concatenated inner dimension cut into `S` pieces (one CTA each);
-// with S > 1 every piece leaves a 64 x 64 partial and the last piece of the
-// tile adds them up in piece order (a counter per tile and column tile).
+template <int PHASE>
+__device__ __forceinline__ int tiles_of(const JobExec& J) { return PHASE == 1 ? J.n1 : J.n2; }
+template <int PHASE>
+__device__ __forceinline__ const int* chunk_prefix(const JobExec& J) { return PHASE == 1 ? J.w1cp : J.tcp; }
+
+template <int PHASE>
 __global__ void __launch_bounds__(WTHREADS)
-w2_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0, int S) {
-    __shared__ WideSmem sm;
+wide_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0, long long C, int G) {
+    extern __shared__ __align__(16) unsigned char wide_smem[];
+    WideSmem& sm = *reinterpret_cast<WideSmem*>(wide_smem);
     __shared__ int last_flag;
-    const long long gi = blockIdx.x;
-    const JobExec& J = jobs ? jobs[find_job(jobs, njobs, gi, true)] : job0;
-    const long long local = gi - J.p2_begin;
-    const int tile = (int)(local / S), s = (int)(local % S);
-    const P2T it = J.p2[tile];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int c0 = blockIdx.y * WT;
-    const int cols = min(WT, J.k - c0);
-    if (cols <= 0) return;
-    const int q0 = (int)((long long)it.width * s / S), q1 = (int)((long long)it.width * (s + 1) / S);
-    // chunk cursor: entry ei, position pos (concatenation index)
-    int ei = it.e0;
-    while (ei + 1 < it.e1 && J.ent[ei + 1].cbeg <= q0) ++ei;
-    int pos = q0;
-    auto load = [&](int buf) {
-        const P2Entry e = J.ent[ei];
-        const int pin = pos - e.cbeg;   // position within the entry
-        const int len = min(KC, min(e.cbeg + e.inner, q1) - pos);
-        if (!e.transA) {
-            const double* A = e.A + it.r0 + (long long)pin * e.lda;
-#pragma unroll
-            for (int x = tid; x < WT * KC; x += WTHREADS) {
-                const int i = x % WT, p = x / WT;   // rows contiguous
-                const bool v = p < len && i < it.rows;
-                cp_async8(&sm.a[buf][p][i], v ? A + i + (long long)p * e.lda : e.A, v);
-            }
+    const int b = blockIdx.x, y = blockIdx.y;
+    const long long g0 = split_start(b, G, C), g1 = split_start(b + 1, G, C);
+    if (g0 >= g1) return;
+    auto job = [&](int j) -> const JobExec& { return jobs ? jobs[j] : job0; };
+    // locate the first chunk
+    ChunkPos cur{};
+    {
+        cur.job = jobs ? find_job(jobs, njobs, g0, PHASE == 2) : 0;
+        const JobExec& J = job(cur.job);
+        const long long local = g0 - (PHASE == 1 ? J.p1_begin : J.p2_begin);
+        const int* cp = chunk_prefix<PHASE>(J);
+        int lo = 0, hi = tiles_of<PHASE>(J) - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (cp[mid] <= local) lo = mid;
+            else hi = mid - 1;
+        }
+        // skip tiles without chunks
+        while (cp[lo + 1] <= local) ++lo;
+        cur.tile = lo;
+        const int kin = (int)(local - cp[lo]);
+        if (PHASE == 1) {
+            cur.pos = kin * KC;
         } else {
-            const double* A = e.A + pin + (long long)it.r0 * e.lda;
+            const P2T it = J.p2[lo];
+            int e = it.e0, eh = it.e1 - 1;
+            while (e < eh) {
+                const int mid = (e + eh + 1) >> 1;
+                if (J.ekc[mid] <= kin) e = mid;
+                else eh = mid - 1;
+            }
+            cur.ei = e;
+            cur.pos = (kin - J.ekc[e]) * KC;
+        }
+    }
+    // loads the chunk at `c` into buffer `buf`; returns whether it is the last
+    // chunk of its tile; advances `c`
+    auto load = [&](ChunkPos& c, int buf) -> bool {
+        const JobExec& J = job(c.job);
+        const int cols = min(WT, J.k - y * WT);
+        bool last;
+        if (PHASE == 1) {
+            const W1Tile* t = J.w1 + c.tile;
+            const int len = min(KC, t->nin - c.pos), rows = t->rows;
 #pragma unroll
-            for (int x = tid; x < WT * KC; x += WTHREADS) {
-                const int p = x % KC, i = x / KC;   // inner index contiguous
-                const bool v = p < len && i < it.rows;
-                cp_async8(&sm.a[buf][p][i], v ? A + p + (long long)i * e.lda : e.A, v);
+            for (int e = tid; e < WT * KC; e += WTHREADS) {
+                const int p = e % KC, i = e / KC;   // W columns are contiguous
+                const bool v = p < len && i < rows;
+                const double* w0 = t->wcol[v ? i : 0];
+                cp_async8(&sm.a[buf][p][i], v ? w0 + c.pos + p : w0, v);
+            }
+            load_b_chunk(sm, buf, J.in + t->in_off + c.pos + (long long)y * WT * J.ldin, J.ldin,
+                         len, cols, tid);
+            c.pos += len;
+            last = c.pos >= t->nin;
+        } else {
+            const P2T it = J.p2[c.tile];
+            const P2Entry e = J.ent[c.ei];
+            const int len = min(KC, e.inner - c.pos);
+            if (!e.transA) {
+                const double* A = e.A + it.r0 + (long long)c.pos * e.lda;
+#pragma unroll
+                for (int x = tid; x < WT * KC; x += WTHREADS) {
+                    const int i = x % WT, p = x / WT;   // rows contiguous
+                    const bool v = p < len && i < it.rows;
+                    cp_async8(&sm.a[buf][p][i], v ? A + i + (long long)p * e.lda : e.A, v);
+                }
+            } else {
+                const double* A = e.A + c.pos + (long long)it.r0 * e.lda;
+#pragma unroll
+                for (int x = tid; x < WT * KC; x += WTHREADS) {
+                    const int p = x % KC, i = x / KC;   // inner index contiguous
+                    const bool v = p < len && i < it.rows;
+                    cp_async8(&sm.a[buf][p][i], v ? A + p + (long long)i * e.lda : e.A, v);
+                }
+            }
+            const double* EB;
+            int ldb;
+            entry_b(e, J, EB, ldb);
+            load_b_chunk(sm, buf, EB + c.pos + (long long)y * WT * ldb, ldb, len, cols, tid);
+            c.pos += len;
+            last = false;
+            if (c.pos >= e.inner) {
+                c.pos = 0;
+                ++c.ei;
+                last = c.ei >= it.e1;
             }
         }
-        const double* EB;
-        int ldb;
-        entry_b(e, J, EB, ldb);
-        load_b_chunk(sm, buf, EB + pin + (long long)c0 * ldb, ldb, len, cols, tid);
         cp_async_commit();
-        pos += len;
-        if (pos >= e.cbeg + e.inner) ++ei;
+        if (last) {   // move to the next tile with chunks (possibly of the next job)
+            c.pos = 0;
+            for (;;) {
+                ++c.tile;
+                if (c.tile >= tiles_of<PHASE>(job(c.job))) {
+                    if (!jobs || c.job + 1 >= njobs) break;
+                    ++c.job;
+                    c.tile = -1;
+                    continue;
+                }
+                const int* cp = chunk_prefix<PHASE>(job(c.job));
+                if (cp[c.tile + 1] > cp[c.tile]) break;
+            }
+            if (PHASE == 2 && c.tile < tiles_of<PHASE>(job(c.job))) c.ei = job(c.job).p2[c.tile].e0;
+        }
+        return last;
     };
     double acc[32];
 #pragma unroll
     for (int q = 0; q < 32; ++q) acc[q] = 0.0;
-    const bool any = q1 > q0;
-    if (any) load(0);
-    for (int buf = 0; any; buf ^= 1) {
-        const bool more = pos < q1;
-        if (more) {
-            load(buf ^ 1);
-            cp_async_wait<1>();
+    // NSTAGE-deep ring: chunk q sits in buffer q % NSTAGE and is issued
+    // NSTAGE - 1 chunks ahead; one commit group per chunk slot (empty past
+    // the end) keeps the wait count constant
+    ChunkPos loaded[NSTAGE];
+    bool lastc[NSTAGE];
+    const long long n = g1 - g0;
+#pragma unroll
+    for (int s = 0; s < NSTAGE - 1; ++s) {
+        if (s < n) {
+            loaded[s] = cur;
+            lastc[s] = load(cur, s);
         } else {
-            cp_async_wait<0>();
+            cp_async_commit();
         }
+    }
+    bool first_piece = true;
+    for (long long q = 0; q < n; ++q) {
+        const long long qn = q + NSTAGE - 1;
+        const int bn = (int)(qn % NSTAGE);
+        if (qn < n) {
+            loaded[bn] = cur;
+            lastc[bn] = load(cur, bn);
+        } else {
+            cp_async_commit();
+        }
+        cp_async_wait<NSTAGE - 1>();
         __syncthreads();
+        const int buf = (int)(q % NSTAGE);
         wide_mma(sm, buf, warp, lane, acc);
         __syncthreads();
-        if (!more) break;
-    }
-    if (S == 1) {
-#pragma unroll
-        for (int q = 0; q < 32; ++q) {
-            const int i = acc_row(q, warp, lane), c = acc_col(q, warp, lane);
-            if (i < it.rows && c < cols) store_out(J, it, i, c0 + c, acc[q]);
+        if (!lastc[buf] && q + 1 < n) continue;
+        // flush the tile of this chunk
+        const ChunkPos& t = loaded[buf];
+        const JobExec& J = job(t.job);
+        const int cols = min(WT, J.k - y * WT);
+        const long long base = PHASE == 1 ? J.p1_begin : J.p2_begin;
+        const int* cp = chunk_prefix<PHASE>(J);
+        const long long T0 = base + cp[t.tile], T1 = base + cp[t.tile + 1];
+        const bool whole = T0 >= g0 && T1 <= g1;
+        int rows;
+        const W1Tile* wt = nullptr;
+        P2T it{};
+        if (PHASE == 1) {
+            wt = J.w1 + t.tile;
+            rows = wt->rows;
+        } else {
+            it = J.p2[t.tile];
+            rows = it.rows;
         }
-        return;
-    }
-    // partial of this piece: part[((tile * ct + y) * S + s) * 4096 + i + 64 c]
-    const long long slot = ((long long)(tile * gridDim.y + blockIdx.y) * S + s) * (WT * WT);
-    double* mine = J.part + slot;
+        auto emit = [&](int i, int c, double v) {
+            if (PHASE == 1)
+                J.T[wt->trel[i] * J.k + wt->tj[i] + (long long)(y * WT + c) * wt->tr[i]] = v;
+            else
+                store_out(J, it, i, y * WT + c, v);
+        };
+        if (whole) {
 #pragma unroll
-    for (int q = 0; q < 32; ++q) mine[acc_row(q, warp, lane) + WT * acc_col(q, warp, lane)] = acc[q];
-    __threadfence();
-    __syncthreads();
-    if (tid == 0)
-        last_flag = atomicAdd(J.cnt2 + tile * gridDim.y + blockIdx.y, 1) == S - 1;
-    __syncthreads();
-    if (!last_flag) return;
-    __threadfence();
-    const double* base = J.part + slot - (long long)s * (WT * WT);
-    for (int x = tid; x < it.rows * cols; x += WTHREADS) {
-        const int i = x % it.rows, c = x / it.rows;
-        double v = 0.0;
-        for (int q = 0; q < S; ++q) v += __ldcg(base + (long long)q * (WT * WT) + i + WT * c);
-        store_out(J, it, i, c0 + c, v);
+            for (int k = 0; k < 32; ++k) {
+                const int i = acc_row(k, warp, lane), c = acc_col(k, warp, lane);
+                if (i < rows && c < cols) emit(i, c, acc[k]);
+            }
+        } else {
+            double* part = J.part + ((long long)y * 2 * G) * (WT * WT);
+            double* mine = part + (2LL * b + (first_piece ? 0 : 1)) * (WT * WT);
+#pragma unroll
+            for (int k = 0; k < 32; ++k) mine[acc_row(k, warp, lane) + WT * acc_col(k, warp, lane)] = acc[k];
+            __threadfence();
+            __syncthreads();
+            const long long wa = split_owner(T0, G, C), wb = split_owner(T1 - 1, G, C);
+            int* cnt = (PHASE == 1 ? J.cnt1 : J.cnt2) + (long long)t.tile * gridDim.y + y;
+            if (tid == 0) last_flag = atomicAdd(cnt, 1) == (int)(wb - wa);
+            __syncthreads();
+            if (last_flag) {
+                __threadfence();
+                const bool wa_here = split_start(wa, G, C) == T0;
+                for (int x = tid; x < rows * cols; x += WTHREADS) {
+                    const int i = x % rows, c = x / rows;
+                    double v = 0.0;
+                    for (long long w = wa; w <= wb; ++w)
+                        v += __ldcg(part + piece_slot(w, wa, wa_here) * (WT * WT) + i + WT * c);
+                    emit(i, c, v);
+                }
+                if (tid == 0) *cnt = 0;
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int k = 0; k < 32; ++k) acc[k] = 0.0;
+        first_piece = false;
     }
-    if (tid == 0) J.cnt2[tile * gridDim.y + blockIdx.y] = 0;
 }
 
 // Work lists of one subtree of one H-matrix.
@@ -787,6 +867,25 @@ std::shared_ptr<JobTemplate> build_template(Context& ctx, const HMatrix& H, int 
     T->zero_tiles.upload(zero, ctx.stream);
     T->nw1 = (int)w1.size();
     T->w1.upload(w1, ctx.stream);
+    if (row_tile > 32) {
+        // chunk prefixes of the wide kernels (chunks of KC inner indices,
+        // none spanning two entries)
+        std::vector<int> w1cp(w1.size() + 1, 0), tcp(p2.size() + 1, 0), ekc(ent.size(), 0);
+        for (size_t i = 0; i < w1.size(); ++i) w1cp[i + 1] = w1cp[i] + ceil_div(w1[i].nin, KC);
+        for (size_t t = 0; t < p2.size(); ++t) {
+            int k = 0;
+            for (int e = p2[t].e0; e < p2[t].e1; ++e) {
+                ekc[e] = k;
+                k += ceil_div(ent[e].inner, KC);
+            }
+            tcp[t + 1] = tcp[t] + k;
+        }
+        T->wc1 = w1cp.back();
+        T->wc2 = tcp.back();
+        T->w1cp.upload(w1cp, ctx.stream);
+        T->tcp.upload(tcp, ctx.stream);
+        T->ekc.upload(ekc, ctx.stream);
+    }
     T->hp1 = std::move(p1);
     T->hp2 = std::move(p2);
     T->hent = std::move(ent);
@@ -811,6 +910,20 @@ std::shared_ptr<JobTemplate> get_template(Context& ctx, const HMatrix& H, int ro
 }
 
 namespace {
+
+// Resident CTAs of a persistent kernel of `threads` threads a CTA.
+template <typename K>
+int persistent_grid_n(const Context& ctx, K kernel, int threads, size_t smem = 0) {
+    static std::mutex mu;
+    static std::map<const void*, int> per_sm;
+    std::lock_guard<std::mutex> lock(mu);
+    int& n = per_sm[(const void*)kernel];
+    if (n == 0) {
+        HMB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, smem));
+        n = std::max(1, n);
+    }
+    return n * ctx.num_sms;
+}
 
 // Resident CTAs of a persistent kernel (occupancy x SMs), cached per kernel.
 template <typename K>
@@ -929,15 +1042,6 @@ void run_jobs(Context& ctx, const std::vector<MatJob>& jobs) {
     const int row_tile = wide ? 64 : 32;
     for (const MatJob& J : jobs) tmpl.push_back(get_template(ctx, *J.H, J.root, J.trans, row_tile));
     const int ct = ceil_div(std::max(kmax, 1), kWideTile);   // wide column tiles
-    // wide: cut every row tile's inner dimension into S pieces when there are
-    // too few tiles to fill the GPU
-    int S = 1;
-    if (wide) {
-        long long tiles = 0;
-        for (size_t j = 0; j < jobs.size(); ++j)
-            if (jobs[j].k > 0) tiles += (long long)tmpl[j]->n2 * ct;
-        if (tiles > 0) S = (int)std::min<long long>(8, std::max<long long>(1, (4LL * ctx.num_sms + tiles - 1) / tiles));
-    }
     long long t_total = 0, c_total = 0, p_total = 0;
     std::vector<long long> t_off(jobs.size()), c1_off(jobs.size()), c2_off(jobs.size()),
         p_off(jobs.size());
@@ -946,15 +1050,34 @@ void run_jobs(Context& ctx, const std::vector<MatJob>& jobs) {
         t_off[j] = t_total;
         t_total += T.t_rows * jobs[j].k;
         c1_off[j] = c_total;
-        c_total += wide ? 0 : T.n1;
+        c_total += wide ? (long long)T.nw1 * ct : T.n1;
         c2_off[j] = c_total;
         c_total += wide ? (long long)T.n2 * ct : T.n2;
-        p_off[j] = p_total;
-        if (wide && S > 1) p_total += (long long)T.n2 * ct * S * kWideTile * kWideTile;
     }
+    // wide: persistent grids, 2 partial slots of 64 x 64 per CTA and column tile
+    int G1 = 0, G2 = 0;
+    if (wide) {
+        long long c1 = 0, c2 = 0;
+        for (size_t j = 0; j < jobs.size(); ++j)
+            if (jobs[j].k > 0) {
+                c1 += tmpl[j]->wc1;
+                c2 += tmpl[j]->wc2;
+            }
+        static std::once_flag attr_once;
+        std::call_once(attr_once, [] {
+            cudaFuncSetAttribute(wide_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(WideSmem));
+            cudaFuncSetAttribute(wide_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(WideSmem));
+        });
+        G1 = (int)std::min<long long>(c1, persistent_grid_n(ctx, wide_kernel<1>, WTHREADS, sizeof(WideSmem)));
+        G2 = (int)std::min<long long>(c2, persistent_grid_n(ctx, wide_kernel<2>, WTHREADS, sizeof(WideSmem)));
+        p_total = 2LL * std::max(G1, G2) * ct * kWideTile * kWideTile;
+    }
+    (void)p_off;
     DeviceBuffer<double> tbuf;
     tbuf.allocate((size_t)std::max<long long>(t_total + p_total, 1), st);
-    int* cnt = (wide && S == 1) ? nullptr : ctx.zeroed_counters(std::max<long long>(c_total, 1));
+    int* cnt = ctx.zeroed_counters(std::max<long long>(c_total, 1));
     std::vector<JobExec> ex;
     ex.reserve(jobs.size());
     long long n1 = 0, n2 = 0;
@@ -973,25 +1096,26 @@ void run_jobs(Context& ctx, const std::vector<MatJob>& jobs) {
         e.in = J.in;
         e.out = J.out;
         e.T = tbuf.get() + t_off[j];
-        e.part = tbuf.get() + t_total + p_off[j];
-        if (cnt) {
-            e.cnt1 = cnt + c1_off[j];
-            e.cnt2 = cnt + c2_off[j];
-        }
+        e.part = tbuf.get() + t_total;
+        e.w1cp = T.w1cp.get();
+        e.tcp = T.tcp.get();
+        e.ekc = T.ekc.get();
+        e.cnt1 = cnt + c1_off[j];
+        e.cnt2 = cnt + c2_off[j];
         e.alpha_scale = J.alpha_scale;
         e.alpha = J.alpha;
         e.beta = J.beta;
         e.ldin = J.ldin;
         e.ldout = J.ldout;
         e.k = J.k;
-        e.n1 = T.n1;
+        e.n1 = wide ? T.nw1 : T.n1;
         e.n2 = T.n2;
         e.ct1 = 1;
         e.ct2 = 1;
         e.p1_begin = n1;
         e.p2_begin = n2;
-        n1 += wide ? (long long)T.nw1 : T.c1;
-        n2 += wide ? (long long)T.n2 * S : T.c2;
+        n1 += wide ? T.wc1 : T.c1;
+        n2 += wide ? T.wc2 : T.c2;
         rmax = std::max(rmax, T.rmax);
         ex.push_back(e);
     }
@@ -1023,17 +1147,30 @@ void run_jobs(Context& ctx, const std::vector<MatJob>& jobs) {
         }
         return;
     }
-    HMB_REQUIRE(n1 < (1LL << 31) && n2 < (1LL << 31) && ct < 65536, HM_ERR_UNSUPPORTED,
-                "batch too large");
-    if (n1 > 0) {
+    HMB_REQUIRE(ct < 65536, HM_ERR_UNSUPPORTED, "too many columns");
+    const size_t wsm = sizeof(WideSmem);
+    if (n1 > 0 && G1 > 0) {
         LaunchScope ls(ctx, "hmm_lowrank_inner");
-        w1_kernel<<<dim3((unsigned)n1, (unsigned)ct), WTHREADS, 0, st>>>(jobs_d, nj, job0);
+        wide_kernel<1><<<dim3((unsigned)G1, (unsigned)ct), WTHREADS, wsm, st>>>(jobs_d, nj, job0, n1, G1);
         HMB_CHECK_LAUNCH();
     }
-    if (n2 > 0) {
+    if (n2 > 0 && G2 > 0) {
         LaunchScope ls(ctx, "hmm_row_tiles");
-        w2_kernel<<<dim3((unsigned)n2, (unsigned)ct), WTHREADS, 0, st>>>(jobs_d, nj, job0, S);
+        wide_kernel<2><<<dim3((unsigned)G2, (unsigned)ct), WTHREADS, wsm, st>>>(jobs_d, nj, job0, n2, G2);
         HMB_CHECK_LAUNCH();
+    }
+    // row tiles without entries: output = beta * output
+    size_t jj = 0;
+    for (size_t i = 0; i < jobs.size(); ++i) {
+        if (jobs[i].k == 0) continue;
+        const JobTemplate& T = *tmpl[i];
+        if (T.nz > 0) {
+            LaunchScope ls(ctx, "hmm_zero_tiles");
+            p2_zero_kernel<<<std::min(T.nz, 4 * ctx.num_sms), 256, 0, st>>>(ex[jj], T.zero_tiles.get(),
+                                                                          T.nz);
+            HMB_CHECK_LAUNCH();
+        }
+        ++jj;
     }
 }
 

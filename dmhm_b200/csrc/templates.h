@@ -53,7 +53,11 @@ struct JobTemplate {
     DeviceBuffer<P2Entry> ent;
     DeviceBuffer<int> zero_tiles;   // tiles without entries (output = beta * output)
     DeviceBuffer<W1Tile> w1;        // wide phase-1 tiles
+    DeviceBuffer<int> w1cp;         // wide: chunk prefix over the W1 tiles
+    DeviceBuffer<int> tcp;          // wide: chunk prefix over the row tiles
+    DeviceBuffer<int> ekc;          // wide: first chunk of every entry within its tile
     int nw1 = 0;
+    long long wc1 = 0, wc2 = 0;     // wide: chunks of phase 1 / phase 2
     // Host copies, and per split width GW the first item / (tile, entry) of
     // every warp of the narrow kernels (built on first use).
     std::vector<P1T> hp1;

@@ -9,9 +9,11 @@ Python mirror of the reference's C++ API.
 """
 from ._lib import HMError, LIB_PATH, lib
 from .hmat import (Context, EstimateTwoNorm, Finalize, HMat2d, HMat3d, Initialize,
-                   Oversample, SetOversample, Sparse, natural_to_hierarchical_map)
+                   Oversample, SetOversample, SetCompressionTolerance, CompressionTolerance,
+                   Sparse, natural_to_hierarchical_map)
 from . import operators
 
 __all__ = ["Context", "EstimateTwoNorm", "Finalize", "HMError", "HMat2d", "HMat3d", "Initialize",
-           "LIB_PATH", "Oversample", "SetOversample", "Sparse", "lib",
+           "LIB_PATH", "Oversample", "SetOversample", "SetCompressionTolerance",
+           "CompressionTolerance", "Sparse", "lib",
            "natural_to_hierarchical_map", "operators"]

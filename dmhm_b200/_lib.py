@@ -48,6 +48,8 @@ SIGNATURES = {
     "hm_context_synchronize": [_P],
     "hm_set_oversample": [_P, _I],
     "hm_get_oversample": [_P, _PI],
+    "hm_set_compression_tolerance": [_P, _D],
+    "hm_get_compression_tolerance": [_P, _PD],
     "hm_set_lcg_states": [_P, _U64, _U64],
     "hm_get_lcg_states": [_P, _PU64, _PU64],
     "hm_natural_to_hierarchical_map": [_I, _PI, _I, _PI],

@@ -262,6 +262,21 @@ int hm_get_oversample(hm_context ctx, int* oversample) {
     });
 }
 
+int hm_set_compression_tolerance(hm_context ctx, double tol) {
+    return guarded([&] {
+        HMB_REQUIRE(ctx, HM_ERR_ARGUMENT, "ctx is NULL");
+        HMB_REQUIRE(tol >= 0.0 && tol < 1.0, HM_ERR_ARGUMENT, "tolerance must be in [0, 1)");
+        ctx->c.compression_tol = tol;
+    });
+}
+
+int hm_get_compression_tolerance(hm_context ctx, double* tol) {
+    return guarded([&] {
+        HMB_REQUIRE(ctx && tol, HM_ERR_ARGUMENT, "NULL argument");
+        *tol = ctx->c.compression_tol;
+    });
+}
+
 int hm_set_lcg_states(hm_context ctx, uint64_t serial, uint64_t parallel) {
     return guarded([&] {
         HMB_REQUIRE(ctx, HM_ERR_ARGUMENT, "ctx is NULL");

@@ -31,6 +31,12 @@ struct Context {
     // Next raw state of the serial / parallel LCG (src/core/random.cpp:13-25).
     uint64_t serial_state = 0, parallel_state = 0;
     int num_sms = 148;
+    // Relative truncation tolerance of the H*H compressions: 0 keeps the
+    // reference's fixed rank maxRank; > 0 drops singular values at or below
+    // tol * sigma_0 (capped at maxRank) and stores the products at the ranks
+    // kept (CompressionTolerance, src/core/global.cpp:155-181; SVDTrunc,
+    // src/DistHMat2d/Truncation-incl.hpp:37-63).
+    double compression_tol = 0.0;
     // Work lists and scratch are stream-ordered allocations (cudaMallocAsync
     // / cudaFreeAsync on `stream`), freed right after the launches that use
     // them are queued.

@@ -35,6 +35,7 @@
 
 #include "dense_ops.h"
 #include "lowrank.h"
+#include "schulz.h"
 #include "rng.cuh"
 
 namespace hmb {
@@ -509,6 +510,7 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
             op.vo = const_cast<double*>(t.V);
             op.work = S0 + t.s_work;
             op.alpha = 1.0;
+            op.tol = ctx.compression_tol;
             ops.push_back(op);
         }
         launch_round_ops(ctx, ops, "sample_round");
@@ -639,6 +641,7 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
                 }
                 r.u2 = cu;
                 r.v2 = cv;
+                r.tol = ctx.compression_tol;
                 r.r2 = (op.type == L_SET || (op.type == L_DDC && op.beta == 0.0)) ? 0 : cr;
                 r.ldu2 = Cb.m;
                 r.ldv2 = Cb.n;
@@ -691,6 +694,8 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
     // low-rank C blocks whose final rank is 0 or that received no operation
     // need nothing: their storage is empty.
     ctx.serial_state = serial_after;
+    // tolerance truncation: store C at the ranks kept
+    if (ctx.compression_tol > 0.0) compact_ranks(ctx, C);
 }
 
 }  // namespace hmb

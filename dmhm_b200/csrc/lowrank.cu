@@ -331,23 +331,36 @@ __device__ void do_round(const RoundOp& op, double* dyn, long long smem_doubles,
     cta_order_columns(M, ku, kv, norms, order);
 
     // ---- outputs -------------------------------------------------------------
+    // columns kept: at most rout and the core's size; with a tolerance, the
+    // singular values above tol * sigma_0 (norms holds squared values)
+    int keep = min(rout, min(ku, kv));
+    if (op.tol > 0.0 && keep > 0) {
+        const double s0 = norms[order[0]];
+        const double t2 = op.tol * op.tol;
+        int c = 0;
+        if (s0 >= t2 * t2)
+            while (c < keep && norms[order[c]] > t2 * s0) ++c;
+        keep = c;
+    }
     if (ortho) {
         for (long long e = tid; e < (long long)m * rout; e += kT) {
             int i = (int)(e % m), c = (int)(e / m);
-            const double* g = M + (long long)order[c] * ku;
             double v = 0.0;
-            for (int p = 0; p < ku; ++p) v = fma(op.u1[i + (long long)p * op.ldu1], g[p], v);
+            if (c < keep) {
+                const double* g = M + (long long)order[c] * ku;
+                for (int p = 0; p < ku; ++p) v = fma(op.u1[i + (long long)p * op.ldu1], g[p], v);
+            }
             op.uo[e] = v;
         }
     } else {
         for (long long e = tid; e < (long long)m * rout; e += kT) {
             int i = (int)(e % m), c = (int)(e / m);
-            op.uo[e] = i < ku ? M[i + (long long)order[c] * ku] : 0.0;
+            op.uo[e] = (i < ku && c < keep) ? M[i + (long long)order[c] * ku] : 0.0;
         }
     }
     for (long long e = tid; e < (long long)n * rout; e += kT) {
         int i = (int)(e % n), c = (int)(e / n);
-        op.vo[e] = i < kv ? J[i + (long long)order[c] * kv] : 0.0;
+        op.vo[e] = (i < kv && c < keep) ? J[i + (long long)order[c] * kv] : 0.0;
     }
     __syncthreads();
     if (!ortho) cta_apply_q(Ucat, m, min(m, k), m, tauU, op.uo, rout, m);

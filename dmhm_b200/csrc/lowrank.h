@@ -25,6 +25,10 @@ struct RoundOp {
     double alpha, beta;
     int kind, m, n, r1, r2, rout;
     int ldu1, ldv1, ldu2, ldv2;
+    // > 0: also drop the singular values at or below tol * sigma_0 (all of
+    // them when sigma_0 < tol^2), writing zero columns in their place
+    // (GENERAL, DENSE, ORTHO).
+    double tol;
 };
 
 // Scratch doubles one op needs (0 for SET / CONCAT).

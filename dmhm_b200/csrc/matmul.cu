@@ -373,13 +373,36 @@ p2_stream_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0
     }
 }
 
-// Row tiles without entries: output = beta * output (alpha times an empty sum).
-__global__ void p2_zero_kernel(const JobExec J, const int* __restrict__ tiles, int n) {
+// Row tiles without entries, over all jobs of a launch (list of (job, tile)):
+// output = beta * output (alpha times an empty sum).
+__global__ void p2_zero_kernel(const JobExec* __restrict__ jobs, const JobExec job0,
+                               const int2* __restrict__ list, int n) {
     for (int t = blockIdx.x; t < n; t += gridDim.x) {
-        const P2T it = J.p2[tiles[t]];
+        const int2 jt = list[t];
+        const JobExec& J = jobs ? jobs[jt.x] : job0;
+        const P2T it = J.p2[jt.y];
         for (int o = threadIdx.x; o < it.rows * J.k; o += blockDim.x)
             store_out(J, it, o % it.rows, o / it.rows, 0.0);
     }
+}
+
+// One launch for the tiles without entries of every job.
+void launch_zero_tiles(Context& ctx, const std::vector<std::shared_ptr<JobTemplate>>& tmpl,
+                       const std::vector<MatJob>& jobs, const JobExec* jobs_d, const JobExec& job0) {
+    std::vector<int2> list;
+    int j = 0;
+    for (size_t i = 0; i < jobs.size(); ++i) {
+        if (jobs[i].k == 0) continue;
+        for (int t : tmpl[i]->hzero) list.push_back(make_int2(j, t));
+        ++j;
+    }
+    if (list.empty()) return;
+    DeviceBuffer<int2> d;
+    d.upload(list, ctx.stream);
+    LaunchScope ls(ctx, "hmm_zero_tiles");
+    p2_zero_kernel<<<std::min((int)list.size(), 4 * ctx.num_sms), 256, 0, ctx.stream>>>(
+        jobs_d, job0, d.get(), (int)list.size());
+    HMB_CHECK_LAUNCH();
 }
 
 // ---------------------------------------------------------------------------
@@ -865,6 +888,7 @@ std::shared_ptr<JobTemplate> build_template(Context& ctx, const HMatrix& H, int 
     T->p2.upload(p2, ctx.stream);
     T->ent.upload(ent, ctx.stream);
     T->zero_tiles.upload(zero, ctx.stream);
+    T->hzero = zero;
     T->nw1 = (int)w1.size();
     T->w1.upload(w1, ctx.stream);
     if (row_tile > 32) {
@@ -1133,18 +1157,7 @@ void run_jobs(Context& ctx, const std::vector<MatJob>& jobs) {
         if (kmax <= 1) launch_narrow<1>(ctx, jobs_d, nj, job0, n1, n2, rmax, single);
         else if (kmax <= 4) launch_narrow<4>(ctx, jobs_d, nj, job0, n1, n2, rmax, single);
         else launch_narrow<8>(ctx, jobs_d, nj, job0, n1, n2, rmax, single);
-        size_t j = 0;
-        for (size_t i = 0; i < jobs.size(); ++i) {
-            if (jobs[i].k == 0) continue;
-            const JobTemplate& T = *tmpl[i];
-            if (T.nz > 0) {
-                LaunchScope ls(ctx, "hmm_zero_tiles");
-                p2_zero_kernel<<<std::min(T.nz, 4 * ctx.num_sms), 256, 0, st>>>(
-                    ex[j], T.zero_tiles.get(), T.nz);
-                HMB_CHECK_LAUNCH();
-            }
-            ++j;
-        }
+        launch_zero_tiles(ctx, tmpl, jobs, jobs_d, job0);
         return;
     }
     HMB_REQUIRE(ct < 65536, HM_ERR_UNSUPPORTED, "too many columns");
@@ -1160,18 +1173,7 @@ void run_jobs(Context& ctx, const std::vector<MatJob>& jobs) {
         HMB_CHECK_LAUNCH();
     }
     // row tiles without entries: output = beta * output
-    size_t jj = 0;
-    for (size_t i = 0; i < jobs.size(); ++i) {
-        if (jobs[i].k == 0) continue;
-        const JobTemplate& T = *tmpl[i];
-        if (T.nz > 0) {
-            LaunchScope ls(ctx, "hmm_zero_tiles");
-            p2_zero_kernel<<<std::min(T.nz, 4 * ctx.num_sms), 256, 0, st>>>(ex[jj], T.zero_tiles.get(),
-                                                                          T.nz);
-            HMB_CHECK_LAUNCH();
-        }
-        ++jj;
-    }
+    launch_zero_tiles(ctx, tmpl, jobs, jobs_d, job0);
 }
 
 }  // namespace hmb

@@ -126,6 +126,78 @@ __global__ void set_scalar_kernel(double* p, double v) { *p = v; }
 // ---------------------------------------------------------------------------
 // Elementwise H-matrix operations
 // ---------------------------------------------------------------------------
+// Rank actually used by each listed low-rank block: 1 + the last column of U
+// with a nonzero entry (tolerance truncation leaves zero columns behind).
+__global__ void rank_scan_kernel(const double* const* __restrict__ U, const int* __restrict__ m,
+                                 const int* __restrict__ r, int* __restrict__ out) {
+    const int b = blockIdx.x;
+    const double* u = U[b];
+    const int rows = m[b];
+    int used = 0;
+    for (int c = r[b] - 1; c >= 0; --c) {
+        int nz = 0;
+        for (int i = threadIdx.x; i < rows; i += blockDim.x) nz |= u[i + (long long)c * rows] != 0.0;
+        if (__syncthreads_or(nz)) {
+            used = c + 1;
+            break;
+        }
+    }
+    if (threadIdx.x == 0) out[b] = used;
+}
+
+void compact_ranks(Context& ctx, HMatrix& H) {
+    const Structure& S = *H.S;
+    std::vector<int> blocks;
+    std::vector<const double*> up;
+    std::vector<int> ms, rs;
+    for (int b : S.leaves) {
+        const Block& B = S.blocks[b];
+        if (B.kind != KIND_LOWRANK || H.rank[b] == 0 || B.m == 0 || B.n == 0) continue;
+        blocks.push_back(b);
+        up.push_back(H.U(b));
+        ms.push_back(B.m);
+        rs.push_back(H.rank[b]);
+    }
+    if (blocks.empty()) return;
+    DeviceBuffer<const double*> du;
+    DeviceBuffer<int> dm, dr, dout;
+    du.upload(up, ctx.stream);
+    dm.upload(ms, ctx.stream);
+    dr.upload(rs, ctx.stream);
+    dout.allocate(blocks.size(), ctx.stream);
+    {
+        LaunchScope ls(ctx, "rank_scan");
+        rank_scan_kernel<<<(unsigned)blocks.size(), 128, 0, ctx.stream>>>(du.get(), dm.get(), dr.get(),
+                                                                          dout.get());
+        HMB_CHECK_LAUNCH();
+    }
+    std::vector<int> used(blocks.size());
+    HMB_CUDA(cudaMemcpyAsync(used.data(), dout.get(), used.size() * sizeof(int),
+                             cudaMemcpyDeviceToHost, ctx.stream));
+    HMB_CUDA(cudaStreamSynchronize(ctx.stream));
+    bool same = true;
+    for (size_t i = 0; i < blocks.size(); ++i) same &= used[i] == rs[i];
+    if (same) return;
+    // re-lay out with the used ranks and copy the kept columns over
+    DeviceBuffer<double> old = std::move(H.data);
+    const std::vector<long long> old_off = H.off;
+    const std::vector<int> old_rank = H.rank;
+    for (size_t i = 0; i < blocks.size(); ++i) H.rank[blocks[i]] = used[i];
+    H.layout();
+    std::vector<CopyTask> tasks;
+    for (int b : S.leaves) {
+        const Block& B = S.blocks[b];
+        const double* src = old.get() + old_off[b];
+        if (B.kind == KIND_DENSE) {
+            tasks.push_back({src, H.D(b), 1.0, B.m, B.n, B.m, 0});
+        } else if (H.rank[b] > 0) {
+            tasks.push_back({src, H.U(b), 1.0, B.m, H.rank[b], B.m, 0});
+            tasks.push_back({src + (long long)B.m * old_rank[b], H.V(b), 1.0, B.n, H.rank[b], B.n, 0});
+        }
+    }
+    launch_copy_tasks(ctx, tasks, "rank_compact");
+}
+
 void hmat_copy(Context& ctx, const HMatrix& src, HMatrix& dst) {
     HMB_REQUIRE(&src != &dst, HM_ERR_ARGUMENT, "copy onto itself");
     dst.ctx = &ctx;

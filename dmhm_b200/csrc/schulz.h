@@ -12,6 +12,9 @@ struct SchulzResult {
 };
 
 double estimate_two_norm(Context& ctx, HMatrix& A, double theta, double confidence);
+// Drops the trailing zero columns that tolerance truncation leaves in the
+// low-rank blocks (synchronizes to read the ranks back).
+void compact_ranks(Context& ctx, HMatrix& H);
 SchulzResult schulz_invert(Context& ctx, HMatrix& A, int num_iterations, double theta,
                            double confidence, double stop_tol);
 

@@ -64,6 +64,7 @@ struct JobTemplate {
     std::vector<P2T> hp2;
     std::vector<P2Entry> hent;
     std::vector<int> hent_block;    // leaf block of every entry
+    std::vector<int> hzero;         // tiles without entries
     // Block-streamed one-vector product plan (matvec.cu); null when the
     // blocks do not fit its limits.
     std::shared_ptr<struct MvPlan> mv;

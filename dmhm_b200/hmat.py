@@ -63,6 +63,14 @@ class Context:
         check(lib().hm_get_oversample(self._h, C.byref(v)))
         return v.value
 
+    def set_compression_tolerance(self, tol: float):
+        check(lib().hm_set_compression_tolerance(self._h, float(tol)))
+
+    def compression_tolerance(self) -> float:
+        v = C.c_double()
+        check(lib().hm_get_compression_tolerance(self._h, C.byref(v)))
+        return v.value
+
     def lcg_states(self):
         s, p = C.c_uint64(), C.c_uint64()
         check(lib().hm_get_lcg_states(self._h, C.byref(s), C.byref(p)))
@@ -114,6 +122,16 @@ def SetOversample(p: int, ctx: Optional[Context] = None):
 def Oversample(ctx: Optional[Context] = None) -> int:
     """Oversample (global.cpp:152-153)."""
     return _ctx(ctx).oversample()
+
+
+def SetCompressionTolerance(tol: float, ctx: Optional[Context] = None):
+    """SetCompressionTolerance (global.cpp:160-181): relative truncation of
+    the H*H compressions (0 = the fixed rank maxRank)."""
+    _ctx(ctx).set_compression_tolerance(tol)
+
+
+def CompressionTolerance(ctx: Optional[Context] = None) -> float:
+    return _ctx(ctx).compression_tolerance()
 
 
 def _as_i32(a):

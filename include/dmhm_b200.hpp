@@ -54,6 +54,13 @@ inline int Oversample() {
     return p;
 }
 inline void SetOversample(int oversample) { Check(hm_set_oversample(Context(), oversample)); }
+// SetCompressionTolerance / CompressionTolerance (src/core/global.cpp:160-181).
+inline void SetCompressionTolerance(double tol) { Check(hm_set_compression_tolerance(Context(), tol)); }
+inline double CompressionTolerance() {
+    double t = 0.0;
+    Check(hm_get_compression_tolerance(Context(), &t));
+    return t;
+}
 
 // SeedSerialLcg (src/core/random.cpp:67-68): restart the serial generator
 // (the one the randomized H*H sampling and EstimateTwoNorm draw from).

@@ -497,6 +497,26 @@ def lr_times_lr(alpha, A: LR, B: LR) -> LR:
     return LR(alpha * (A.U @ W), B.V.copy())
 
 
+# CompressionTolerance (src/core/global.cpp:160-181): 0 keeps the fixed rank
+# of HMat2d; > 0 truncates every SVD as the single-rank DistHMat does
+# (SVDTrunc, src/DistHMat2d/Truncation-incl.hpp:37-63): keep the singular
+# values above tol * sigma_0, none when sigma_0 < tol^2, at most the rank cap.
+_COMPRESSION_TOL = [0.0]
+
+
+def set_compression_tolerance(tol: float):
+    _COMPRESSION_TOL[0] = float(tol)
+
+
+def _kept(s: np.ndarray, cap: int) -> int:
+    tol = _COMPRESSION_TOL[0]
+    if tol <= 0.0:
+        return cap
+    if s.size == 0 or s[0] < tol * tol:
+        return 0
+    return int(min(cap, np.count_nonzero(s > tol * s[0])))
+
+
 def rounded_update(max_rank: int, alpha, A: LR, beta, B: LR) -> LR:
     """B :~= alpha A + beta B (src/hmat_tools/RoundedUpdate.cpp:14-162)."""
     m, n = A.U.shape[0], A.V.shape[0]
@@ -511,6 +531,7 @@ def rounded_update(max_rank: int, alpha, A: LR, beta, B: LR) -> LR:
     QV, RV = sla.qr(V, mode="economic")
     W = RU @ RV.T
     Uw, s, VTw = sla.svd(W, full_matrices=False, lapack_driver="gesvd")
+    rr = _kept(s, rr)
     return LR(QU @ (Uw[:, :rr] * s[:rr]), QV @ VTw[:rr].T)
 
 
@@ -520,6 +541,7 @@ def compress_dense(max_rank: int, D: np.ndarray) -> LR:
     m, n = D.shape
     r = min(m, n, max_rank)
     U, s, VT = sla.svd(D, full_matrices=False, lapack_driver="gesvd")
+    r = _kept(s, r)
     return LR(U[:, :r].copy(), VT[:r].T * s[:r])
 
 
@@ -533,6 +555,7 @@ def randomized_product(sample_rank: int, alpha, A: HMat, B: HMat, rng: Rng) -> L
     X = transpose_multiply_dense(A, alpha, Q)
     FV = transpose_multiply_dense(B, 1.0, X)
     Us, s, VT = sla.svd(FV, full_matrices=False, lapack_driver="gesvd")
+    r = _kept(s, min(r, s.size))
     V = Us[:, :r].copy()
     U = Q @ (VT[:r].T * s[:r])
     return LR(U, V)

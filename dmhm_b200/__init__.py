@@ -10,10 +10,10 @@ Python mirror of the reference's C++ API.
 from ._lib import HMError, LIB_PATH, lib
 from .hmat import (Context, EstimateTwoNorm, Finalize, HMat2d, HMat3d, Initialize,
                    Oversample, SetOversample, SetCompressionTolerance, CompressionTolerance,
-                   Sparse, natural_to_hierarchical_map)
+                   RankModel, Sparse, natural_to_hierarchical_map)
 from . import operators
 
 __all__ = ["Context", "EstimateTwoNorm", "Finalize", "HMError", "HMat2d", "HMat3d", "Initialize",
            "LIB_PATH", "Oversample", "SetOversample", "SetCompressionTolerance",
-           "CompressionTolerance", "Sparse", "lib",
+           "CompressionTolerance", "RankModel", "Sparse", "lib",
            "natural_to_hierarchical_map", "operators"]

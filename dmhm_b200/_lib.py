@@ -38,6 +38,7 @@ _PD = C.POINTER(C.c_double)
 _PI64 = C.POINTER(C.c_int64)
 _PI32 = C.POINTER(C.c_int32)
 _PU64 = C.POINTER(C.c_uint64)
+_PF = C.POINTER(C.c_float)
 
 # name -> argtypes (all return int status unless listed in _RESTYPES)
 SIGNATURES = {
@@ -69,11 +70,25 @@ SIGNATURES = {
     "hm_add_constant_to_diagonal": [_P, _D],
     "hm_multiply_vector_noalloc": [_P, _I, _D, _P, _D, _P],
     "hm_multiply_dense_tf32": [_P, _D, _P, _I, _D, _P, _I, _I],
+    "hm_rank_feature_count": [],
+    "hm_rank_param_count": [],
+    "hm_rank_model_create": [_P, _U64, C.POINTER(_P)],
+    "hm_rank_model_destroy": [_P],
+    "hm_rank_model_set_params": [_P, _PF, _I],
+    "hm_rank_model_get_params": [_P, _PF, _I],
+    "hm_rank_model_loss_grad": [_P, _PF, _PF, _I, _PF, _PF],
+    "hm_rank_model_train": [_P, _PF, _PF, _I, _I, C.c_float, _PF],
+    "hm_rank_model_predict": [_P, _PF, _I, _PF],
+    "hm_use_rank_model": [_P, _P, _I, _I],
+    "hm_rank_log_enable": [_P, _I],
+    "hm_rank_log_read": [_P, _PF, _PF, _I, _PI, _I],
+    "hm_rank_stats": [_P, _PI64, _PI64, _PI64, _PI64],
     "hm_kernel_launches": [],
     "hm_profile_enable": [_P, _I],
     "hm_profile_read": [_P, _I, C.c_char_p, _I, _PD, _PI64],
 }
 _RESTYPES = {"hm_last_error": C.c_char_p, "hm_version": C.c_int,
+             "hm_rank_feature_count": C.c_int, "hm_rank_param_count": C.c_int,
              "hm_kernel_launches": C.c_ulonglong}
 
 

@@ -6,6 +6,7 @@
 #include <string>
 
 #include "engine.h"
+#include "mlp.h"
 #include "hh.h"
 #include "rng.cuh"
 #include "schulz.h"
@@ -15,10 +16,16 @@ struct hm_matrix_s;
 struct hm_context_s {
     hmb::Context c;
     std::set<hm_matrix_s*> live;   // handles created on this context
+    std::set<struct hm_rank_model_s*> models;
 };
 
 struct hm_matrix_s {
     hmb::HMatrix h;
+    hm_context_s* owner = nullptr;
+};
+
+struct hm_rank_model_s {
+    hmb::RankModel m;
     hm_context_s* owner = nullptr;
 };
 
@@ -231,6 +238,16 @@ int hm_context_destroy(hm_context ctx) {
             m->h.ctx = nullptr;
         }
         ctx->live.clear();
+        for (hm_rank_model_s* m : ctx->models) {
+            m->m.params.reset();
+            m->m.grad.reset();
+            m->m.m.reset();
+            m->m.v.reset();
+            m->m.ctx = nullptr;
+            m->owner = nullptr;
+        }
+        ctx->models.clear();
+        ctx->c.rank_model = nullptr;
         ctx->c.collect();
         ctx->c.counters.reset();
         ctx->c.errword.reset();
@@ -541,6 +558,130 @@ int hm_profile_read(hm_context ctx, int index, char* name, int name_cap, double*
         std::snprintf(name, (size_t)name_cap, "%s", it->first.c_str());
         *ms = it->second.ms;
         *launches = it->second.launches;
+    });
+}
+
+// ---------------------------------------------------------------------------
+// Learned sample counts
+// ---------------------------------------------------------------------------
+int hm_rank_feature_count(void) { return hmb::kMlpFeatures; }
+int hm_rank_param_count(void) { return hmb::kMlpParams; }
+
+int hm_rank_model_create(hm_context ctx, uint64_t seed, hm_rank_model* out) {
+    return guarded([&] {
+        HMB_REQUIRE(ctx && out, HM_ERR_ARGUMENT, "NULL argument");
+        auto* m = new hm_rank_model_s();
+        m->owner = ctx;
+        m->m.ctx = &ctx->c;
+        try {
+            m->m.init(seed);
+        } catch (...) {
+            delete m;
+            throw;
+        }
+        ctx->models.insert(m);
+        *out = m;
+    });
+}
+
+int hm_rank_model_destroy(hm_rank_model m) {
+    return guarded([&] {
+        if (!m) return;
+        if (m->owner) {
+            if (m->owner->c.rank_model == &m->m) m->owner->c.rank_model = nullptr;
+            m->owner->models.erase(m);
+        }
+        delete m;
+    });
+}
+
+int hm_rank_model_set_params(hm_rank_model m, const float* params, int n) {
+    return guarded([&] {
+        HMB_REQUIRE(m && m->owner && params, HM_ERR_ARGUMENT, "NULL argument");
+        HMB_REQUIRE(n == hmb::kMlpParams, HM_ERR_ARGUMENT, "wrong parameter count");
+        m->m.set_params(params);
+    });
+}
+
+int hm_rank_model_get_params(hm_rank_model m, float* params, int n) {
+    return guarded([&] {
+        HMB_REQUIRE(m && m->owner && params, HM_ERR_ARGUMENT, "NULL argument");
+        HMB_REQUIRE(n == hmb::kMlpParams, HM_ERR_ARGUMENT, "wrong parameter count");
+        m->m.get_params(params);
+    });
+}
+
+int hm_rank_model_loss_grad(hm_rank_model m, const float* x, const float* t, int n, float* loss,
+                            float* grad) {
+    return guarded([&] {
+        HMB_REQUIRE(m && m->owner && x && t && loss, HM_ERR_ARGUMENT, "NULL argument");
+        HMB_REQUIRE(n > 0, HM_ERR_ARGUMENT, "empty batch");
+        *loss = m->m.loss_and_grad(x, t, n, grad);
+    });
+}
+
+int hm_rank_model_train(hm_rank_model m, const float* x, const float* t, int n, int epochs,
+                        float lr, float* loss) {
+    return guarded([&] {
+        HMB_REQUIRE(m && m->owner && x && t, HM_ERR_ARGUMENT, "NULL argument");
+        const float l = m->m.train(x, t, n, epochs, lr);
+        if (loss) *loss = l;
+    });
+}
+
+int hm_rank_model_predict(hm_rank_model m, const float* x, int n, float* out) {
+    return guarded([&] {
+        HMB_REQUIRE(m && m->owner && x && out, HM_ERR_ARGUMENT, "NULL argument");
+        HMB_REQUIRE(n >= 0, HM_ERR_ARGUMENT, "negative count");
+        m->m.predict(x, n, out);
+    });
+}
+
+int hm_use_rank_model(hm_context ctx, hm_rank_model m, int margin, int probes) {
+    return guarded([&] {
+        HMB_REQUIRE(ctx, HM_ERR_ARGUMENT, "ctx is NULL");
+        HMB_REQUIRE(!m || m->owner == ctx, HM_ERR_ARGUMENT, "model belongs to another context");
+        HMB_REQUIRE(margin >= 0 && probes >= 1, HM_ERR_ARGUMENT, "margin >= 0, probes >= 1");
+        ctx->c.rank_model = m ? &m->m : nullptr;
+        ctx->c.rank_margin = margin;
+        ctx->c.rank_probes = probes;
+    });
+}
+
+int hm_rank_log_enable(hm_context ctx, int on) {
+    return guarded([&] {
+        HMB_REQUIRE(ctx, HM_ERR_ARGUMENT, "ctx is NULL");
+        ctx->c.rank_log = on != 0;
+    });
+}
+
+int hm_rank_log_read(hm_context ctx, float* x, float* t, int cap, int* n, int clear) {
+    return guarded([&] {
+        HMB_REQUIRE(ctx && n, HM_ERR_ARGUMENT, "NULL argument");
+        const int have = (int)ctx->c.log_t.size();
+        const int take = std::min(std::max(cap, 0), have);
+        if (take > 0) {
+            HMB_REQUIRE(x && t, HM_ERR_ARGUMENT, "NULL buffers");
+            std::copy(ctx->c.log_x.begin(), ctx->c.log_x.begin() + (long long)take * hmb::kMlpFeatures, x);
+            std::copy(ctx->c.log_t.begin(), ctx->c.log_t.begin() + take, t);
+        }
+        *n = have;
+        if (clear) {
+            ctx->c.log_x.clear();
+            ctx->c.log_t.clear();
+        }
+    });
+}
+
+int hm_rank_stats(hm_context ctx, int64_t* compressions, int64_t* samples, int64_t* samples_plain,
+                  int64_t* fallbacks) {
+    return guarded([&] {
+        HMB_REQUIRE(ctx, HM_ERR_ARGUMENT, "ctx is NULL");
+        const auto& s = ctx->c.rank_stats;
+        if (compressions) *compressions = s.compressions;
+        if (samples) *samples = s.samples;
+        if (samples_plain) *samples_plain = s.samples_plain;
+        if (fallbacks) *fallbacks = s.fallbacks;
     });
 }
 

@@ -37,6 +37,19 @@ struct Context {
     // kept (CompressionTolerance, src/core/global.cpp:155-181; SVDTrunc,
     // src/DistHMat2d/Truncation-incl.hpp:37-63).
     double compression_tol = 0.0;
+    // Learned sample counts of the randomized H*H compressions (mlp.cu):
+    // when set, each compression draws (predicted rank + margin) +
+    // oversample samples, checked by probe vectors.
+    struct RankModel* rank_model = nullptr;
+    int rank_margin = 2;
+    int rank_probes = 4;
+    // Training log: features and kept-rank fractions of every compression
+    // (filled when rank_log is on and a tolerance is set).
+    bool rank_log = false;
+    std::vector<float> log_x, log_t;
+    struct RankStats {
+        long long compressions = 0, samples = 0, samples_plain = 0, fallbacks = 0;
+    } rank_stats;
     // Work lists and scratch are stream-ordered allocations (cudaMallocAsync
     // / cudaFreeAsync on `stream`), freed right after the launches that use
     // them are queued.

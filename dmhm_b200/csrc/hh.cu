@@ -31,11 +31,13 @@
 #include "hh.h"
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 
 #include "dense_ops.h"
 #include "lowrank.h"
 #include "schulz.h"
+#include "mlp.h"
 #include "rng.cuh"
 
 namespace hmb {
@@ -277,6 +279,177 @@ struct Arena {
     }
 };
 
+// Features of the randomized compressions (the rank predictor's inputs, all
+// in [0, 1] roughly):
+//   0 level / numLevels      1 log2(1 + m) / 16     2 log2(1 + n) / 16
+//   3 admissibility distance max|coord_t - coord_s| / 8 (capped at 1)
+//   4, 5 mean rank of the low-rank leaves below A's / B's block / maxRank
+//   6, 7 share of dense entries below A's / B's block
+//   8 rank cap of the product / maxRank             9 dimension / 3
+struct SubtreeStat {
+    double rank_sum = 0, lr_count = 0, dense_entries = 0, lr_entries = 0;
+    bool done = false;
+};
+
+void subtree_stats(const Structure& S, const HMatrix& H, int b, std::vector<SubtreeStat>& st) {
+    if (st[b].done) return;
+    SubtreeStat s;
+    const Block& B = S.blocks[b];
+    if (B.kind == KIND_NODE) {
+        for (int c = 0; c < S.q * S.q; ++c) {
+            const int ch = B.first_child + c;
+            subtree_stats(S, H, ch, st);
+            s.rank_sum += st[ch].rank_sum;
+            s.lr_count += st[ch].lr_count;
+            s.dense_entries += st[ch].dense_entries;
+            s.lr_entries += st[ch].lr_entries;
+        }
+    } else if (B.kind == KIND_DENSE) {
+        s.dense_entries = (double)B.m * B.n;
+    } else {
+        s.rank_sum = H.rank[b];
+        s.lr_count = 1;
+        s.lr_entries = (double)(B.m + B.n) * H.rank[b];
+    }
+    s.done = true;
+    st[b] = s;
+}
+
+std::vector<float> rank_features(const Structure& S, const HMatrix& A, const HMatrix& B,
+                                 const std::vector<WTask>& w, const std::vector<int>& ids,
+                                 int maxRank) {
+    std::vector<SubtreeStat> sa(S.blocks.size()), sb(S.blocks.size());
+    std::vector<float> f;
+    f.reserve(ids.size() * kMlpFeatures);
+    const float mr = (float)std::max(1, maxRank);
+    for (int i : ids) {
+        const WTask& t = w[i];
+        subtree_stats(S, A, t.a, sa);
+        subtree_stats(S, B, t.b, sb);
+        const Block& Ba = S.blocks[t.a];
+        const Block& Bb = S.blocks[t.b];
+        const Box& tb = S.boxes[Ba.tgt_box];
+        const Box& xb = S.boxes[Bb.src_box];
+        int dist = 0;
+        for (int d = 0; d < S.dim; ++d) dist = std::max(dist, std::abs(tb.coord[d] - xb.coord[d]));
+        const SubtreeStat& A1 = sa[t.a];
+        const SubtreeStat& B1 = sb[t.b];
+        auto frac = [](double d, double l) { return (float)(d + l > 0 ? d / (d + l) : 0.0); };
+        f.push_back((float)Ba.level / (float)std::max(1, S.num_levels));
+        f.push_back(std::log2(1.0f + (float)t.m) / 16.0f);
+        f.push_back(std::log2(1.0f + (float)t.n) / 16.0f);
+        f.push_back(std::min(1.0f, (float)dist / 8.0f));
+        f.push_back(A1.lr_count > 0 ? (float)(A1.rank_sum / A1.lr_count) / mr : 0.0f);
+        f.push_back(B1.lr_count > 0 ? (float)(B1.rank_sum / B1.lr_count) / mr : 0.0f);
+        f.push_back(frac(A1.dense_entries, A1.lr_entries));
+        f.push_back(frac(B1.dense_entries, B1.lr_entries));
+        f.push_back((float)t.r / mr);
+        f.push_back((float)S.dim / 3.0f);
+    }
+    return f;
+}
+
+__global__ void sq_norms_kernel(const double* const* __restrict__ p, const long long* __restrict__ n,
+                                double* __restrict__ out) {
+    __shared__ double red[256];
+    const double* x = p[blockIdx.x];
+    double s = 0.0;
+    for (long long e = threadIdx.x; e < n[blockIdx.x]; e += 256) s = fma(x[e], x[e], s);
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[blockIdx.x] = red[0];
+}
+
+// Squared Frobenius norms of the listed (pointer, length) arrays (host result).
+std::vector<double> sq_norms(Context& ctx, const std::vector<const double*>& ptr,
+                             const std::vector<long long>& len) {
+    std::vector<double> out(ptr.size(), 0.0);
+    if (ptr.empty()) return out;
+    DeviceBuffer<const double*> dp;
+    DeviceBuffer<long long> dl;
+    DeviceBuffer<double> dout;
+    dp.upload(ptr, ctx.stream);
+    dl.upload(len, ctx.stream);
+    dout.allocate(ptr.size(), ctx.stream);
+    {
+        LaunchScope ls(ctx, "probe_norms");
+        sq_norms_kernel<<<(unsigned)ptr.size(), 256, 0, ctx.stream>>>(dp.get(), dl.get(), dout.get());
+        HMB_CHECK_LAUNCH();
+    }
+    HMB_CUDA(cudaMemcpyAsync(out.data(), dout.get(), out.size() * sizeof(double),
+                             cudaMemcpyDeviceToHost, ctx.stream));
+    HMB_CUDA(cudaStreamSynchronize(ctx.stream));
+    return out;
+}
+
+// Relative error of every listed compression W ~= alpha A_a B_b, estimated
+// with q Gaussian probe vectors G: ||A (alpha B G) - U (V^T G)|| / ||A (alpha B G)||.
+std::vector<double> probe_errors(Context& ctx, const Structure& S, const HMatrix& A,
+                                 const HMatrix& B, const std::vector<WTask>& w,
+                                 const std::vector<int>& ids) {
+    const int q = std::max(1, ctx.rank_probes);
+    Arena ar;
+    std::vector<long long> g_off(ids.size()), x_off(ids.size()), y_off(ids.size()), v_off(ids.size());
+    for (size_t i = 0; i < ids.size(); ++i) {
+        const WTask& t = w[ids[i]];
+        g_off[i] = ar.take((long long)S.blocks[t.b].n * q);
+        x_off[i] = ar.take((long long)S.blocks[t.b].m * q);
+        y_off[i] = ar.take((long long)t.m * q);
+        v_off[i] = ar.take((long long)t.r * q);
+    }
+    DeviceBuffer<double> buf;
+    buf.allocate((size_t)std::max<long long>(ar.used, 2), ctx.stream);
+    double* P0 = buf.get();
+    // probes from the parallel generator's stream, past the current state
+    uint64_t state = lcg_skip_host(ctx.parallel_state, 0x5DEECE66DULL);
+    std::vector<FillOp> fills;
+    for (size_t i = 0; i < ids.size(); ++i) {
+        const int n = S.blocks[w[ids[i]].b].n;
+        fills.push_back({P0 + g_off[i], state, n, q});
+        state = lcg_skip_host(state, 2ULL * (uint64_t)q * (uint64_t)(n + 1));
+    }
+    launch_gaussian_fills(ctx, fills, "probe_fill");
+    std::vector<MatJob> jobs;
+    for (size_t i = 0; i < ids.size(); ++i) {
+        const WTask& t = w[ids[i]];
+        const Block& Bb = S.blocks[t.b];
+        jobs.push_back({&B, t.b, false, t.alpha, 0.0, P0 + g_off[i], Bb.n, P0 + x_off[i], Bb.m, q});
+    }
+    run_jobs(ctx, jobs);
+    jobs.clear();
+    for (size_t i = 0; i < ids.size(); ++i) {
+        const WTask& t = w[ids[i]];
+        const Block& Ba = S.blocks[t.a];
+        jobs.push_back({&A, t.a, false, 1.0, 0.0, P0 + x_off[i], Ba.n, P0 + y_off[i], Ba.m, q});
+    }
+    run_jobs(ctx, jobs);
+    std::vector<const double*> ptr(ids.size());
+    std::vector<long long> len(ids.size());
+    for (size_t i = 0; i < ids.size(); ++i) {
+        ptr[i] = P0 + y_off[i];
+        len[i] = (long long)w[ids[i]].m * q;
+    }
+    const std::vector<double> ref = sq_norms(ctx, ptr, len);
+    std::vector<GemmOp> g1, g2;
+    for (size_t i = 0; i < ids.size(); ++i) {
+        const WTask& t = w[ids[i]];
+        // VG = V^T G (r x q); Y -= U VG
+        g1.push_back({t.V, P0 + g_off[i], P0 + v_off[i], 1.0, 0.0, t.r, q, t.n, t.ldV, t.n, t.r, 1, 0});
+        g2.push_back({t.U, P0 + v_off[i], P0 + y_off[i], -1.0, 1.0, t.m, q, t.r, t.ldU, t.r, t.m, 0, 0});
+    }
+    launch_gemm_ops(ctx, g1, "probe_vg");
+    launch_gemm_ops(ctx, g2, "probe_residual");
+    const std::vector<double> res = sq_norms(ctx, ptr, len);
+    std::vector<double> rel(ids.size());
+    for (size_t i = 0; i < ids.size(); ++i)
+        rel[i] = ref[i] > 0.0 ? std::sqrt(res[i] / ref[i]) : (res[i] > 0.0 ? 1.0 : 0.0);
+    return rel;
+}
+
 }  // namespace
 
 void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha, double beta,
@@ -426,94 +599,173 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
     std::vector<int> hh;
     for (int i = 0; i < (int)P.w.size(); ++i)
         if (P.w[i].type == W_HH && P.w[i].r > 0) hh.push_back(i);
-    {
-        // Gaussian test matrices: SerialGaussianRandomVectors(Omega), n_b x k
-        std::vector<FillOp> fills;
-        for (int i : hh) {
-            const WTask& t = P.w[i];
-            fills.push_back({S0 + t.s_omega, t.omega, S.blocks[t.b].n, t.k});
-        }
-        launch_gaussian_fills(ctx, fills, "omega_fill");
+    const bool log_ranks = ctx.rank_log && ctx.compression_tol > 0.0 && !hh.empty();
+    const bool learned = ctx.rank_model != nullptr && !hh.empty();
+    std::vector<float> feats;
+    if (log_ranks || learned) feats = rank_features(S, A, B, P.w, hh, maxRankC);
+    std::vector<int> k_plain(hh.size()), kq_plain(hh.size());
+    for (size_t i = 0; i < hh.size(); ++i) {
+        k_plain[i] = P.w[hh[i]].k;
+        kq_plain[i] = P.w[hh[i]].kq;
     }
-    // X = alpha B Omega, and W.U = alpha A B.U for node x low-rank
+    if (learned) {
+        // sample counts from the predicted kept-rank fractions
+        std::vector<float> pred(hh.size());
+        ctx.rank_model->predict(feats.data(), (int)hh.size(), pred.data());
+        for (size_t i = 0; i < hh.size(); ++i) {
+            WTask& t = P.w[hh[i]];
+            int rp = (int)std::ceil(pred[i] * t.r) + ctx.rank_margin;
+            rp = std::max(1, std::min(rp, t.r));
+            t.k = std::min(k_plain[i], rp + ctx.oversample);
+            t.kq = std::min(S.blocks[t.a].m, t.k);
+        }
+    }
+    DeviceBuffer<int> kept;
+    if (log_ranks) kept.allocate(hh.size(), st);
+    // the sampling pipeline for the listed tasks, at their current k
+    auto sample = [&](const std::vector<int>& ids) {
+        {
+            // Gaussian test matrices: SerialGaussianRandomVectors(Omega), n_b x k
+            std::vector<FillOp> fills;
+            for (int i : ids) {
+                const WTask& t = P.w[i];
+                fills.push_back({S0 + t.s_omega, t.omega, S.blocks[t.b].n, t.k});
+            }
+            launch_gaussian_fills(ctx, fills, "omega_fill");
+        }
+        // X = alpha B Omega
+        {
+            std::vector<MatJob> jobs;
+            for (int i : ids) {
+                const WTask& t = P.w[i];
+                const Block& Bb = S.blocks[t.b];
+                jobs.push_back({&B, t.b, false, t.alpha, 0.0, S0 + t.s_omega, Bb.n, S0 + t.s_x,
+                                Bb.m, t.k});
+            }
+            run_jobs(ctx, jobs);
+        }
+        // Y = A X
+        {
+            std::vector<MatJob> jobs;
+            for (int i : ids) {
+                const WTask& t = P.w[i];
+                const Block& Ba = S.blocks[t.a];
+                jobs.push_back({&A, t.a, false, 1.0, 0.0, S0 + t.s_x, Ba.n, S0 + t.s_y, Ba.m, t.k});
+            }
+            run_jobs(ctx, jobs);
+        }
+        // Q = orth(Y)
+        {
+            std::vector<QrOp> q;
+            for (int i : ids) {
+                const WTask& t = P.w[i];
+                q.push_back({S0 + t.s_y, S0 + t.s_q, S0 + t.s_tau, t.m, t.k, t.m, 0});
+            }
+            launch_qr_formq(ctx, q, "sample_qr");
+        }
+        // Z1 = alpha A^T Q
+        {
+            std::vector<MatJob> jobs;
+            for (int i : ids) {
+                const WTask& t = P.w[i];
+                const Block& Ba = S.blocks[t.a];
+                jobs.push_back({&A, t.a, true, t.alpha, 0.0, S0 + t.s_q, Ba.m, S0 + t.s_z1, Ba.n,
+                                t.kq});
+            }
+            run_jobs(ctx, jobs);
+        }
+        // Z = B^T Z1
+        {
+            std::vector<MatJob> jobs;
+            for (int i : ids) {
+                const WTask& t = P.w[i];
+                const Block& Bb = S.blocks[t.b];
+                jobs.push_back({&B, t.b, true, 1.0, 0.0, S0 + t.s_z1, Bb.m, S0 + t.s_z, Bb.n, t.kq});
+            }
+            run_jobs(ctx, jobs);
+        }
+        // W = best rank-r of Q Z^T (the gesvd truncation of hmat_tools.hpp:1712-1745)
+        {
+            std::vector<RoundOp> ops;
+            for (size_t j = 0; j < ids.size(); ++j) {
+                const WTask& t = P.w[ids[j]];
+                RoundOp op{};
+                op.kind = ROUND_ORTHO;
+                op.m = t.m;
+                op.n = t.n;
+                op.u1 = S0 + t.s_q; op.ldu1 = t.m; op.r1 = t.kq;
+                op.v1 = S0 + t.s_z; op.ldv1 = t.n;
+                op.rout = t.r;
+                op.uo = const_cast<double*>(t.U);
+                op.vo = const_cast<double*>(t.V);
+                op.work = S0 + t.s_work;
+                op.alpha = 1.0;
+                op.tol = ctx.compression_tol;
+                if (log_ranks && ids.size() == hh.size()) op.rank_out = kept.get() + j;
+                ops.push_back(op);
+            }
+            launch_round_ops(ctx, ops, "sample_round");
+        }
+    };
+    // W.U = alpha A B.U for node x low-rank, W.V = alpha B^T A.V for
+    // low-rank x node
     {
         std::vector<MatJob> jobs;
-        for (int i : hh) {
-            const WTask& t = P.w[i];
-            const Block& Bb = S.blocks[t.b];
-            jobs.push_back({&B, t.b, false, t.alpha, 0.0, S0 + t.s_omega, Bb.n, S0 + t.s_x, Bb.m,
-                            t.k});
-        }
         for (const WTask& t : P.w)
             if (t.type == W_HLR && t.r > 0)
                 jobs.push_back({&A, t.a, false, t.alpha, 0.0, B.U(t.b), S.blocks[t.b].m,
                                 const_cast<double*>(t.U), t.m, t.r});
         run_jobs(ctx, jobs);
-    }
-    // Y = A X
-    {
-        std::vector<MatJob> jobs;
-        for (int i : hh) {
-            const WTask& t = P.w[i];
-            const Block& Ba = S.blocks[t.a];
-            jobs.push_back({&A, t.a, false, 1.0, 0.0, S0 + t.s_x, Ba.n, S0 + t.s_y, Ba.m, t.k});
-        }
-        run_jobs(ctx, jobs);
-    }
-    // Q = orth(Y)
-    {
-        std::vector<QrOp> q;
-        for (int i : hh) {
-            const WTask& t = P.w[i];
-            q.push_back({S0 + t.s_y, S0 + t.s_q, S0 + t.s_tau, t.m, t.k, t.m, 0});
-        }
-        launch_qr_formq(ctx, q, "sample_qr");
-    }
-    // Z1 = alpha A^T Q, and W.V = alpha B^T A.V for low-rank x node
-    {
-        std::vector<MatJob> jobs;
-        for (int i : hh) {
-            const WTask& t = P.w[i];
-            const Block& Ba = S.blocks[t.a];
-            jobs.push_back({&A, t.a, true, t.alpha, 0.0, S0 + t.s_q, Ba.m, S0 + t.s_z1, Ba.n,
-                            t.kq});
-        }
+        jobs.clear();
         for (const WTask& t : P.w)
             if (t.type == W_LRH && t.r > 0)
                 jobs.push_back({&B, t.b, true, t.alpha, 0.0, A.V(t.a), S.blocks[t.a].n,
                                 const_cast<double*>(t.V), t.n, t.r});
         run_jobs(ctx, jobs);
     }
-    // Z = B^T Z1
-    {
-        std::vector<MatJob> jobs;
-        for (int i : hh) {
-            const WTask& t = P.w[i];
-            const Block& Bb = S.blocks[t.b];
-            jobs.push_back({&B, t.b, true, 1.0, 0.0, S0 + t.s_z1, Bb.m, S0 + t.s_z, Bb.n, t.kq});
+    if (!hh.empty()) sample(hh);
+    if (learned) {
+        // probe check: redo with the plain sample count every compression
+        // whose estimated error exceeds the tolerance's scale
+        const std::vector<double> err = probe_errors(ctx, S, A, B, P.w, hh);
+        const double limit = std::max(10.0 * ctx.compression_tol, 1e-13);
+        std::vector<int> redo;
+        for (size_t i = 0; i < hh.size(); ++i)
+            if (!(err[i] <= limit) && P.w[hh[i]].k < k_plain[i]) redo.push_back((int)i);
+        ctx.rank_stats.compressions += (long long)hh.size();
+        ctx.rank_stats.fallbacks += (long long)redo.size();
+        for (size_t i = 0; i < hh.size(); ++i) {
+            ctx.rank_stats.samples += P.w[hh[i]].k;
+            ctx.rank_stats.samples_plain += k_plain[i];
         }
-        run_jobs(ctx, jobs);
+        if (!redo.empty()) {
+            std::vector<int> ids;
+            for (int i : redo) {
+                WTask& t = P.w[hh[i]];
+                t.k = k_plain[i];
+                t.kq = kq_plain[i];
+                ctx.rank_stats.samples += t.k;
+                ids.push_back(hh[i]);
+            }
+            sample(ids);
+        }
+    } else if (!hh.empty()) {
+        ctx.rank_stats.compressions += (long long)hh.size();
+        for (size_t i = 0; i < hh.size(); ++i) {
+            ctx.rank_stats.samples += k_plain[i];
+            ctx.rank_stats.samples_plain += k_plain[i];
+        }
     }
-    // W = best rank-r of Q Z^T (the gesvd truncation of hmat_tools.hpp:1712-1745)
-    {
-        std::vector<RoundOp> ops;
-        for (int i : hh) {
-            const WTask& t = P.w[i];
-            RoundOp op{};
-            op.kind = ROUND_ORTHO;
-            op.m = t.m;
-            op.n = t.n;
-            op.u1 = S0 + t.s_q; op.ldu1 = t.m; op.r1 = t.kq;
-            op.v1 = S0 + t.s_z; op.ldv1 = t.n;
-            op.rout = t.r;
-            op.uo = const_cast<double*>(t.U);
-            op.vo = const_cast<double*>(t.V);
-            op.work = S0 + t.s_work;
-            op.alpha = 1.0;
-            op.tol = ctx.compression_tol;
-            ops.push_back(op);
+    if (log_ranks) {
+        std::vector<int> kh(hh.size());
+        HMB_CUDA(cudaMemcpyAsync(kh.data(), kept.get(), kh.size() * sizeof(int),
+                                 cudaMemcpyDeviceToHost, st));
+        HMB_CUDA(cudaStreamSynchronize(st));
+        for (size_t i = 0; i < hh.size(); ++i) {
+            ctx.log_x.insert(ctx.log_x.end(), feats.begin() + (long long)i * kMlpFeatures,
+                             feats.begin() + (long long)(i + 1) * kMlpFeatures);
+            ctx.log_t.push_back((float)kh[i] / (float)std::max(1, P.w[hh[i]].r));
         }
-        launch_round_ops(ctx, ops, "sample_round");
     }
     // HH products with rank 0 (empty blocks): nothing to compute.
 

@@ -342,6 +342,7 @@ __device__ void do_round(const RoundOp& op, double* dyn, long long smem_doubles,
             while (c < keep && norms[order[c]] > t2 * s0) ++c;
         keep = c;
     }
+    if (tid == 0 && op.rank_out) *op.rank_out = keep;
     if (ortho) {
         for (long long e = tid; e < (long long)m * rout; e += kT) {
             int i = (int)(e % m), c = (int)(e / m);

@@ -29,6 +29,7 @@ struct RoundOp {
     // them when sigma_0 < tol^2), writing zero columns in their place
     // (GENERAL, DENSE, ORTHO).
     double tol;
+    int* rank_out;      // if set: receives the number of columns kept
 };
 
 // Scratch doubles one op needs (0 for SET / CONCAT).

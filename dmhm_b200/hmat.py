@@ -71,6 +71,34 @@ class Context:
         check(lib().hm_get_compression_tolerance(self._h, C.byref(v)))
         return v.value
 
+    # -- learned sample counts ------------------------------------------------
+    def use_rank_model(self, model, margin: int = 2, probes: int = 4):
+        """Attach a RankModel to the H*H compressions (None detaches)."""
+        check(lib().hm_use_rank_model(self._h, model.handle if model is not None else None,
+                                      int(margin), int(probes)))
+
+    def rank_log_enable(self, on: bool = True):
+        check(lib().hm_rank_log_enable(self._h, 1 if on else 0))
+
+    def rank_log(self, clear: bool = False):
+        """(features [n x F] float32, kept-rank fractions [n] float32)."""
+        import numpy as np
+        n = C.c_int()
+        check(lib().hm_rank_log_read(self._h, None, None, 0, C.byref(n), 0))
+        F = lib().hm_rank_feature_count()
+        x = np.zeros((n.value, F), dtype=np.float32)
+        t = np.zeros(n.value, dtype=np.float32)
+        check(lib().hm_rank_log_read(self._h, x.ctypes.data_as(C.POINTER(C.c_float)),
+                                     t.ctypes.data_as(C.POINTER(C.c_float)), n.value,
+                                     C.byref(n), 1 if clear else 0))
+        return x, t
+
+    def rank_stats(self) -> dict:
+        v = [C.c_int64() for _ in range(4)]
+        check(lib().hm_rank_stats(self._h, *[C.byref(x) for x in v]))
+        return {"compressions": v[0].value, "samples": v[1].value,
+                "samples_plain": v[2].value, "fallbacks": v[3].value}
+
     def lcg_states(self):
         s, p = C.c_uint64(), C.c_uint64()
         check(lib().hm_get_lcg_states(self._h, C.byref(s), C.byref(p)))
@@ -399,3 +427,79 @@ class HMat3d(_HMatBase):
     def BuildNaturalToHierarchicalMap(xSize: int, ySize: int, zSize: int,
                                       numLevels: int) -> np.ndarray:
         return natural_to_hierarchical_map((xSize, ySize, zSize), numLevels)
+
+
+class RankModel:
+    """Learned rank predictor of the randomized H*H compressions (a 3-layer
+    perceptron trained and evaluated by the library's GPU kernels)."""
+
+    def __init__(self, ctx: Optional[Context] = None, seed: int = 1):
+        self.ctx = _ctx(ctx)
+        h = C.c_void_p()
+        check(lib().hm_rank_model_create(self.ctx.handle, C.c_uint64(seed), C.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    @staticmethod
+    def num_features() -> int:
+        return lib().hm_rank_feature_count()
+
+    @staticmethod
+    def num_params() -> int:
+        return lib().hm_rank_param_count()
+
+    def close(self):
+        if self._h:
+            lib().hm_rank_model_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _f32(a):
+        import numpy as np
+        return np.ascontiguousarray(a, dtype=np.float32)
+
+    def params(self):
+        import numpy as np
+        p = np.zeros(self.num_params(), dtype=np.float32)
+        check(lib().hm_rank_model_get_params(self._h, p.ctypes.data_as(C.POINTER(C.c_float)), p.size))
+        return p
+
+    def set_params(self, p):
+        p = self._f32(p)
+        check(lib().hm_rank_model_set_params(self._h, p.ctypes.data_as(C.POINTER(C.c_float)), p.size))
+
+    def loss_grad(self, x, t):
+        import numpy as np
+        x, t = self._f32(x), self._f32(t)
+        g = np.zeros(self.num_params(), dtype=np.float32)
+        loss = C.c_float()
+        P = C.POINTER(C.c_float)
+        check(lib().hm_rank_model_loss_grad(self._h, x.ctypes.data_as(P), t.ctypes.data_as(P),
+                                            t.size, C.byref(loss), g.ctypes.data_as(P)))
+        return float(loss.value), g
+
+    def train(self, x, t, epochs: int = 500, lr: float = 1e-2) -> float:
+        x, t = self._f32(x), self._f32(t)
+        loss = C.c_float()
+        P = C.POINTER(C.c_float)
+        check(lib().hm_rank_model_train(self._h, x.ctypes.data_as(P), t.ctypes.data_as(P), t.size,
+                                        int(epochs), C.c_float(lr), C.byref(loss)))
+        return float(loss.value)
+
+    def predict(self, x):
+        import numpy as np
+        x = self._f32(x)
+        n = x.shape[0]
+        out = np.zeros(n, dtype=np.float32)
+        P = C.POINTER(C.c_float)
+        check(lib().hm_rank_model_predict(self._h, x.ctypes.data_as(P), n, out.ctypes.data_as(P)))
+        return out

@@ -40,6 +40,7 @@ extern "C" {
 
 typedef struct hm_context_s* hm_context;  /* device, stream, generators     */
 typedef struct hm_matrix_s* hm_matrix;    /* one H-matrix resident in HBM    */
+typedef struct hm_rank_model_s* hm_rank_model;  /* learned rank predictor  */
 
 /* Message of the last failed call on this thread ("" if none). */
 HM_API const char* hm_last_error(void);
@@ -183,6 +184,52 @@ HM_API int hm_add_constant_to_diagonal(hm_matrix h, double alpha);
  */
 HM_API int hm_multiply_vector_noalloc(hm_matrix h, int transpose, double alpha,
                                       const double* x, double beta, double* y);
+
+/*
+ * Learned sample counts for the randomized H*H compressions.  No counterpart
+ * in the reference, whose randomized product always draws SampleRank =
+ * maxRank + Oversample() samples (include/dmhm/hmat_tools.hpp:1657-1746).
+ * A three-layer perceptron (hm_rank_feature_count() inputs, two hidden
+ * layers of 64, FP32; hm_rank_param_count() parameters) predicts, from the
+ * features of one compression, the fraction of its rank cap that the
+ * tolerance truncation keeps; with the model attached (hm_use_rank_model)
+ * each compression draws ceil(fraction * cap) + margin + Oversample()
+ * samples, estimates its error with `probes` Gaussian probe vectors and is
+ * redone with the full sample count when that estimate exceeds 10 * the
+ * compression tolerance.  Training data come from runs with the log on
+ * (hm_rank_log_enable; needs a tolerance): features and kept fractions of
+ * every compression.  Forward, backward and Adam run on the GPU.
+ * Features (float rows of hm_rank_feature_count()): level / numLevels,
+ * log2(1+m)/16, log2(1+n)/16, min(1, admissibility distance / 8), mean rank
+ * of the low-rank leaves below the A block / maxRank, the same below the B
+ * block, dense share of the entries below A, the same below B, rank cap /
+ * maxRank, dimension / 3.
+ */
+HM_API int hm_rank_feature_count(void);
+HM_API int hm_rank_param_count(void);
+HM_API int hm_rank_model_create(hm_context ctx, uint64_t seed, hm_rank_model* out);
+HM_API int hm_rank_model_destroy(hm_rank_model m);
+HM_API int hm_rank_model_set_params(hm_rank_model m, const float* params, int n);
+HM_API int hm_rank_model_get_params(hm_rank_model m, float* params, int n);
+/* Mean squared error of the predictions on (x: n rows, t: n targets) and its
+   gradient (grad: hm_rank_param_count() floats, may be NULL). */
+HM_API int hm_rank_model_loss_grad(hm_rank_model m, const float* x, const float* t, int n,
+                                   float* loss, float* grad);
+/* `epochs` full-batch Adam steps (learning rate lr); *loss = final loss. */
+HM_API int hm_rank_model_train(hm_rank_model m, const float* x, const float* t, int n,
+                               int epochs, float lr, float* loss);
+HM_API int hm_rank_model_predict(hm_rank_model m, const float* x, int n, float* out);
+/* Attach (m != NULL) or detach the model; margin: extra rank over the
+   prediction; probes: probe vectors of the error check. */
+HM_API int hm_use_rank_model(hm_context ctx, hm_rank_model m, int margin, int probes);
+HM_API int hm_rank_log_enable(hm_context ctx, int on);
+/* Copies min(cap, *n) logged rows (x: cap * features floats, t: cap floats);
+   *n receives the number logged; clear = 1 empties the log afterwards. */
+HM_API int hm_rank_log_read(hm_context ctx, float* x, float* t, int cap, int* n, int clear);
+/* Compressions run, samples drawn, samples the fixed count would have drawn,
+   compressions redone after a failed probe check (since context creation). */
+HM_API int hm_rank_stats(hm_context ctx, int64_t* compressions, int64_t* samples,
+                         int64_t* samples_plain, int64_t* fallbacks);
 
 /* Diagnostics (no reference counterpart): number of kernels this library has
    launched so far in the process, and per-kernel CUDA-event timing on the

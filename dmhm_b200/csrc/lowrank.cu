@@ -123,51 +123,72 @@ __device__ __forceinline__ int rr_pos(int i, int step, int n) {
 // they are mutually orthogonal, accumulating the rotations in J (cols x cols,
 // J starts as I), so M_in = M_out J^T.  Round-robin ordering: cols/2
 // disjoint pairs per step, one warp per pair.  Bounded number of sweeps.
-__device__ void cta_jacobi(double* M, int rows, int cols, double* J, int* flag) {
+// Pairs with a column below rounding level (squared norm under 1e-32 times
+// the squared Frobenius norm of M) are left alone: rotating noise against
+// noise never settles, and such columns carry no singular value above
+// rounding level.
+__device__ void cta_jacobi(double* M, int rows, int cols, double* J, int* flag, double* red) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int e = threadIdx.x; e < cols * cols; e += kT)
         J[e] = (e % cols == e / cols) ? 1.0 : 0.0;
+    double fro = 0.0;
+    for (long long e = threadIdx.x; e < (long long)rows * cols; e += kT) fro = fma(M[e], M[e], fro);
+    fro = block_sum(fro, red);
+    const double tiny = 1e-32 * fro;
     __syncthreads();
     if (cols < 2) return;
     const int n = cols + (cols & 1);
+    // one half-warp (16 lanes) per pair: all cols/2 pairs of a step at once
+    // for up to 32 columns
+    const int hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
     for (int sweep = 0; sweep < kJacobiSweeps; ++sweep) {
         if (threadIdx.x == 0) *flag = 0;
         __syncthreads();
         for (int step = 0; step < n - 1; ++step) {
-            for (int k = warp; k < n / 2; k += kW) {
-                int p = rr_pos(k, step, n), q = rr_pos(n - 1 - k, step, n);
-                if (p >= cols || q >= cols) continue;
+            // warp-uniform trip count: both half-warps of a warp iterate
+            // together (their shuffles span the whole warp)
+            for (int kb = 2 * warp; kb < n / 2; kb += 2 * kW) {
+                const int k = kb + (hw & 1);
+                int p = 0, q = 1;
+                if (k < n / 2) {
+                    p = rr_pos(k, step, n);
+                    q = rr_pos(n - 1 - k, step, n);
+                }
+                const bool live = k < n / 2 && p < cols && q < cols;
                 if (p > q) { int t = p; p = q; q = t; }
                 double* gp = M + (long long)p * rows;
                 double* gq = M + (long long)q * rows;
                 double a = 0.0, b = 0.0, c = 0.0;
-                for (int i = lane; i < rows; i += 32) {
-                    const double x = gp[i], y = gq[i];
-                    a = fma(x, x, a);
-                    b = fma(y, y, b);
-                    c = fma(x, y, c);
+                if (live)
+                    for (int i = hl; i < rows; i += 16) {
+                        const double x = gp[i], y = gq[i];
+                        a = fma(x, x, a);
+                        b = fma(y, y, b);
+                        c = fma(x, y, c);
+                    }
+#pragma unroll
+                for (int o = 8; o > 0; o >>= 1) {
+                    a += __shfl_xor_sync(0xffffffffu, a, o);
+                    b += __shfl_xor_sync(0xffffffffu, b, o);
+                    c += __shfl_xor_sync(0xffffffffu, c, o);
                 }
-                a = warp_sum(a);
-                b = warp_sum(b);
-                c = warp_sum(c);
-                if (c != 0.0 && fabs(c) > kJacobiTol * sqrt(a * b)) {
+                if (live && c != 0.0 && a > tiny && b > tiny && fabs(c) > kJacobiTol * sqrt(a * b)) {
                     const double zeta = (b - a) / (2.0 * c);
                     const double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
                     const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
-                    __syncwarp();
-                    for (int i = lane; i < rows; i += 32) {
+                    for (int i = hl; i < rows; i += 16) {
                         const double x = gp[i], y = gq[i];
                         gp[i] = cs * x - sn * y;
                         gq[i] = sn * x + cs * y;
                     }
                     double* jp = J + (long long)p * cols;
                     double* jq = J + (long long)q * cols;
-                    for (int i = lane; i < cols; i += 32) {
+                    for (int i = hl; i < cols; i += 16) {
                         const double x = jp[i], y = jq[i];
                         jp[i] = cs * x - sn * y;
                         jq[i] = sn * x + cs * y;
                     }
-                    if (lane == 0) *flag = 1;
+                    if (hl == 0) *flag = 1;
                 }
             }
             __syncthreads();
@@ -176,6 +197,7 @@ __device__ void cta_jacobi(double* M, int rows, int cols, double* J, int* flag) 
         __syncthreads();
         if (!again) break;
     }
+    (void)lane;
 }
 
 // order[0..cols) = column indices of M by decreasing norm (ties by index).
@@ -327,7 +349,7 @@ __device__ void do_round(const RoundOp& op, double* dyn, long long smem_doubles,
     __syncthreads();
 
     // ---- SVD of the core ---------------------------------------------------
-    cta_jacobi(M, ku, kv, J, &sh.flag);
+    cta_jacobi(M, ku, kv, J, &sh.flag, red);
     cta_order_columns(M, ku, kv, norms, order);
 
     // ---- outputs -------------------------------------------------------------

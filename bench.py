@@ -297,6 +297,7 @@ def gpu_arm(args):
         line["cpu_baseline"] = cpu_baseline(coef, Xh, nbytes)
     if not args.no_schulz:
         line["schulz"] = schulz_leg(local, rank == 0 and not args.no_cpu_baseline)
+        line["schulz_modes"] = schulz_modes_leg(local)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
@@ -476,6 +477,73 @@ def schulz_leg(device, with_reference):
                                           "estimate) of the same operator, extrapolated to "
                                           f"{its} iterations"}
         out["speedup_vs_cpu_reference"] = per_it * its / gpu_s
+    return out
+
+
+SCHULZ_MODES = dict(sizes=(64, 64), levels=5, rank=16, oversample=4, seed=1, stop_tol=1e-8,
+                    tol=1e-10)
+
+
+def schulz_modes_leg(device):
+    """SchulzInvert(-1, 1.5, 6, stopTol 1e-8) on the 64 x 64 five-point
+    operator (N = 4096, 16-point leaves, maxRank 16), three ways, each from a
+    fresh context: the plain method (fixed rank maxRank, the reference's
+    HMat2d semantics), tolerance truncation at 1e-10 (CompressionTolerance),
+    and tolerance truncation with learned sample counts (the rank predictor
+    trained, on the GPU, on the kept ranks logged by a 6-iteration run of the
+    same operator family with another coefficient seed).  Each reports wall
+    seconds (the iteration reads one norm estimate back per step), iterations,
+    the attained ||I - X A|| estimate, the residual ||X A p - p|| / ||p|| on
+    probe vectors, and the sample counts drawn."""
+    import dmhm_b200 as D
+    cfg = SCHULZ_MODES
+    sz, L, r = cfg["sizes"], cfg["levels"], cfg["rank"]
+
+    def make(seed, tol, log=False):
+        coef = D.operators.uniform_coefficients(sz, seed)
+        S = D.operators.stencil(sz, coef, L)
+        ctx = D.Context(device)
+        ctx.set_oversample(cfg["oversample"])
+        ctx.set_compression_tolerance(tol)
+        if log:
+            ctx.rank_log_enable(True)
+        return ctx, S
+
+    # training data: kept ranks of a short run on another coefficient field
+    t0 = time.perf_counter()
+    ctx, S = make(cfg["seed"] + 100, cfg["tol"], log=True)
+    H = D.HMat2d(S, L, r, True, *sz, ctx=ctx)
+    H.SchulzInvert(6, 1.5, 6.0, 1e-30)
+    x, t = ctx.rank_log(clear=True)
+    model = D.RankModel(ctx, seed=7)
+    loss0, _ = model.loss_grad(x, t)
+    loss = model.train(x, t, epochs=800, lr=1e-2)
+    params = model.params()
+    train_s = time.perf_counter() - t0
+    out = {"workload": "SchulzInvert(-1, theta 1.5, confidence 6, stopTol 1e-8), HMat2d<double> "
+                       "64x64 five-point operator, numLevels 5, maxRank 16, oversample 4",
+           "training": {"rows": int(x.shape[0]), "loss_initial": loss0, "loss_final": loss,
+                        "epochs": 800, "seconds": train_s}}
+    for mode, tol, learned in (("plain_fp64", 0.0, False), ("tolerance_1e-10", cfg["tol"], False),
+                               ("learned_1e-10", cfg["tol"], True)):
+        ctx, S = make(cfg["seed"], tol)
+        if learned:
+            m = D.RankModel(ctx, seed=7)
+            m.set_params(params)
+            ctx.use_rank_model(m, 2, 4)
+        H = D.HMat2d(S, L, r, True, *sz, ctx=ctx)
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        its, trace = H.SchulzInvert(-1, 1.5, 6.0, cfg["stop_tol"])
+        ctx.synchronize()
+        secs = time.perf_counter() - t0
+        A = D.HMat2d(S, L, r, True, *sz, ctx=ctx)
+        P = np.random.default_rng(5).standard_normal((A.Width(), 4))
+        res = np.linalg.norm(H.Multiply(1.0, A.Multiply(1.0, P)) - P) / np.linalg.norm(P)
+        out[mode] = {"seconds": secs, "iterations": its, "final_norm_estimate": trace[-1],
+                     "relative_residual_XAp_minus_p": float(res),
+                     "rank_sum": H.BlockCensus()["rank_sum"], "sampling": ctx.rank_stats()}
+    out["speedup_learned_vs_plain"] = out["plain_fp64"]["seconds"] / out["learned_1e-10"]["seconds"]
     return out
 
 

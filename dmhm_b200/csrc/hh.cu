@@ -620,8 +620,12 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
             t.kq = std::min(S.blocks[t.a].m, t.k);
         }
     }
+    // kept ranks of the sampled products (truncating runs: later operations
+    // read them on the device, the log reads them back)
     DeviceBuffer<int> kept;
-    if (log_ranks) kept.allocate(hh.size(), st);
+    std::vector<int> hh_pos(P.w.size(), -1);
+    for (size_t i = 0; i < hh.size(); ++i) hh_pos[hh[i]] = (int)i;
+    if (ctx.compression_tol > 0.0 && !hh.empty()) kept.allocate(hh.size(), st);
     // the sampling pipeline for the listed tasks, at their current k
     auto sample = [&](const std::vector<int>& ids) {
         {
@@ -701,7 +705,7 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
                 op.work = S0 + t.s_work;
                 op.alpha = 1.0;
                 op.tol = ctx.compression_tol;
-                if (log_ranks && ids.size() == hh.size()) op.rank_out = kept.get() + j;
+                if (kept.get()) op.rank_out = kept.get() + hh_pos[ids[j]];
                 ops.push_back(op);
             }
             launch_round_ops(ctx, ops, "sample_round");
@@ -842,6 +846,11 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
     std::vector<RoundOp> rops;
     std::vector<int> rbegin{0};
     std::vector<long long> rwork;   // per op: offset into the work arena
+    // truncating runs: every op leaves its output rank in rk, the next op of
+    // the block (and a sampled W's kept rank) set its input ranks on the device
+    const bool dyn = ctx.compression_tol > 0.0;
+    DeviceBuffer<int> rk;
+    if (dyn) rk.allocate(std::max<size_t>(1, P.lops.ops.size()), st);
     std::vector<GemmOp> gops;
     std::vector<int> gbegin{0};
     for (int c : S.leaves) {
@@ -861,11 +870,13 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
             }
             long long wmax = 0;
             const size_t first = rops.size();
+            int prev = -1;   // op whose output is (cu, cv)
             for (int j = 0; j < nops; ++j) {
                 const LOp& op = ops[j];
                 const int rnew = state_rank[obase + j];
                 if (op.type == L_RESET) {
                     cr = 0;
+                    prev = -1;
                     continue;
                 }
                 double* ou = (j + 1 == nops) ? C.U(c)
@@ -897,7 +908,14 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
                 r.r2 = (op.type == L_SET || (op.type == L_DDC && op.beta == 0.0)) ? 0 : cr;
                 r.ldu2 = Cb.m;
                 r.ldv2 = Cb.n;
+                if (dyn) {
+                    r.rank_out = rk.get() + rops.size();
+                    if (r.r2 > 0 && prev >= 0) r.r2_dev = rk.get() + prev;
+                    if (op.type != L_DDC && hh_pos[op.w] >= 0) r.r1_dev = kept.get() + hh_pos[op.w];
+                }
+                prev = -1;
                 if (rnew > 0 && Cb.m > 0 && Cb.n > 0) {
+                    prev = (int)rops.size();
                     rops.push_back(r);
                     wmax = std::max(wmax, round_work_size(r));
                 }

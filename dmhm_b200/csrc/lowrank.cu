@@ -233,37 +233,34 @@ struct RoundShared {
 
 // One rounding operation, executed by the whole CTA.  `dyn` holds the core
 // and the rotations in shared memory when they fit in `smem_doubles` doubles.
-__device__ void do_round(const RoundOp& op, double* dyn, long long smem_doubles,
+__device__ void do_round(const RoundOp& op_in, double* dyn, long long smem_doubles,
                          RoundShared& sh) {
     double* red = sh.red;
     double* norms = sh.norms;
     int* order = sh.order;
+    RoundOp op = op_in;
+    if (op.r1_dev) op.r1 = min(op.r1, *op.r1_dev);
+    if (op.r2_dev) op.r2 = min(op.r2, *op.r2_dev);
     const int m = op.m, n = op.n;
     const int tid = threadIdx.x;
 
-    if (op.kind == ROUND_SET) {
-        for (long long e = tid; e < (long long)m * op.r1; e += kT) {
+    if (op.kind == ROUND_SET || op.kind == ROUND_CONCAT) {
+        // exact: [beta U2, alpha U1], [V2, V1] (SET: r2 = 0), zero beyond
+        const int r2 = op.kind == ROUND_SET ? 0 : op.r2, r = op.r1 + r2;
+        const int cap = max(r, op.rout);
+        for (long long e = tid; e < (long long)m * cap; e += kT) {
             int i = (int)(e % m), c = (int)(e / m);
-            op.uo[e] = op.alpha * op.u1[i + (long long)c * op.ldu1];
+            op.uo[e] = c >= r    ? 0.0
+                       : c < r2 ? op.beta * op.u2[i + (long long)c * op.ldu2]
+                                : op.alpha * op.u1[i + (long long)(c - r2) * op.ldu1];
         }
-        for (long long e = tid; e < (long long)n * op.r1; e += kT) {
+        for (long long e = tid; e < (long long)n * cap; e += kT) {
             int i = (int)(e % n), c = (int)(e / n);
-            op.vo[e] = op.v1[i + (long long)c * op.ldv1];
+            op.vo[e] = c >= r    ? 0.0
+                       : c < r2 ? op.v2[i + (long long)c * op.ldv2]
+                                : op.v1[i + (long long)(c - r2) * op.ldv1];
         }
-        return;
-    }
-    if (op.kind == ROUND_CONCAT) {
-        const int r2 = op.r2, r = op.r1 + op.r2;
-        for (long long e = tid; e < (long long)m * r; e += kT) {
-            int i = (int)(e % m), c = (int)(e / m);
-            op.uo[e] = c < r2 ? op.beta * op.u2[i + (long long)c * op.ldu2]
-                              : op.alpha * op.u1[i + (long long)(c - r2) * op.ldu1];
-        }
-        for (long long e = tid; e < (long long)n * r; e += kT) {
-            int i = (int)(e % n), c = (int)(e / n);
-            op.vo[e] = c < r2 ? op.v2[i + (long long)c * op.ldv2]
-                              : op.v1[i + (long long)(c - r2) * op.ldv1];
-        }
+        if (tid == 0 && op.rank_out) *op.rank_out = r;
         return;
     }
 

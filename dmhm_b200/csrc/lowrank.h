@@ -29,7 +29,12 @@ struct RoundOp {
     // them when sigma_0 < tol^2), writing zero columns in their place
     // (GENERAL, DENSE, ORTHO).
     double tol;
-    int* rank_out;      // if set: receives the number of columns kept
+    int* rank_out;      // if set: receives the rank of the output
+    // if set: the ranks of the inputs are min(r1, *r1_dev) / min(r2, *r2_dev),
+    // read when the op runs (ranks left by earlier ops of a truncating run);
+    // outputs are zero beyond their rank
+    const int* r1_dev;
+    const int* r2_dev;
 };
 
 // Scratch doubles one op needs (0 for SET / CONCAT).

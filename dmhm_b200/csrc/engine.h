@@ -67,6 +67,8 @@ struct Context {
     int* zeroed_counters(long long n);
     DeviceBuffer<int> counters;
     long long counters_cap = 0;
+    // Symbolic H*H plans of recent products (hh.cu).
+    std::shared_ptr<struct HHPlanCache> hh_cache;
     // Device word set by kernels whose bounded waits gave up (zero = fine).
     int* error_word();
     DeviceBuffer<int> errword;

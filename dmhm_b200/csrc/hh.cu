@@ -60,6 +60,7 @@ struct WTask {
     // randomized sampling
     int k = 0, kq = 0;
     uint64_t omega = 0;
+    uint64_t omega_steps = 0;   // serial-generator draws before this sample's
     long long s_omega = -1, s_x = -1, s_y = -1, s_q = -1, s_tau = -1, s_z1 = -1, s_z = -1,
               s_work = -1;
 };
@@ -114,6 +115,7 @@ struct Planner {
     int maxRankC;
     int oversample;
     uint64_t serial;
+    uint64_t steps = 0;   // serial-generator draws so far
     std::vector<WTask> w;
     PerBlock<LOp> lops;
     PerBlock<DOp> dops;
@@ -158,7 +160,10 @@ struct Planner {
                         "Gaussian fill would write past its columns)");
             t.kq = std::min(BA.m, t.k);
             t.omega = serial;
-            serial = lcg_skip_host(serial, (uint64_t)t.k * 2ULL * (uint64_t)((BB.n + 1) / 2));
+            t.omega_steps = steps;
+            const uint64_t draws = (uint64_t)t.k * 2ULL * (uint64_t)((BB.n + 1) / 2);
+            serial = lcg_skip_host(serial, draws);
+            steps += draws;
         } else if (ka == KIND_DENSE && kb == KIND_DENSE) {
             t.type = W_DD;
             t.r = -1;
@@ -450,39 +455,69 @@ std::vector<double> probe_errors(Context& ctx, const Structure& S, const HMatrix
     return rel;
 }
 
+// The symbolic phase depends only on the structure, the ranks of the
+// factors (and of C for the update form), alpha, beta, the rank cap and the
+// oversampling; generator positions are kept as draw counts from the
+// starting state.  Plans are cached per context (the last kHHPlans), so the
+// iterations of SchulzInvert, whose ranks repeat, plan once.
+struct SymPlan {
+    std::vector<WTask> w;
+    PerBlock<LOp> lops;
+    PerBlock<DOp> dops;
+    uint64_t serial_steps = 0;
+    std::vector<int> crank, state_rank, op_kind;
+};
+
+struct SymKey {
+    const Structure* S = nullptr;
+    int fresh = 1, maxRankC = 0, oversample = 0, maxA = 0, maxB = 0;
+    double alpha = 0, beta = 0;
+    std::vector<int> ra, rb, rc;
+    uint64_t hash = 0;
+    bool operator==(const SymKey& o) const {
+        return hash == o.hash && S == o.S && fresh == o.fresh && maxRankC == o.maxRankC &&
+               oversample == o.oversample && maxA == o.maxA && maxB == o.maxB &&
+               alpha == o.alpha && beta == o.beta && ra == o.ra && rb == o.rb && rc == o.rc;
+    }
+};
+
+uint64_t fnv(uint64_t h, const void* p, size_t n) {
+    const unsigned char* c = static_cast<const unsigned char*>(p);
+    for (size_t i = 0; i < n; ++i) h = (h ^ c[i]) * 1099511628211ULL;
+    return h;
+}
+
+constexpr size_t kHHPlans = 8;
+
 }  // namespace
 
-void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha, double beta,
-                 HMatrix& C, bool fresh) {
-    HMB_REQUIRE(A.S && B.S && (A.S == B.S || same_structure(*A.S, *B.S)), HM_ERR_ARGUMENT,
-                "H*H multiply needs both factors on the same block structure");
-    HMB_REQUIRE(&C != &A && &C != &B, HM_ERR_ARGUMENT,
-                "the product must not overwrite a factor");
-    const Structure& S = *A.S;
-    cudaStream_t st = ctx.stream;
-    if (!fresh) {
-        HMB_REQUIRE(C.S && (C.S == A.S || same_structure(*C.S, *A.S)), HM_ERR_ARGUMENT,
-                    "C must share the factors' block structure");
-    }
-    const int maxRankC = fresh ? A.max_rank : C.max_rank;
+struct HHPlanCache {
+    std::vector<std::pair<SymKey, std::shared_ptr<SymPlan>>> entries;   // most recent last
+};
 
-    // ---------------- symbolic phase ----------------
-    std::unique_ptr<HostScope> hs(new HostScope(ctx, "hh_symbolic"));
-    Planner P(A, B, maxRankC, ctx.oversample, ctx.serial_state);
+namespace {
+
+std::shared_ptr<SymPlan> make_plan(const HMatrix& A, const HMatrix& B, const HMatrix& C,
+                                   double alpha, double beta, bool fresh, int maxRankC,
+                                   int oversample) {
+    const Structure& S = *A.S;
+    Planner P(A, B, maxRankC, oversample, 0);
     if (fresh)
         P.fresh(0, 0, 0, alpha);
     else
         P.update(0, 0, 0, alpha, beta);
-    const uint64_t serial_after = P.serial;
     P.lops.finalize(S.blocks.size());
     P.dops.finalize(S.blocks.size());
-
-    // final ranks of C
-    std::vector<int> crank(S.blocks.size(), 0);
-    std::vector<int> nops_lr(S.blocks.size(), 0);
-    // rank after each operation and its rounding kind (-1: rank reset),
-    // parallel to P.lops.ops
-    std::vector<int> state_rank(P.lops.ops.size()), op_kind(P.lops.ops.size());
+    auto plan = std::make_shared<SymPlan>();
+    plan->serial_steps = P.steps;
+    // final ranks of C, and the rank after each operation with its rounding
+    // kind (-1: rank reset), parallel to lops.ops
+    std::vector<int>& crank = plan->crank;
+    std::vector<int>& state_rank = plan->state_rank;
+    std::vector<int>& op_kind = plan->op_kind;
+    crank.assign(S.blocks.size(), 0);
+    state_rank.assign(P.lops.ops.size(), 0);
+    op_kind.assign(P.lops.ops.size(), 0);
     for (int c : S.leaves) {
         const Block& Cb = S.blocks[c];
         if (Cb.kind != KIND_LOWRANK) continue;
@@ -519,6 +554,82 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
         }
         crank[c] = rank;
     }
+    plan->w = std::move(P.w);
+    plan->lops = std::move(P.lops);
+    plan->dops = std::move(P.dops);
+    return plan;
+}
+
+std::shared_ptr<SymPlan> get_plan(Context& ctx, const HMatrix& A, const HMatrix& B,
+                                  const HMatrix& C, double alpha, double beta, bool fresh,
+                                  int maxRankC) {
+    SymKey key;
+    key.S = A.S.get();
+    key.fresh = fresh ? 1 : 0;
+    key.maxRankC = maxRankC;
+    key.oversample = ctx.oversample;
+    key.maxA = A.max_rank;
+    key.maxB = B.max_rank;
+    key.alpha = alpha;
+    key.beta = beta;
+    key.ra = A.rank;
+    key.rb = B.rank;
+    if (!fresh) key.rc = C.rank;
+    uint64_t h = 1469598103934665603ULL;
+    h = fnv(h, &key.S, sizeof(key.S));
+    h = fnv(h, &key.fresh, sizeof(int) * 5);
+    h = fnv(h, &key.alpha, sizeof(double) * 2);
+    h = fnv(h, key.ra.data(), key.ra.size() * sizeof(int));
+    h = fnv(h, key.rb.data(), key.rb.size() * sizeof(int));
+    h = fnv(h, key.rc.data(), key.rc.size() * sizeof(int));
+    key.hash = h;
+    if (!ctx.hh_cache) ctx.hh_cache = std::make_shared<HHPlanCache>();
+    auto& E = ctx.hh_cache->entries;
+    for (size_t i = 0; i < E.size(); ++i) {
+        if (E[i].first == key) {
+            auto hit = E[i];
+            E.erase(E.begin() + (long long)i);
+            E.push_back(hit);
+            return hit.second;
+        }
+    }
+    auto plan = make_plan(A, B, C, alpha, beta, fresh, maxRankC, ctx.oversample);
+    E.emplace_back(std::move(key), plan);
+    if (E.size() > kHHPlans) E.erase(E.begin());
+    return plan;
+}
+
+}  // namespace
+
+void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha, double beta,
+                 HMatrix& C, bool fresh) {
+    HMB_REQUIRE(A.S && B.S && (A.S == B.S || same_structure(*A.S, *B.S)), HM_ERR_ARGUMENT,
+                "H*H multiply needs both factors on the same block structure");
+    HMB_REQUIRE(&C != &A && &C != &B, HM_ERR_ARGUMENT,
+                "the product must not overwrite a factor");
+    const Structure& S = *A.S;
+    cudaStream_t st = ctx.stream;
+    if (!fresh) {
+        HMB_REQUIRE(C.S && (C.S == A.S || same_structure(*C.S, *A.S)), HM_ERR_ARGUMENT,
+                    "C must share the factors' block structure");
+    }
+    const int maxRankC = fresh ? A.max_rank : C.max_rank;
+
+    // ---------------- symbolic phase ----------------
+    std::unique_ptr<HostScope> hs(new HostScope(ctx, "hh_symbolic"));
+    const std::shared_ptr<SymPlan> plan = get_plan(ctx, A, B, C, alpha, beta, fresh, maxRankC);
+    struct PlanView {
+        std::vector<WTask> w;
+        const PerBlock<LOp>& lops;
+        const PerBlock<DOp>& dops;
+    } P{plan->w, plan->lops, plan->dops};
+    // generator positions of the samples, from this call's starting state
+    for (WTask& t : P.w)
+        if (t.type == W_HH) t.omega = lcg_skip_host(ctx.serial_state, t.omega_steps);
+    const uint64_t serial_after = lcg_skip_host(ctx.serial_state, plan->serial_steps);
+    const std::vector<int>& crank = plan->crank;
+    const std::vector<int>& state_rank = plan->state_rank;
+    const std::vector<int>& op_kind = plan->op_kind;
 
     // ---------------- allocation ----------------
     // keep the old C storage if C is updated in place

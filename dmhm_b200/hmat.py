@@ -283,8 +283,12 @@ class _HMatBase:
             else:
                 C2 = Cout.reshape(-1, 1) if Cout.dim() == 1 else Cout
                 Ct = C2.t().contiguous()
+            # the engine runs on its context's stream: order it after torch's
+            # work on the operands, and torch's later reads after the product
+            torch.cuda.current_stream(B.device).synchronize()
             check(lib().hm_multiply_dense(self._h, transpose, float(alpha), C.c_void_p(Bt.data_ptr()),
                                           n, float(beta), C.c_void_p(Ct.data_ptr()), m, k))
+            self.ctx.synchronize()
             Cres = Ct.t()
             if Cout is not None:
                 (Cout.reshape(-1, 1) if Cout.dim() == 1 else Cout).copy_(Cres)

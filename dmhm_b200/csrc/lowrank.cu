@@ -172,10 +172,15 @@ __device__ void cta_jacobi(double* M, int rows, int cols, double* J, int* flag, 
                     b += __shfl_xor_sync(0xffffffffu, b, o);
                     c += __shfl_xor_sync(0xffffffffu, c, o);
                 }
-                if (live && c != 0.0 && a > tiny && b > tiny && fabs(c) > kJacobiTol * sqrt(a * b)) {
-                    const double zeta = (b - a) / (2.0 * c);
-                    const double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-                    const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
+                if (live && c != 0.0 && a > tiny && b > tiny &&
+                    c * c > (kJacobiTol * kJacobiTol) * (a * b)) {
+                    // t = tan of the rotation angle, the smaller root of
+                    // t^2 + 2 zeta t - 1 = 0 with zeta = (b - a) / (2c),
+                    // written as 2|c| / (|b - a| + sqrt((b - a)^2 + 4c^2))
+                    const double d = b - a;
+                    const double t = copysign(2.0 * fabs(c), d * c) /
+                                     (fabs(d) + sqrt(fma(d, d, 4.0 * c * c)));
+                    const double cs = rsqrt(fma(t, t, 1.0)), sn = cs * t;
                     for (int i = hl; i < rows; i += 16) {
                         const double x = gp[i], y = gq[i];
                         gp[i] = cs * x - sn * y;
@@ -457,9 +462,22 @@ void launch_round_workers(Context& ctx, const std::vector<RoundOp>& ops,
         HMB_REQUIRE(k <= kMaxK, HM_ERR_UNSUPPORTED,
                     "low-rank rounding of more than 128 stacked columns");
     }
-    // One launch; ops whose core and rotations fit use `kSmemDoubles` of
-    // shared memory for them, the stacked factors stay in the (L1-cached)
-    // global work area.
+    // One launch.  The core and the rotations of an op live in shared memory
+    // when they fit the launch's size, otherwise in the (L1-cached) global
+    // work area; the size is the largest need of the non-dense ops (dense
+    // compressions with larger cores take the global path), so that more
+    // CTAs share an SM.
+    long long smem = 0;
+    for (const RoundOp& op : ops) {
+        if (op.kind == ROUND_SET || op.kind == ROUND_CONCAT) continue;
+        const bool dense = op.kind == ROUND_DENSE;
+        const long long k = dense ? op.n : op.r1 + (op.kind == ROUND_GENERAL ? op.r2 : 0);
+        const long long ku = op.kind == ROUND_ORTHO ? op.r1 : std::min<long long>(op.m, k);
+        const long long kv = dense ? op.n : std::min<long long>(op.n, k);
+        const long long need = ku * kv + kv * kv;
+        if (!dense || need <= 3072) smem = std::max(smem, need);
+    }
+    smem = std::min(smem, kSmemDoubles);
     const int nw = (int)begin.size() - 1;
     std::vector<int> workers(nw);
     for (int w = 0; w < nw; ++w) workers[w] = w;
@@ -478,8 +496,8 @@ void launch_round_workers(Context& ctx, const std::vector<RoundOp>& ops,
     db.upload(begin, ctx.stream);
     dw.upload(workers, ctx.stream);
     LaunchScope ls(ctx, name);
-    round_worker_kernel<<<(unsigned)nw, kT, kSmemDoubles * sizeof(double), ctx.stream>>>(
-        d.get(), db.get(), dw.get(), kSmemDoubles);
+    round_worker_kernel<<<(unsigned)nw, kT, smem * sizeof(double), ctx.stream>>>(
+        d.get(), db.get(), dw.get(), smem);
     HMB_CHECK_LAUNCH();
 }
 

@@ -41,7 +41,7 @@ hm_matrix_s* new_handle(hm_context_s* ctx) {
 
 // Releases the device storage of a handle (stream-ordered frees).
 void release_storage(hm_matrix_s* m) {
-    m->h.templates.clear();
+    m->h.group.reset();
     m->h.data32.reset();
     m->h.data.reset();
     m->h.table.reset();
@@ -249,9 +249,14 @@ int hm_context_destroy(hm_context ctx) {
         ctx->models.clear();
         ctx->c.rank_model = nullptr;
         ctx->c.collect();
+        // everything holding device memory is freed on the stream before the
+        // stream goes away
+        ctx->c.layouts.clear();
+        ctx->c.hh_cache.reset();
         ctx->c.counters.reset();
         ctx->c.errword.reset();
         cudaStreamSynchronize(ctx->c.stream);
+        hmb::release_staging(ctx->c.stream);
         if (ctx->c.own_stream) cudaStreamDestroy(ctx->c.stream);
         delete ctx;
     });

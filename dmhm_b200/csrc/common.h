@@ -36,6 +36,13 @@ void set_last_error(const std::string& msg);
         if (!(cond)) throw ::hmb::Error((code), (msg));                       \
     } while (0)
 
+// Host-to-device copy of `bytes` from pageable `src` that does not block the
+// host behind the stream's earlier work: the data go through a pinned staging
+// ring owned per stream (the ring is reused after the stream has passed the
+// copies that read it).  Falls back to a plain copy when the data do not fit.
+void staged_h2d(void* dst, const void* src, size_t bytes, cudaStream_t s);
+void release_staging(cudaStream_t s);
+
 // Owning device allocation (cudaMallocAsync on the engine stream).
 template <typename T>
 class DeviceBuffer {
@@ -72,9 +79,7 @@ class DeviceBuffer {
     }
     void upload(const std::vector<T>& h, cudaStream_t s) {
         allocate(h.size(), s);
-        if (!h.empty())
-            HMB_CUDA(cudaMemcpyAsync(p_, h.data(), h.size() * sizeof(T),
-                                     cudaMemcpyHostToDevice, s));
+        if (!h.empty()) staged_h2d(p_, h.data(), h.size() * sizeof(T), s);
     }
     T* get() const { return p_; }
     size_t size() const { return n_; }

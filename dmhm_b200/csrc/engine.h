@@ -67,6 +67,9 @@ struct Context {
     int* zeroed_counters(long long n);
     DeviceBuffer<int> counters;
     long long counters_cap = 0;
+    // Layout groups (structure + ranks) with their product work lists
+    // (matmul.cu), most recently used last.
+    std::vector<std::shared_ptr<struct LayoutGroup>> layouts;
     // Symbolic H*H plans of recent products (hh.cu).
     std::shared_ptr<struct HHPlanCache> hh_cache;
     // Device word set by kernels whose bounded waits gave up (zero = fine).
@@ -132,9 +135,11 @@ class HMatrix {
     // made on first use, dropped whenever `data` changes.
     DeviceBuffer<float> data32;
     bool shadow_valid = false;
-    // Cached multiply work lists keyed by (subtree root, transpose); dropped
-    // whenever the storage is re-laid out.
-    mutable std::map<std::tuple<int, int, int>, std::shared_ptr<struct JobTemplate>> templates;
+    // Work lists of the products with this matrix, shared by every matrix of
+    // the context with the same structure and ranks (they hold storage
+    // offsets); found on first use, dropped whenever the storage is re-laid
+    // out.
+    mutable std::shared_ptr<struct LayoutGroup> group;
 
     int height() const { return S->N; }
     int width() const { return S->N; }

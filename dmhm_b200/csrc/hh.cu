@@ -618,6 +618,7 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
     // ---------------- symbolic phase ----------------
     std::unique_ptr<HostScope> hs(new HostScope(ctx, "hh_symbolic"));
     const std::shared_ptr<SymPlan> plan = get_plan(ctx, A, B, C, alpha, beta, fresh, maxRankC);
+    hs.reset(new HostScope(ctx, "hh_plan_copy"));
     struct PlanView {
         std::vector<WTask> w;
         const PerBlock<LOp>& lops;
@@ -631,6 +632,7 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
     const std::vector<int>& state_rank = plan->state_rank;
     const std::vector<int>& op_kind = plan->op_kind;
 
+    hs.reset(new HostScope(ctx, "hh_alloc_sampling"));
     // ---------------- allocation ----------------
     // keep the old C storage if C is updated in place
     DeviceBuffer<double> c_old_data;
@@ -1070,6 +1072,7 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
         wbuf.allocate((size_t)std::max<long long>(wk.used, 2), st);
         for (size_t i = 0; i < rops.size(); ++i) rops[i].work = wbuf.get() + rwork[i];
     }
+    hs.reset(new HostScope(ctx, "hh_block_launch"));
     launch_round_workers(ctx, rops, rbegin, "block_round");
     launch_gemm_workers(ctx, gops, gbegin, "dense_update");
     // low-rank C blocks whose final rank is 0 or that received no operation

@@ -6,6 +6,9 @@
 // are laid out in depth-first order so that a subtree's data is contiguous.
 #include <algorithm>
 
+#include <map>
+#include <mutex>
+#include <cstring>
 #include "engine.h"
 #include "rng.cuh"
 
@@ -13,7 +16,7 @@ namespace hmb {
 
 void HMatrix::layout() {
     const Structure& St = *S;
-    templates.clear();
+    group.reset();
     shadow_valid = false;
     off.assign(St.blocks.size(), -1);
     long long cur = 0;
@@ -47,6 +50,59 @@ void HMatrix::upload_table() {
         t[b] = d;
     }
     table.upload(t, ctx->stream);
+}
+
+namespace {
+
+// Pinned staging ring of one stream: copies take [head, head + bytes); when
+// the ring is full the host waits for the stream once (all copies that read
+// the ring are then done) and starts over.
+struct StagingRing {
+    char* buf = nullptr;
+    size_t cap = 0, head = 0;
+};
+constexpr size_t kStagingBytes = size_t(64) << 20;
+std::mutex g_staging_mu;
+std::map<cudaStream_t, StagingRing> g_staging;
+
+}  // namespace
+
+void staged_h2d(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    if (bytes == 0) return;
+    if (bytes > kStagingBytes / 4) {
+        HMB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+        return;
+    }
+    std::lock_guard<std::mutex> lock(g_staging_mu);
+    StagingRing& R = g_staging[s];
+    if (!R.buf) {
+        if (cudaMallocHost((void**)&R.buf, kStagingBytes) != cudaSuccess) {
+            R.buf = nullptr;
+            cudaGetLastError();
+            HMB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+            return;
+        }
+        R.cap = kStagingBytes;
+    }
+    const size_t need = (bytes + 255) & ~size_t(255);
+    if (R.head + need > R.cap) {
+        HMB_CUDA(cudaStreamSynchronize(s));
+        R.head = 0;
+    }
+    char* p = R.buf + R.head;
+    std::memcpy(p, src, bytes);
+    R.head += need;
+    HMB_CUDA(cudaMemcpyAsync(dst, p, bytes, cudaMemcpyHostToDevice, s));
+}
+
+// Drops the staging ring of a stream that is about to be destroyed.
+void release_staging(cudaStream_t s) {
+    std::lock_guard<std::mutex> lock(g_staging_mu);
+    auto it = g_staging.find(s);
+    if (it == g_staging.end()) return;
+    cudaStreamSynchronize(s);
+    if (it->second.buf) cudaFreeHost(it->second.buf);
+    g_staging.erase(it);
 }
 
 namespace {

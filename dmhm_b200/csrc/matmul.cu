@@ -30,6 +30,7 @@ namespace hmb {
 
 // What a CTA needs to run its share of one job.
 struct JobExec {
+    const double* hb;    // storage of the job's H-matrix (work lists hold offsets)
     const P1T* p1;
     const W1Tile* w1;
     const int* w1cp;     // wide: chunk prefix over the W1 tiles (n_w1 + 1)
@@ -53,6 +54,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
+constexpr size_t kLayoutGroups = 16;   // layout groups kept per context
 
 __device__ __forceinline__ int find_job(const JobExec* jobs, int njobs, long long idx,
                                         bool phase2) {
@@ -148,7 +150,7 @@ p1_stream_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0
             double v[16];
 #pragma unroll
             for (int f = 0; f < 16; ++f) v[f] = 0.0;
-            const double* wp = it.W + (long long)j0 * it.ldw;
+            const double* wp = J.hb + it.w + (long long)j0 * it.ldw;
             for (int pa = p0 + lane; pa < p1; pa += 64) {
                 const int pb = pa + 32;
                 const bool okb = pb < p1;
@@ -205,9 +207,9 @@ p1_stream_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0
 // ---------------------------------------------------------------------------
 // Phase 2: Y_tile = alpha sum_e A_e B_e + beta Y_tile
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double load_a(const P2Entry& e, int i, int p) {
-    return e.transA ? __ldg(e.A + p + (long long)i * e.lda)
-                    : __ldg(e.A + i + (long long)p * e.lda);
+__device__ __forceinline__ double load_a(const double* hb, const P2Entry& e, int i, int p) {
+    const double* A = hb + e.a;
+    return e.transA ? __ldg(A + p + (long long)i * e.lda) : __ldg(A + i + (long long)p * e.lda);
 }
 
 // B operand of an entry: (pointer to element (0,0), leading dimension).
@@ -313,7 +315,7 @@ p2_stream_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0
 #pragma unroll
                         for (int c = 0; c < NC; ++c)
                             bv[u][c] = (c < cols) ? __ldg(EB + (q + u) + (long long)c * ldb) : 0.0;
-                        av[u] = row_ok ? load_a(e, row, q + u) : 0.0;
+                        av[u] = row_ok ? load_a(J.hb, e, row, q + u) : 0.0;
                     }
 #pragma unroll
                     for (int u = 0; u < U; ++u)
@@ -321,7 +323,7 @@ p2_stream_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0
                         for (int c = 0; c < NC; ++c) acc[c] = fma(av[u], bv[u][c], acc[c]);
                 }
                 for (; q < qstop; ++q) {
-                    const double av = row_ok ? load_a(e, row, q) : 0.0;
+                    const double av = row_ok ? load_a(J.hb, e, row, q) : 0.0;
 #pragma unroll
                     for (int c = 0; c < NC; ++c)
                         if (c < cols) acc[c] = fma(av, __ldg(EB + q + (long long)c * ldb), acc[c]);
@@ -554,7 +556,7 @@ wide_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0, lon
             for (int e = tid; e < WT * KC; e += WTHREADS) {
                 const int p = e % KC, i = e / KC;   // W columns are contiguous
                 const bool v = p < len && i < rows;
-                const double* w0 = t->wcol[v ? i : 0];
+                const double* w0 = J.hb + t->wcol[v ? i : 0];
                 cp_async8(&sm.a[buf][p][i], v ? w0 + c.pos + p : w0, v);
             }
             load_b_chunk(sm, buf, J.in + t->in_off + c.pos + (long long)y * WT * J.ldin, J.ldin,
@@ -565,21 +567,22 @@ wide_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0, lon
             const P2T it = J.p2[c.tile];
             const P2Entry e = J.ent[c.ei];
             const int len = min(KC, e.inner - c.pos);
+            const double* E = J.hb + e.a;
             if (!e.transA) {
-                const double* A = e.A + it.r0 + (long long)c.pos * e.lda;
+                const double* A = E + it.r0 + (long long)c.pos * e.lda;
 #pragma unroll
                 for (int x = tid; x < WT * KC; x += WTHREADS) {
                     const int i = x % WT, p = x / WT;   // rows contiguous
                     const bool v = p < len && i < it.rows;
-                    cp_async8(&sm.a[buf][p][i], v ? A + i + (long long)p * e.lda : e.A, v);
+                    cp_async8(&sm.a[buf][p][i], v ? A + i + (long long)p * e.lda : E, v);
                 }
             } else {
-                const double* A = e.A + c.pos + (long long)it.r0 * e.lda;
+                const double* A = E + c.pos + (long long)it.r0 * e.lda;
 #pragma unroll
                 for (int x = tid; x < WT * KC; x += WTHREADS) {
                     const int p = x % KC, i = x / KC;   // inner index contiguous
                     const bool v = p < len && i < it.rows;
-                    cp_async8(&sm.a[buf][p][i], v ? A + p + (long long)i * e.lda : e.A, v);
+                    cp_async8(&sm.a[buf][p][i], v ? A + p + (long long)i * e.lda : E, v);
                 }
             }
             const double* EB;
@@ -739,12 +742,12 @@ std::shared_ptr<JobTemplate> build_template(Context& ctx, const HMatrix& H, int 
         if (B.kind != KIND_LOWRANK || H.rank[b] == 0) continue;
         P1T it{};
         if (!trans) {
-            it.W = H.V(b);
+            it.w = H.V(b) - H.data.get();
             it.nin = B.n;
             it.ldw = B.n;
             it.in_off = B.col_off - R.col_off;
         } else {
-            it.W = H.U(b);
+            it.w = H.U(b) - H.data.get();
             it.nin = B.m;
             it.ldw = B.m;
             it.in_off = B.row_off - R.row_off;
@@ -782,7 +785,7 @@ std::shared_ptr<JobTemplate> build_template(Context& ctx, const HMatrix& H, int 
                         cur.in_off = io;
                         cur.nin = ni;
                     }
-                    cur.wcol[cur.rows] = p1[i].W + (long long)j * p1[i].ldw;
+                    cur.wcol[cur.rows] = p1[i].w + (long long)j * p1[i].ldw;
                     cur.trel[cur.rows] = p1[i].t_rel;
                     cur.tj[cur.rows] = j;
                     cur.tr[cur.rows] = p1[i].r;
@@ -829,13 +832,13 @@ std::shared_ptr<JobTemplate> build_template(Context& ctx, const HMatrix& H, int 
             P2Entry e{};
             if (B.kind == KIND_DENSE) {
                 if (!trans) {
-                    e.A = H.D(b) + (cl.offset - B.row_off);
+                    e.a = H.D(b) - H.data.get() + (cl.offset - B.row_off);
                     e.lda = B.m;
                     e.transA = 0;
                     e.inner = B.n;
                     e.b_off = B.col_off - R.col_off;
                 } else {
-                    e.A = H.D(b) + (long long)(cl.offset - B.col_off) * B.m;
+                    e.a = H.D(b) - H.data.get() + (long long)(cl.offset - B.col_off) * B.m;
                     e.lda = B.m;
                     e.transA = 1;
                     e.inner = B.m;
@@ -845,10 +848,10 @@ std::shared_ptr<JobTemplate> build_template(Context& ctx, const HMatrix& H, int 
             } else {
                 if (H.rank[b] == 0) continue;
                 if (!trans) {
-                    e.A = H.U(b) + (cl.offset - B.row_off);
+                    e.a = H.U(b) - H.data.get() + (cl.offset - B.row_off);
                     e.lda = B.m;
                 } else {
-                    e.A = H.V(b) + (cl.offset - B.col_off);
+                    e.a = H.V(b) - H.data.get() + (cl.offset - B.col_off);
                     e.lda = B.n;
                 }
                 e.transA = 0;
@@ -919,17 +922,52 @@ std::shared_ptr<JobTemplate> build_template(Context& ctx, const HMatrix& H, int 
 
 }  // namespace
 
+// The layout group of H in its context (created on first use).
+LayoutGroup& layout_group(Context& ctx, const HMatrix& H) {
+    if (H.group) return *H.group;
+    uint64_t h = 1469598103934665603ULL;
+    auto mix = [&](const void* p, size_t n) {
+        const unsigned char* c = static_cast<const unsigned char*>(p);
+        for (size_t i = 0; i < n; ++i) h = (h ^ c[i]) * 1099511628211ULL;
+    };
+    const Structure* S = H.S.get();
+    mix(&S, sizeof(S));
+    mix(&H.max_rank, sizeof(int));
+    mix(H.rank.data(), H.rank.size() * sizeof(int));
+    auto& L = ctx.layouts;
+    for (size_t i = 0; i < L.size(); ++i) {
+        LayoutGroup& g = *L[i];
+        if (g.hash == h && g.S == S && g.max_rank == H.max_rank && g.rank == H.rank) {
+            auto keep = L[i];
+            L.erase(L.begin() + (long long)i);
+            L.push_back(keep);
+            H.group = keep;
+            return *keep;
+        }
+    }
+    auto g = std::make_shared<LayoutGroup>();
+    g->S = S;
+    g->max_rank = H.max_rank;
+    g->rank = H.rank;
+    g->hash = h;
+    L.push_back(g);
+    if (L.size() > kLayoutGroups) L.erase(L.begin());
+    H.group = g;
+    return *g;
+}
+
 std::shared_ptr<JobTemplate> get_template(Context& ctx, const HMatrix& H, int root, bool trans,
                                           int row_tile) {
     HMB_REQUIRE(row_tile >= 1 && row_tile <= 64, HM_ERR_INTERNAL, "row tile out of range");
+    LayoutGroup& G = layout_group(ctx, H);
     auto key = std::make_tuple(root, trans ? 1 : 0, row_tile);
-    auto it = H.templates.find(key);
-    if (it != H.templates.end()) return it->second;
+    auto it = G.templates.find(key);
+    if (it != G.templates.end()) return it->second;
     auto T = build_template(ctx, H, root, trans, row_tile);
     HMB_REQUIRE((T->n1 == 0 || T->p1.get()) && (T->n2 == 0 || (T->p2.get() && T->ent.get())) &&
                     (T->nz == 0 || T->zero_tiles.get()) && (T->nw1 == 0 || T->w1.get()),
                 HM_ERR_INTERNAL, "work lists missing on the device");
-    H.templates.emplace(key, T);
+    G.templates.emplace(key, T);
     return T;
 }
 
@@ -1113,6 +1151,7 @@ void run_jobs(Context& ctx, const std::vector<MatJob>& jobs) {
         if (ex.empty()) first_job = j;
         const JobTemplate& T = *tmpl[j];
         JobExec e{};
+        e.hb = J.H->data.get();
         e.p1 = T.p1.get();
         e.w1 = T.w1.get();
         e.p2 = T.p2.get();

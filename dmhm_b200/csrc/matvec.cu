@@ -45,8 +45,7 @@ enum : int { MU_LR = 0, MU_DENSE = 1, MU_DENSE_T = 2, MU_TSLAB = 3, MU_YSLAB = 4
 //  MU_YSLAB:   y = M2 (sum of the big block's tparts) (M2: rows_out x r)
 // y is the partial buffer at y_off.
 struct MvUnit {
-    const double* M1;
-    const double* M2;
+    long long m1, m2;   // element offsets of M1, M2 in the matrix storage
     long long in_off, y_off;
     int kind, rows_in, rows_out, r;
     int ld1, ld2, big, slab;
@@ -247,6 +246,7 @@ __device__ void dispatch_rc(const double* M, int ld, int R, int C, const double*
 }
 
 struct MvArgs {
+    const double* hb;  // matrix storage
     const MvUnit* units;
     const MvBig* big;
     const double* x;
@@ -276,24 +276,26 @@ __global__ void __launch_bounds__(kThreads, 2) mv_blocks_kernel(const MvArgs a) 
         if (un_next < a.nunits && lane == 0)
             asm volatile("prefetch.global.L1 [%0];" ::"l"(a.units + un_next));
         const MvUnit un = a.units[u];
+        const double* M1 = a.hb + un.m1;
+        const double* M2 = a.hb + un.m2;
         const double* x = a.x + un.in_off;
         double* y = a.part + un.y_off;
         switch (un.kind) {
             case MU_LR:
-                dispatch_cd(un.M1, un.ld1, un.rows_in, un.r, x, t, lane, pol);
+                dispatch_cd(M1, un.ld1, un.rows_in, un.r, x, t, lane, pol);
                 __syncwarp();
-                dispatch_rc<false>(un.M2, un.ld2, un.rows_out, un.r, t, y, lane, pol, keep);
+                dispatch_rc<false>(M2, un.ld2, un.rows_out, un.r, t, y, lane, pol, keep);
                 __syncwarp();
                 break;
             case MU_DENSE:
-                dispatch_rc<true>(un.M1, un.ld1, un.rows_out, un.r, x, y, lane, pol, keep);
+                dispatch_rc<true>(M1, un.ld1, un.rows_out, un.r, x, y, lane, pol, keep);
                 break;
             case MU_DENSE_T:
-                dispatch_cd(un.M1, un.ld1, un.rows_in, un.r, x, y, lane, pol);
+                dispatch_cd(M1, un.ld1, un.rows_in, un.r, x, y, lane, pol);
                 break;
             case MU_TSLAB: {
                 const MvBig B = a.big[un.big];
-                dispatch_cd(un.M1, un.ld1, un.rows_in, un.r, x, a.tpart + B.t_off + (long long)un.slab * B.r,
+                dispatch_cd(M1, un.ld1, un.rows_in, un.r, x, a.tpart + B.t_off + (long long)un.slab * B.r,
                             lane, pol);
                 __syncwarp();
                 if (lane == 0) red_add_release(a.done + un.big, 1);
@@ -317,7 +319,7 @@ __global__ void __launch_bounds__(kThreads, 2) mv_blocks_kernel(const MvArgs a) 
                     t[j] = s;
                 }
                 __syncwarp();
-                dispatch_rc<false>(un.M2, un.ld2, un.rows_out, un.r, t, y, lane, pol, keep);
+                dispatch_rc<false>(M2, un.ld2, un.rows_out, un.r, t, y, lane, pol, keep);
                 __syncwarp();
                 break;
             }
@@ -458,7 +460,7 @@ std::shared_ptr<MvPlan> build_plan(Context& ctx, const HMatrix& H, int root, boo
             yoff[b] = part;
             MvUnit u{};
             u.kind = trans ? MU_DENSE_T : MU_DENSE;
-            u.M1 = H.D(b);
+            u.m1 = H.D(b) - H.data.get();
             u.ld1 = B.m;
             if (!trans) {
                 u.rows_out = nout;
@@ -477,15 +479,15 @@ std::shared_ptr<MvPlan> build_plan(Context& ctx, const HMatrix& H, int root, boo
         const int r = H.rank[b];
         if (r == 0) continue;
         if (r > kMaxRank) return nullptr;
-        const double* W = trans ? H.U(b) : H.V(b);
-        const double* A = trans ? H.V(b) : H.U(b);
+        const long long W = (trans ? H.U(b) : H.V(b)) - H.data.get();
+        const long long A = (trans ? H.V(b) : H.U(b)) - H.data.get();
         yoff[b] = part;
         if (nin <= kMaxRows && nout <= kMaxRows) {
             MvUnit u{};
             u.kind = MU_LR;
-            u.M1 = W;
+            u.m1 = W;
             u.ld1 = nin;
-            u.M2 = A;
+            u.m2 = A;
             u.ld2 = nout;
             u.rows_in = nin;
             u.rows_out = nout;
@@ -505,7 +507,7 @@ std::shared_ptr<MvPlan> build_plan(Context& ctx, const HMatrix& H, int root, boo
             for (int sl = 0; sl < g.nslab; ++sl) {
                 MvUnit u{};
                 u.kind = MU_TSLAB;
-                u.M1 = W + (long long)sl * kMaxRows;
+                u.m1 = W + (long long)sl * kMaxRows;
                 u.ld1 = nin;
                 u.rows_in = std::min(kMaxRows, nin - sl * kMaxRows);
                 u.r = r;
@@ -518,7 +520,7 @@ std::shared_ptr<MvPlan> build_plan(Context& ctx, const HMatrix& H, int root, boo
             for (auto [a0, a1] : pcs) {
                 MvUnit u{};
                 u.kind = MU_YSLAB;
-                u.M2 = A + a0;
+                u.m2 = A + a0;
                 u.ld2 = nout;
                 u.rows_out = a1 - a0;
                 u.r = r;
@@ -585,6 +587,7 @@ bool multiply_vector_streamed(Context& ctx, const MatJob& J) {
     });
     const int g = std::max(1, std::min(per_sm * ctx.num_sms, (P.nunits + kWarps - 1) / kWarps));
     MvArgs a{};
+    a.hb = J.H->data.get();
     a.units = P.units.get();
     a.big = P.big.get();
     a.x = J.in;

@@ -379,7 +379,7 @@ SchulzResult schulz_invert(Context& ctx, HMatrix& A, int num_iterations, double 
     A.data = std::move(X->data);
     A.shadow_valid = false;
     A.table = std::move(X->table);
-    A.templates.clear();
+    A.group.reset();
     return res;
 }
 

@@ -123,7 +123,7 @@ __device__ __forceinline__ int kmaj_off(int r, int k) {
     return (r >> 3) * ((kKC / 4) * 128) + (k >> 2) * 128 + (r & 7) * 16 + (k & 3) * 4;
 }
 struct TcArgs {
-    const double* base64;    // H-matrix FP64 storage (template pointers live here)
+    const double* base64;    // H-matrix FP64 storage
     const float* base32;     // its TF32-rounded FP32 copy
     const float* X;          // input, FP32, column-major (n x k, ld ldx)
     float* T;                // phase-1 results T_b^T, k x r each (ld r)
@@ -136,9 +136,6 @@ struct TcArgs {
     int ldx, ldy, k;
 };
 
-__device__ __forceinline__ const float* to32(const TcArgs& a, const double* p) {
-    return a.base32 + (p - a.base64);
-}
 
 // ---------------------------------------------------------------------------
 // Phase 1: T_b^T (k x r) = X_b^T (k x n) * V_b (n x r), one CTA per block.
@@ -169,7 +166,7 @@ __global__ void __launch_bounds__(kTcThreads) tc_lowrank_inner_kernel(const TcAr
     tc_fence_after();
     const uint32_t tmem = tmem_base;
     const float* X = a.X + it.in_off;
-    const float* V = to32(a, it.W);
+    const float* V = a.base32 + it.w;
     const uint32_t idesc = idesc_tf32(kM, N, 0, 0);
     uint32_t phase = 0;
     bool ok = true;
@@ -268,7 +265,7 @@ __global__ void __launch_bounds__(kTcThreads) tc_row_tiles_kernel(const TcArgs a
     bool ok = true, any = false;
     for (int ei = it.e0; ei < it.e1 && ok; ++ei) {
         const P2Entry e = a.ent[ei];
-        const float* Bsrc = to32(a, e.A);      // rows of U or D (staged K-major)
+        const float* Bsrc = a.base32 + e.a;    // rows of U or D (staged K-major)
         const float* Asrc;                     // T_b^T or X rows
         int lda_src;
         if (e.b_from_t) { Asrc = a.T + e.b_off * a.k; lda_src = e.ldt; }

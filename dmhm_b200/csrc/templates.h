@@ -2,6 +2,7 @@
 // by the FP64 and the tensor-core H-matrix x dense products.
 #pragma once
 #include <map>
+#include <tuple>
 #include <memory>
 #include <vector>
 
@@ -9,9 +10,11 @@
 
 namespace hmb {
 
-// Work lists of one subtree (device arrays), independent of the operands.
+// Work lists of one subtree (device arrays), independent of the operands and
+// of where the matrix storage lives: every block is an element offset into
+// the storage, so matrices with the same structure and ranks share them.
 struct P1T {
-    const double* W;   // nin x r, ld ldw
+    long long w;       // W: nin x r, ld ldw, at storage + w
     long long in_off;  // row offset into the job input
     long long t_rel;   // T_b = T + t_rel * k (r x k, ld r)
     long long c0;      // first row of this item in the concatenation of all items' rows
@@ -27,7 +30,7 @@ struct P2T {
 };
 
 struct P2Entry {
-    const double* A;   // element (i,p) = transA ? A[p + i*lda] : A[i + p*lda]
+    long long a;       // A at storage + a: element (i,p) = transA ? A[p + i*lda] : A[i + p*lda]
     long long b_off;   // b_from_t ? T + b_off * k (ld ldt) : job input + b_off
     int lda, inner, transA, b_from_t, ldt;
     int cbeg;          // first column of this entry in its tile's concatenation
@@ -36,12 +39,12 @@ struct P2Entry {
 // Phase-1 tile of the wide (many-column) product: 64 rows of T gathered from
 // the low-rank blocks that share one source box (so one input slice, rows
 // [in_off, in_off + nin)).  Row i is column wcol[i] of some W; its results
-// go to T[trel[i] * k + tj[i] + c * tr[i]].
+// go to T[trel[i] * k + tj[i] + c * tr[i]].  wcol: storage offsets.
 constexpr int kWideTile = 64;
 struct W1Tile {
     long long in_off;
     int nin, rows;
-    const double* wcol[kWideTile];
+    long long wcol[kWideTile];
     long long trel[kWideTile];
     int tj[kWideTile];
     int tr[kWideTile];
@@ -75,6 +78,16 @@ struct JobTemplate {
     long long c1 = 0, c2 = 0;       // rows of all items, columns of all tiles
     int rmax = 0;                   // largest rank among the items
     long long t_rows = 0;   // sum of the ranks: T holds t_rows * k entries
+};
+
+// Matrices of one context with the same structure, rank cap and ranks (so the
+// same storage layout) and the work lists of their products.
+struct LayoutGroup {
+    const Structure* S = nullptr;
+    int max_rank = 0;
+    std::vector<int> rank;
+    uint64_t hash = 0;
+    std::map<std::tuple<int, int, int>, std::shared_ptr<JobTemplate>> templates;
 };
 
 }  // namespace hmb

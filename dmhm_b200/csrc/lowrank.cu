@@ -127,7 +127,8 @@ __device__ __forceinline__ int rr_pos(int i, int step, int n) {
 // the squared Frobenius norm of M) are left alone: rotating noise against
 // noise never settles, and such columns carry no singular value above
 // rounding level.
-__device__ void cta_jacobi(double* M, int rows, int cols, double* J, int* flag, double* red) {
+__device__ void cta_jacobi(double* M, int rows, int cols, double* J, int* flag, double* red,
+                           double* nrm) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int e = threadIdx.x; e < cols * cols; e += kT)
         J[e] = (e % cols == e / cols) ? 1.0 : 0.0;
@@ -139,9 +140,18 @@ __device__ void cta_jacobi(double* M, int rows, int cols, double* J, int* flag, 
     if (cols < 2) return;
     const int n = cols + (cols & 1);
     // one half-warp (16 lanes) per pair: all cols/2 pairs of a step at once
-    // for up to 32 columns
+    // for up to 32 columns.  Squared column norms are kept in nrm (exact at
+    // the start of every sweep, then updated by the rotations), so a pair
+    // reduces only its inner product.
     const int hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
     for (int sweep = 0; sweep < kJacobiSweeps; ++sweep) {
+        for (int c = warp; c < cols; c += kW) {
+            const double* g = M + (long long)c * rows;
+            double sq = 0.0;
+            for (int i = lane; i < rows; i += 32) sq = fma(g[i], g[i], sq);
+            sq = warp_sum(sq);
+            if (lane == 0) nrm[c] = sq;
+        }
         if (threadIdx.x == 0) *flag = 0;
         __syncthreads();
         for (int step = 0; step < n - 1; ++step) {
@@ -158,20 +168,12 @@ __device__ void cta_jacobi(double* M, int rows, int cols, double* J, int* flag, 
                 if (p > q) { int t = p; p = q; q = t; }
                 double* gp = M + (long long)p * rows;
                 double* gq = M + (long long)q * rows;
-                double a = 0.0, b = 0.0, c = 0.0;
+                double c = 0.0;
                 if (live)
-                    for (int i = hl; i < rows; i += 16) {
-                        const double x = gp[i], y = gq[i];
-                        a = fma(x, x, a);
-                        b = fma(y, y, b);
-                        c = fma(x, y, c);
-                    }
+                    for (int i = hl; i < rows; i += 16) c = fma(gp[i], gq[i], c);
 #pragma unroll
-                for (int o = 8; o > 0; o >>= 1) {
-                    a += __shfl_xor_sync(0xffffffffu, a, o);
-                    b += __shfl_xor_sync(0xffffffffu, b, o);
-                    c += __shfl_xor_sync(0xffffffffu, c, o);
-                }
+                for (int o = 8; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+                const double a = live ? nrm[p] : 0.0, b = live ? nrm[q] : 0.0;
                 if (live && c != 0.0 && a > tiny && b > tiny &&
                     c * c > (kJacobiTol * kJacobiTol) * (a * b)) {
                     // t = tan of the rotation angle, the smaller root of
@@ -193,7 +195,11 @@ __device__ void cta_jacobi(double* M, int rows, int cols, double* J, int* flag, 
                         jp[i] = cs * x - sn * y;
                         jq[i] = sn * x + cs * y;
                     }
-                    if (hl == 0) *flag = 1;
+                    if (hl == 0) {
+                        nrm[p] = fma(-t, c, a);
+                        nrm[q] = fma(t, c, b);
+                        *flag = 1;
+                    }
                 }
             }
             __syncthreads();
@@ -202,7 +208,6 @@ __device__ void cta_jacobi(double* M, int rows, int cols, double* J, int* flag, 
         __syncthreads();
         if (!again) break;
     }
-    (void)lane;
 }
 
 // order[0..cols) = column indices of M by decreasing norm (ties by index).
@@ -232,6 +237,7 @@ __device__ void cta_order_columns(const double* M, int rows, int cols, double* n
 struct RoundShared {
     double red[kW + 1];
     double norms[kMaxK];
+    double nrm[kMaxK];    // Jacobi's running squared column norms
     int order[kMaxK];
     int flag;
 };
@@ -301,16 +307,20 @@ __device__ void do_round(const RoundOp& op_in, double* dyn, long long smem_doubl
 
     // ---- stacked factors ---------------------------------------------------
     if (op.kind == ROUND_GENERAL) {
-        const int r1 = op.r1;
+        // [beta U2, alpha U1], [V2, V1]: U2 (the block's current factors, the
+        // output of an earlier rounding) has orthogonal columns and V2
+        // orthonormal ones, so the leading part of the core is already
+        // diagonal and the Jacobi sweeps mostly rotate the new columns in
+        const int r2 = op.r2;
         for (long long e = tid; e < (long long)m * k; e += kT) {
             int i = (int)(e % m), c = (int)(e / m);
-            Ucat[e] = c < r1 ? op.alpha * op.u1[i + (long long)c * op.ldu1]
-                             : op.beta * op.u2[i + (long long)(c - r1) * op.ldu2];
+            Ucat[e] = c < r2 ? op.beta * op.u2[i + (long long)c * op.ldu2]
+                             : op.alpha * op.u1[i + (long long)(c - r2) * op.ldu1];
         }
         for (long long e = tid; e < (long long)n * k; e += kT) {
             int i = (int)(e % n), c = (int)(e / n);
-            Vcat[e] = c < r1 ? op.v1[i + (long long)c * op.ldv1]
-                             : op.v2[i + (long long)(c - r1) * op.ldv2];
+            Vcat[e] = c < r2 ? op.v2[i + (long long)c * op.ldv2]
+                             : op.v1[i + (long long)(c - r2) * op.ldv1];
         }
     } else if (dense) {
         for (long long e = tid; e < (long long)m * n; e += kT) {
@@ -351,7 +361,7 @@ __device__ void do_round(const RoundOp& op_in, double* dyn, long long smem_doubl
     __syncthreads();
 
     // ---- SVD of the core ---------------------------------------------------
-    cta_jacobi(M, ku, kv, J, &sh.flag, red);
+    cta_jacobi(M, ku, kv, J, &sh.flag, red, sh.nrm);
     cta_order_columns(M, ku, kv, norms, order);
 
     // ---- outputs -------------------------------------------------------------

@@ -632,7 +632,7 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
     const std::vector<int>& state_rank = plan->state_rank;
     const std::vector<int>& op_kind = plan->op_kind;
 
-    hs.reset(new HostScope(ctx, "hh_alloc_sampling"));
+    hs.reset(new HostScope(ctx, "hh_alloc"));
     // ---------------- allocation ----------------
     // keep the old C storage if C is updated in place
     DeviceBuffer<double> c_old_data;
@@ -709,6 +709,7 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
     }
 
     // ---------------- randomized sampling ----------------
+    hs.reset(new HostScope(ctx, "hh_sampling"));
     std::vector<int> hh;
     for (int i = 0; i < (int)P.w.size(); ++i)
         if (P.w[i].type == W_HH && P.w[i].r > 0) hh.push_back(i);
@@ -824,6 +825,7 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
             launch_round_ops(ctx, ops, "sample_round");
         }
     };
+    hs.reset(new HostScope(ctx, "hh_lr_jobs"));
     // W.U = alpha A B.U for node x low-rank, W.V = alpha B^T A.V for
     // low-rank x node
     {
@@ -840,6 +842,7 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
                                 const_cast<double*>(t.V), t.n, t.r});
         run_jobs(ctx, jobs);
     }
+    hs.reset(new HostScope(ctx, "hh_sample_pipeline"));
     if (!hh.empty()) sample(hh);
     if (learned) {
         // probe check: redo with the plain sample count every compression

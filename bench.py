@@ -382,16 +382,25 @@ def tf32_leg(ctx, H, stream, X, Y, nrhs, nbytes, args):
         _lib.check(lib.hm_multiply_dense_tf32(H.handle, 1.0, C.c_void_p(X.data_ptr()), N, 0.0,
                                               C.c_void_p(Y2.data_ptr()), N, nrhs))
 
-    for _ in range(max(3, args.warmup)):
-        mm()
-    ctx.synchronize()
-    ms = _time_steps(stream, mm, max(5, args.steps))
     _lib.check(lib.hm_multiply_dense(H.handle, 0, 1.0, C.c_void_p(X.data_ptr()), N, 0.0,
                                      C.c_void_p(Y.data_ptr()), N, nrhs))
     ctx.synchronize()
-    err = float((Y2 - Y).norm() / Y.norm())
+    forms = {}
+    for which, name in ((1, "tcgen05"), (2, "mma_sync"), (0, "autotuned")):
+        _lib.check(lib.hm_set_tf32_kernel(ctx.handle, which))
+        for _ in range(max(3, args.warmup)):
+            mm()
+        ctx.synchronize()
+        ms = _time_steps(stream, mm, max(5, args.steps))
+        err = float((Y2 - Y).norm() / Y.norm())
+        forms[name] = {"ms_per_step": ms, "rel_err_vs_fp64": err}
+    w = C.c_int(0)
+    _lib.check(lib.hm_tf32_kernel_choice(H.handle, C.c_void_p(X.data_ptr()), N, nrhs, C.byref(w)))
+    ms = forms["autotuned"]["ms_per_step"]
     return {"value": nbytes / (ms * 1e-3) / 1e9, "unit": "GB/s", "ms_per_step": ms,
-            "rel_err_vs_fp64": err, "dtype": "tf32 inputs, f32 accumulation"}
+            "rel_err_vs_fp64": forms["autotuned"]["rel_err_vs_fp64"],
+            "autotuned_choice": {1: "tcgen05", 2: "mma_sync"}[w.value], "forms": forms,
+            "dtype": "tf32 inputs, f32 accumulation"}
 
 
 def kernel_bytes(name, census, N, nrhs, H):

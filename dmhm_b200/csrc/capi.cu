@@ -292,6 +292,25 @@ int hm_set_compression_tolerance(hm_context ctx, double tol) {
     });
 }
 
+int hm_set_tf32_kernel(hm_context ctx, int which) {
+    return guarded([&] {
+        HMB_REQUIRE(ctx, HM_ERR_ARGUMENT, "ctx is NULL");
+        HMB_REQUIRE(which >= 0 && which <= 2, HM_ERR_ARGUMENT, "which must be 0, 1 or 2");
+        ctx->c.tf32_kernel = which;
+    });
+}
+
+int hm_tf32_kernel_choice(hm_matrix h, const double* B, int ldb, int nrhs, int* which) {
+    return guarded([&] {
+        HMB_REQUIRE(h && which && (nrhs == 0 || B), HM_ERR_ARGUMENT, "NULL argument");
+        owner_of(h);
+        HMB_REQUIRE(h->h.S != nullptr, HM_ERR_ARGUMENT, "empty H-matrix");
+        HMB_REQUIRE(nrhs > 0 && ldb >= std::max(1, h->h.width()), HM_ERR_ARGUMENT,
+                    "bad right-hand sides");
+        *which = tf32_kernel_choice(*h->h.ctx, h->h, B, ldb, nrhs);
+    });
+}
+
 int hm_get_compression_tolerance(hm_context ctx, double* tol) {
     return guarded([&] {
         HMB_REQUIRE(ctx && tol, HM_ERR_ARGUMENT, "NULL argument");

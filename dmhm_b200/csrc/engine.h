@@ -72,6 +72,10 @@ struct Context {
     std::vector<std::shared_ptr<struct LayoutGroup>> layouts;
     // Symbolic H*H plans of recent products (hh.cu).
     std::shared_ptr<struct HHPlanCache> hh_cache;
+    // Kernels of the TF32 dense product: 0 autotuned per (layout, column
+    // bucket), 1 tcgen05 (at most 64 columns, ranks <= 256), 2 mma.sync.
+    int tf32_kernel = 0;
+    std::map<std::pair<uint64_t, int>, int> tf32_tuned;
     // Device word set by kernels whose bounded waits gave up (zero = fine).
     int* error_word();
     DeviceBuffer<int> errword;
@@ -177,14 +181,21 @@ std::shared_ptr<JobTemplate> get_template(Context& ctx, const HMatrix& H, int ro
 
 // Runs a batch of jobs as two level-batched launches (low-rank inner products,
 // then one fused output pass per row tile).  Outputs of different jobs must
-// not overlap; inputs may alias each other but not outputs.
-void run_jobs(Context& ctx, const std::vector<MatJob>& jobs);
+// not overlap; inputs may alias each other but not outputs.  tf32: jobs with
+// more than 8 columns multiply on the TF32 tensor cores (FP32 copies of the
+// blocks and inputs, FP32 accumulation, FP64 output).
+void run_jobs(Context& ctx, const std::vector<MatJob>& jobs, bool tf32 = false);
 // One-vector product of one job streamed block by block (matvec.cu); false
 // when the matrix does not fit that kernel (the caller uses run_jobs' lists).
 bool multiply_vector_streamed(Context& ctx, const MatJob& job);
 
 // Tensor-core (TF32, FP32 accumulation) H-matrix x dense, device pointers;
-// at most 64 right-hand sides; synchronizes (checks the kernels' error word).
+// synchronizes (checks the kernels' error word).  The kernel form comes from
+// tf32_kernel_choice (tc_matmul.cu).
+int tf32_kernel_choice(Context& ctx, HMatrix& H, const double* B, int ldb, int nrhs);
+// FP32 copy of the block data rounded to TF32 (data32), made on first use
+// and kept until the data change.
+void ensure_tf32_copy(Context& ctx, HMatrix& H);
 void multiply_dense_tf32(HMatrix& H, double alpha, const double* B, int ldb, double beta,
                          double* C, int ldc, int nrhs);
 

@@ -19,6 +19,8 @@
 // Every stored matrix entry is read exactly once per launch pair.  A CTA finds
 // its job by binary search over the jobs' first work-item indices.
 #include <algorithm>
+#include <tuple>
+#include <type_traits>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -31,6 +33,10 @@ namespace hmb {
 // What a CTA needs to run its share of one job.
 struct JobExec {
     const double* hb;    // storage of the job's H-matrix (work lists hold offsets)
+    const float* hb32;   // TF32 path: its TF32-rounded FP32 copy
+    const float* in32;   // TF32 path: the input, rounded, ld ldin32
+    float* T32;          // TF32 path: phase-1 results
+    int ldin32, pad32;
     const P1T* p1;
     const W1Tile* w1;
     const int* w1cp;     // wide: chunk prefix over the W1 tiles (n_w1 + 1)
@@ -420,10 +426,36 @@ constexpr int WTHREADS = 128;   // 2 x 2 warps of 32 x 32
 constexpr int SP = WT + 8;      // smem row: fragment loads hit 32 distinct banks
 
 constexpr int NSTAGE = 2;       // chunk buffers per CTA
-struct WideSmem {
-    double a[NSTAGE][KC][SP];   // a[buf][p][i] = A(i, p)
-    double b[NSTAGE][KC][SP];   // b[buf][p][c] = B(p, c)
+template <typename E>
+struct WideSmemT {
+    E a[NSTAGE][KC][SP];   // a[buf][p][i] = A(i, p)
+    E b[NSTAGE][KC][SP];   // b[buf][p][c] = B(p, c)
 };
+using WideSmem = WideSmemT<double>;
+
+__device__ __forceinline__ void cp_async4(float* dst, const float* src, bool valid) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src),
+                 "r"(valid ? 4 : 0)
+                 : "memory");
+}
+
+// TF32 tensor-core MMA 16 x 8 x 8, FP32 accumulation.  Fragments (g = lane/4,
+// t = lane%4): A a0 (g, t), a1 (g+8, t), a2 (g, t+4), a3 (g+8, t+4); B b0 (t, g),
+// b1 (t+4, g); C c0 (g, 2t), c1 (g, 2t+1), c2 (g+8, 2t), c3 (g+8, 2t+1).
+__device__ __forceinline__ void tmma(float* d, const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+        "{%8, %9}, {%0, %1, %2, %3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__device__ __forceinline__ float round_tf32(double x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"((float)x));
+    return __uint_as_float(r);
+}
 
 __device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
@@ -449,6 +481,41 @@ __device__ __forceinline__ int acc_row(int s, int warp, int lane) {
 }
 __device__ __forceinline__ int acc_col(int s, int warp, int lane) {
     return (warp >> 1) * 32 + ((s >> 1) & 3) * 8 + 2 * (lane & 3) + (s & 1);
+}
+
+// TF32 tiles: slot s = ((mb * 4 + nb) * 4 + e) of MMA block (mb, nb) (16 x 8)
+// of the warp's 32 x 32 quarter, C fragment element e.
+__device__ __forceinline__ int acc_row_tf(int s, int warp, int lane) {
+    return (warp & 1) * 32 + (s >> 4) * 16 + (lane >> 2) + ((s & 2) ? 8 : 0);
+}
+__device__ __forceinline__ int acc_col_tf(int s, int warp, int lane) {
+    return (warp >> 1) * 32 + ((s >> 2) & 3) * 8 + 2 * (lane & 3) + (s & 1);
+}
+
+__device__ __forceinline__ void wide_mma_tf(const WideSmemT<float>& sm, int buf, int warp, int lane,
+                                            float (&acc)[32]) {
+    const int g = lane >> 2, t = lane & 3;
+    const int r0 = (warp & 1) * 32 + g, c0 = (warp >> 1) * 32 + g;
+#pragma unroll
+    for (int kb = 0; kb < KC; kb += 8) {
+        uint32_t a[2][4], b[4][2];
+#pragma unroll
+        for (int mb = 0; mb < 2; ++mb) {
+            a[mb][0] = __float_as_uint(sm.a[buf][kb + t][r0 + mb * 16]);
+            a[mb][1] = __float_as_uint(sm.a[buf][kb + t][r0 + mb * 16 + 8]);
+            a[mb][2] = __float_as_uint(sm.a[buf][kb + t + 4][r0 + mb * 16]);
+            a[mb][3] = __float_as_uint(sm.a[buf][kb + t + 4][r0 + mb * 16 + 8]);
+        }
+#pragma unroll
+        for (int nb = 0; nb < 4; ++nb) {
+            b[nb][0] = __float_as_uint(sm.b[buf][kb + t][c0 + nb * 8]);
+            b[nb][1] = __float_as_uint(sm.b[buf][kb + t + 4][c0 + nb * 8]);
+        }
+#pragma unroll
+        for (int mb = 0; mb < 2; ++mb)
+#pragma unroll
+            for (int nb = 0; nb < 4; ++nb) tmma(&acc[(mb * 4 + nb) * 4], a[mb], b[nb]);
+    }
 }
 
 // acc += A(warp rows, chunk) B(chunk, warp columns) over one staged chunk.
@@ -484,6 +551,16 @@ __device__ __forceinline__ void load_b_chunk(WideSmem& sm, int buf, const double
     }
 }
 
+__device__ __forceinline__ void load_b_chunk(WideSmemT<float>& sm, int buf, const float* Bp, int ldb,
+                                             int len, int cols, int tid) {
+#pragma unroll
+    for (int e = tid; e < KC * WT; e += WTHREADS) {
+        const int p = e % KC, c = e / KC;
+        const bool v = p < len && c < cols;
+        cp_async4(&sm.b[buf][p][c], v ? Bp + p + (long long)c * ldb : Bp, v);
+    }
+}
+
 // The wide kernels stream a sequence of KC-chunks: phase 1 the chunks of
 // every W1 tile (its nin input rows), phase 2 the chunks of every row tile's
 // entries (no chunk spans two entries), over all jobs.  A persistent CTA takes
@@ -501,11 +578,14 @@ __device__ __forceinline__ int tiles_of(const JobExec& J) { return PHASE == 1 ? 
 template <int PHASE>
 __device__ __forceinline__ const int* chunk_prefix(const JobExec& J) { return PHASE == 1 ? J.w1cp : J.tcp; }
 
-template <int PHASE>
+// TF: the TF32 form (FP32 copy of the blocks and of the input, TF32
+// tensor-core MMA, FP32 accumulation, FP64 output).
+template <int PHASE, bool TF>
 __global__ void __launch_bounds__(WTHREADS)
 wide_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0, long long C, int G) {
+    using E = typename std::conditional<TF, float, double>::type;
     extern __shared__ __align__(16) unsigned char wide_smem[];
-    WideSmem& sm = *reinterpret_cast<WideSmem*>(wide_smem);
+    WideSmemT<E>& sm = *reinterpret_cast<WideSmemT<E>*>(wide_smem);
     __shared__ int last_flag;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int b = blockIdx.x, y = blockIdx.y;
@@ -556,39 +636,61 @@ wide_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0, lon
             for (int e = tid; e < WT * KC; e += WTHREADS) {
                 const int p = e % KC, i = e / KC;   // W columns are contiguous
                 const bool v = p < len && i < rows;
-                const double* w0 = J.hb + t->wcol[v ? i : 0];
-                cp_async8(&sm.a[buf][p][i], v ? w0 + c.pos + p : w0, v);
+                const long long wo = t->wcol[v ? i : 0];
+                if constexpr (TF) {
+                    const float* w0 = J.hb32 + wo;
+                    cp_async4(&sm.a[buf][p][i], v ? w0 + c.pos + p : w0, v);
+                } else {
+                    const double* w0 = J.hb + wo;
+                    cp_async8(&sm.a[buf][p][i], v ? w0 + c.pos + p : w0, v);
+                }
             }
-            load_b_chunk(sm, buf, J.in + t->in_off + c.pos + (long long)y * WT * J.ldin, J.ldin,
-                         len, cols, tid);
+            if constexpr (TF)
+                load_b_chunk(sm, buf, J.in32 + t->in_off + c.pos + (long long)y * WT * J.ldin32,
+                             J.ldin32, len, cols, tid);
+            else
+                load_b_chunk(sm, buf, J.in + t->in_off + c.pos + (long long)y * WT * J.ldin,
+                             J.ldin, len, cols, tid);
             c.pos += len;
             last = c.pos >= t->nin;
         } else {
             const P2T it = J.p2[c.tile];
             const P2Entry e = J.ent[c.ei];
             const int len = min(KC, e.inner - c.pos);
-            const double* E = J.hb + e.a;
+            const E* Eb;
+            if constexpr (TF) Eb = J.hb32 + e.a;
+            else Eb = J.hb + e.a;
             if (!e.transA) {
-                const double* A = E + it.r0 + (long long)c.pos * e.lda;
+                const E* A = Eb + it.r0 + (long long)c.pos * e.lda;
 #pragma unroll
                 for (int x = tid; x < WT * KC; x += WTHREADS) {
                     const int i = x % WT, p = x / WT;   // rows contiguous
                     const bool v = p < len && i < it.rows;
-                    cp_async8(&sm.a[buf][p][i], v ? A + i + (long long)p * e.lda : E, v);
+                    if constexpr (TF) cp_async4(&sm.a[buf][p][i], v ? A + i + (long long)p * e.lda : Eb, v);
+                    else cp_async8(&sm.a[buf][p][i], v ? A + i + (long long)p * e.lda : Eb, v);
                 }
             } else {
-                const double* A = E + c.pos + (long long)it.r0 * e.lda;
+                const E* A = Eb + c.pos + (long long)it.r0 * e.lda;
 #pragma unroll
                 for (int x = tid; x < WT * KC; x += WTHREADS) {
                     const int p = x % KC, i = x / KC;   // inner index contiguous
                     const bool v = p < len && i < it.rows;
-                    cp_async8(&sm.a[buf][p][i], v ? A + p + (long long)i * e.lda : E, v);
+                    if constexpr (TF) cp_async4(&sm.a[buf][p][i], v ? A + p + (long long)i * e.lda : Eb, v);
+                    else cp_async8(&sm.a[buf][p][i], v ? A + p + (long long)i * e.lda : Eb, v);
                 }
             }
-            const double* EB;
-            int ldb;
-            entry_b(e, J, EB, ldb);
-            load_b_chunk(sm, buf, EB + c.pos + (long long)y * WT * ldb, ldb, len, cols, tid);
+            if constexpr (TF) {
+                const float* EB;
+                int ldb;
+                if (e.b_from_t) { EB = J.T32 + e.b_off * J.k; ldb = e.ldt; }
+                else { EB = J.in32 + e.b_off; ldb = J.ldin32; }
+                load_b_chunk(sm, buf, EB + c.pos + (long long)y * WT * ldb, ldb, len, cols, tid);
+            } else {
+                const double* EB;
+                int ldb;
+                entry_b(e, J, EB, ldb);
+                load_b_chunk(sm, buf, EB + c.pos + (long long)y * WT * ldb, ldb, len, cols, tid);
+            }
             c.pos += len;
             last = false;
             if (c.pos >= e.inner) {
@@ -615,9 +717,11 @@ wide_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0, lon
         }
         return last;
     };
-    double acc[32];
+    E acc[32];
 #pragma unroll
-    for (int q = 0; q < 32; ++q) acc[q] = 0.0;
+    for (int q = 0; q < 32; ++q) acc[q] = 0;
+    auto arow = [&](int k) { return TF ? acc_row_tf(k, warp, lane) : acc_row(k, warp, lane); };
+    auto acol = [&](int k) { return TF ? acc_col_tf(k, warp, lane) : acc_col(k, warp, lane); };
     // NSTAGE-deep ring: chunk q sits in buffer q % NSTAGE and is issued
     // NSTAGE - 1 chunks ahead; one commit group per chunk slot (empty past
     // the end) keeps the wait count constant
@@ -646,7 +750,8 @@ wide_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0, lon
         cp_async_wait<NSTAGE - 1>();
         __syncthreads();
         const int buf = (int)(q % NSTAGE);
-        wide_mma(sm, buf, warp, lane, acc);
+        if constexpr (TF) wide_mma_tf(sm, buf, warp, lane, acc);
+        else wide_mma(sm, buf, warp, lane, acc);
         __syncthreads();
         if (!lastc[buf] && q + 1 < n) continue;
         // flush the tile of this chunk
@@ -668,22 +773,25 @@ wide_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0, lon
             rows = it.rows;
         }
         auto emit = [&](int i, int c, double v) {
-            if (PHASE == 1)
-                J.T[wt->trel[i] * J.k + wt->tj[i] + (long long)(y * WT + c) * wt->tr[i]] = v;
-            else
+            if (PHASE == 1) {
+                const long long o = wt->trel[i] * J.k + wt->tj[i] + (long long)(y * WT + c) * wt->tr[i];
+                if constexpr (TF) J.T32[o] = round_tf32(v);
+                else J.T[o] = v;
+            } else {
                 store_out(J, it, i, y * WT + c, v);
+            }
         };
         if (whole) {
 #pragma unroll
             for (int k = 0; k < 32; ++k) {
-                const int i = acc_row(k, warp, lane), c = acc_col(k, warp, lane);
-                if (i < rows && c < cols) emit(i, c, acc[k]);
+                const int i = arow(k), c = acol(k);
+                if (i < rows && c < cols) emit(i, c, (double)acc[k]);
             }
         } else {
             double* part = J.part + ((long long)y * 2 * G) * (WT * WT);
             double* mine = part + (2LL * b + (first_piece ? 0 : 1)) * (WT * WT);
 #pragma unroll
-            for (int k = 0; k < 32; ++k) mine[acc_row(k, warp, lane) + WT * acc_col(k, warp, lane)] = acc[k];
+            for (int k = 0; k < 32; ++k) mine[arow(k) + WT * acol(k)] = (double)acc[k];
             __threadfence();
             __syncthreads();
             const long long wa = split_owner(T0, G, C), wb = split_owner(T1 - 1, G, C);
@@ -705,7 +813,7 @@ wide_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0, lon
             __syncthreads();
         }
 #pragma unroll
-        for (int k = 0; k < 32; ++k) acc[k] = 0.0;
+        for (int k = 0; k < 32; ++k) acc[k] = 0;
         first_piece = false;
     }
 }
@@ -1066,6 +1174,57 @@ void launch_narrow(Context& ctx, const JobExec* jobs_d, int nj, const JobExec& j
     }
 }
 
+// Inputs of TF32 products: X (n x k, ld ldx, FP64) -> Xf (n x k, ld n,
+// FP32 rounded to TF32), one launch for all distinct inputs (blockIdx.y).
+struct InConv {
+    const double* src;
+    float* dst;
+    long long ld, n, total;
+};
+
+__global__ void in_tf32_kernel(const InConv* __restrict__ cv) {
+    const InConv c = cv[blockIdx.y];
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < c.total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long i = e % c.n, j = e / c.n;
+        c.dst[e] = round_tf32(c.src[i + j * c.ld]);
+    }
+}
+
+template <bool TF>
+using WideElem = typename std::conditional<TF, float, double>::type;
+
+template <bool TF>
+void wide_grids(Context& ctx, long long c1, long long c2, int& G1, int& G2) {
+    constexpr size_t smem = sizeof(WideSmemT<WideElem<TF>>);
+    static std::once_flag attr_once;
+    std::call_once(attr_once, [] {
+        cudaFuncSetAttribute(wide_kernel<1, TF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(wide_kernel<2, TF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    });
+    G1 = (int)std::min<long long>(c1, persistent_grid_n(ctx, wide_kernel<1, TF>, WTHREADS, smem));
+    G2 = (int)std::min<long long>(c2, persistent_grid_n(ctx, wide_kernel<2, TF>, WTHREADS, smem));
+}
+
+template <bool TF>
+void launch_wide(Context& ctx, const JobExec* jobs_d, int nj, const JobExec& job0, long long n1,
+                 long long n2, int G1, int G2, int ct) {
+    constexpr size_t smem = sizeof(WideSmemT<WideElem<TF>>);
+    cudaStream_t st = ctx.stream;
+    if (n1 > 0 && G1 > 0) {
+        LaunchScope ls(ctx, TF ? "hmm_lowrank_inner_tf32" : "hmm_lowrank_inner");
+        wide_kernel<1, TF><<<dim3((unsigned)G1, (unsigned)ct), WTHREADS, smem, st>>>(jobs_d, nj, job0,
+                                                                                    n1, G1);
+        HMB_CHECK_LAUNCH();
+    }
+    if (n2 > 0 && G2 > 0) {
+        LaunchScope ls(ctx, TF ? "hmm_row_tiles_tf32" : "hmm_row_tiles");
+        wide_kernel<2, TF><<<dim3((unsigned)G2, (unsigned)ct), WTHREADS, smem, st>>>(jobs_d, nj, job0,
+                                                                                    n2, G2);
+        HMB_CHECK_LAUNCH();
+    }
+}
+
 }  // namespace
 
 int* Context::error_word() {
@@ -1086,7 +1245,7 @@ int* Context::zeroed_counters(long long n) {
     return counters.get();
 }
 
-void run_jobs(Context& ctx, const std::vector<MatJob>& jobs) {
+void run_jobs(Context& ctx, const std::vector<MatJob>& jobs, bool tf32) {
     if (jobs.empty()) return;
     cudaStream_t st = ctx.stream;
     std::vector<std::shared_ptr<JobTemplate>> tmpl;
@@ -1097,16 +1256,16 @@ void run_jobs(Context& ctx, const std::vector<MatJob>& jobs) {
         kmax = std::max(kmax, J.k);
     }
     // one vector, one job: stream the blocks (matvec.cu)
-    if (jobs.size() == 1 && jobs[0].k == 1 && multiply_vector_streamed(ctx, jobs[0])) return;
+    if (!tf32 && jobs.size() == 1 && jobs[0].k == 1 && multiply_vector_streamed(ctx, jobs[0])) return;
     // few columns: 32-row tiles, work split evenly over all resident warps;
-    // many columns: 64 x 64 FP64 tiles
+    // many columns: 64 x 64 tiles on the tensor cores (FP64, or TF32 when asked)
     const bool wide = kmax > 8;
+    tf32 = tf32 && wide;
     const int row_tile = wide ? 64 : 32;
     for (const MatJob& J : jobs) tmpl.push_back(get_template(ctx, *J.H, J.root, J.trans, row_tile));
     const int ct = ceil_div(std::max(kmax, 1), kWideTile);   // wide column tiles
-    long long t_total = 0, c_total = 0, p_total = 0;
-    std::vector<long long> t_off(jobs.size()), c1_off(jobs.size()), c2_off(jobs.size()),
-        p_off(jobs.size());
+    long long t_total = 0, c_total = 0;
+    std::vector<long long> t_off(jobs.size()), c1_off(jobs.size()), c2_off(jobs.size());
     for (size_t j = 0; j < jobs.size(); ++j) {
         const JobTemplate& T = *tmpl[j];
         t_off[j] = t_total;
@@ -1118,6 +1277,7 @@ void run_jobs(Context& ctx, const std::vector<MatJob>& jobs) {
     }
     // wide: persistent grids, 2 partial slots of 64 x 64 per CTA and column tile
     int G1 = 0, G2 = 0;
+    long long p_total = 0;
     if (wide) {
         long long c1 = 0, c2 = 0;
         for (size_t j = 0; j < jobs.size(); ++j)
@@ -1125,20 +1285,60 @@ void run_jobs(Context& ctx, const std::vector<MatJob>& jobs) {
                 c1 += tmpl[j]->wc1;
                 c2 += tmpl[j]->wc2;
             }
-        static std::once_flag attr_once;
-        std::call_once(attr_once, [] {
-            cudaFuncSetAttribute(wide_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)sizeof(WideSmem));
-            cudaFuncSetAttribute(wide_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)sizeof(WideSmem));
-        });
-        G1 = (int)std::min<long long>(c1, persistent_grid_n(ctx, wide_kernel<1>, WTHREADS, sizeof(WideSmem)));
-        G2 = (int)std::min<long long>(c2, persistent_grid_n(ctx, wide_kernel<2>, WTHREADS, sizeof(WideSmem)));
+        if (tf32) wide_grids<true>(ctx, c1, c2, G1, G2);
+        else wide_grids<false>(ctx, c1, c2, G1, G2);
         p_total = 2LL * std::max(G1, G2) * ct * kWideTile * kWideTile;
     }
-    (void)p_off;
+    // TF32: the blocks' FP32 copies, the inputs rounded once (inputs shared
+    // by several jobs converted once), an FP32 intermediate
     DeviceBuffer<double> tbuf;
-    tbuf.allocate((size_t)std::max<long long>(t_total + p_total, 1), st);
+    DeviceBuffer<float> tbuf32, inbuf32;
+    std::vector<const float*> in32(jobs.size(), nullptr);
+    std::vector<int> ldin32(jobs.size(), 0);
+    if (tf32) {
+        std::map<std::tuple<const double*, int, int, int>, long long> seen;
+        std::vector<InConv> conv;
+        std::vector<long long> conv_job(jobs.size(), -1), conv_off;
+        long long in_total = 0, maxconv = 0;
+        for (size_t j = 0; j < jobs.size(); ++j) {
+            const MatJob& J = jobs[j];
+            if (J.k == 0) continue;
+            ensure_tf32_copy(ctx, const_cast<HMatrix&>(*J.H));
+            const Block& R = J.H->S->blocks[J.root];
+            const int nin = J.trans ? R.m : R.n;
+            auto key = std::make_tuple(J.in, J.ldin, nin, J.k);
+            auto f = seen.find(key);
+            if (f == seen.end()) {
+                InConv c{};
+                c.src = J.in;
+                c.ld = J.ldin;
+                c.n = std::max(nin, 1);
+                c.total = (long long)nin * J.k;
+                f = seen.emplace(key, (long long)conv.size()).first;
+                conv.push_back(c);
+                conv_off.push_back(in_total);
+                in_total += std::max<long long>(c.total, 1);
+                maxconv = std::max(maxconv, c.total);
+            }
+            conv_job[j] = f->second;
+            ldin32[j] = std::max(nin, 1);
+        }
+        inbuf32.allocate((size_t)std::max<long long>(in_total, 1), st);
+        tbuf32.allocate((size_t)std::max<long long>(t_total, 1), st);
+        for (size_t c = 0; c < conv.size(); ++c) conv[c].dst = inbuf32.get() + conv_off[c];
+        for (size_t j = 0; j < jobs.size(); ++j)
+            if (conv_job[j] >= 0) in32[j] = conv[(size_t)conv_job[j]].dst;
+        HMB_REQUIRE(conv.size() < 65536, HM_ERR_UNSUPPORTED, "too many distinct inputs");
+        if (!conv.empty() && maxconv > 0) {
+            DeviceBuffer<InConv> dconv;
+            dconv.upload(conv, st);
+            const long long gx = std::min<long long>(ceil_div(maxconv, 256LL), 2LL * ctx.num_sms);
+            LaunchScope ls(ctx, "input_tf32");
+            in_tf32_kernel<<<dim3((unsigned)gx, (unsigned)conv.size()), 256, 0, st>>>(dconv.get());
+            HMB_CHECK_LAUNCH();
+        }
+    }
+    tbuf.allocate((size_t)std::max<long long>((tf32 ? 0 : t_total) + p_total, 1), st);
     int* cnt = ctx.zeroed_counters(std::max<long long>(c_total, 1));
     std::vector<JobExec> ex;
     ex.reserve(jobs.size());
@@ -1158,8 +1358,16 @@ void run_jobs(Context& ctx, const std::vector<MatJob>& jobs) {
         e.ent = T.ent.get();
         e.in = J.in;
         e.out = J.out;
-        e.T = tbuf.get() + t_off[j];
-        e.part = tbuf.get() + t_total;
+        if (tf32) {
+            e.hb32 = J.H->data32.get();
+            e.in32 = in32[j];
+            e.ldin32 = ldin32[j];
+            e.T32 = tbuf32.get() + t_off[j];
+            e.part = tbuf.get();
+        } else {
+            e.T = tbuf.get() + t_off[j];
+            e.part = tbuf.get() + t_total;
+        }
         e.w1cp = T.w1cp.get();
         e.tcp = T.tcp.get();
         e.ekc = T.ekc.get();
@@ -1200,17 +1408,8 @@ void run_jobs(Context& ctx, const std::vector<MatJob>& jobs) {
         return;
     }
     HMB_REQUIRE(ct < 65536, HM_ERR_UNSUPPORTED, "too many columns");
-    const size_t wsm = sizeof(WideSmem);
-    if (n1 > 0 && G1 > 0) {
-        LaunchScope ls(ctx, "hmm_lowrank_inner");
-        wide_kernel<1><<<dim3((unsigned)G1, (unsigned)ct), WTHREADS, wsm, st>>>(jobs_d, nj, job0, n1, G1);
-        HMB_CHECK_LAUNCH();
-    }
-    if (n2 > 0 && G2 > 0) {
-        LaunchScope ls(ctx, "hmm_row_tiles");
-        wide_kernel<2><<<dim3((unsigned)G2, (unsigned)ct), WTHREADS, wsm, st>>>(jobs_d, nj, job0, n2, G2);
-        HMB_CHECK_LAUNCH();
-    }
+    if (tf32) launch_wide<true>(ctx, jobs_d, nj, job0, n1, n2, G1, G2, ct);
+    else launch_wide<false>(ctx, jobs_d, nj, job0, n1, n2, G1, G2, ct);
     // row tiles without entries: output = beta * output
     launch_zero_tiles(ctx, tmpl, jobs, jobs_d, job0);
 }

@@ -20,6 +20,8 @@
 // are translated to the FP32 copy by their offset in the H-matrix storage.
 #include <cuda_runtime.h>
 
+#include <utility>
+
 #include "engine.h"
 #include "templates.h"
 
@@ -364,17 +366,11 @@ void ensure_tf32_copy(Context& ctx, HMatrix& H) {
     H.shadow_valid = true;
 }
 
-void multiply_dense_tf32(HMatrix& H, double alpha, const double* B, int ldb, double beta,
-                         double* Cout, int ldc, int nrhs) {
-    Context& ctx = *H.ctx;
-    HMB_REQUIRE(nrhs >= 0 && nrhs <= kM, HM_ERR_UNSUPPORTED,
-                "the tensor-core product handles at most 64 right-hand sides per call");
-    HMB_REQUIRE(ldb >= std::max(1, H.width()) && ldc >= std::max(1, H.height()), HM_ERR_ARGUMENT,
-                "leading dimension too small");
-    if (nrhs == 0) return;
-    for (size_t b = 0; b < H.S->blocks.size(); ++b)
-        HMB_REQUIRE(H.S->blocks[b].kind != KIND_LOWRANK || H.rank[b] <= 256, HM_ERR_UNSUPPORTED,
-                    "tensor-core product supports ranks up to 256");
+namespace {
+
+// The tcgen05 form: nrhs <= 64, ranks <= 256; synchronizes.
+void dense_tf32_tc(Context& ctx, HMatrix& H, double alpha, const double* B, int ldb, double beta,
+                   double* Cout, int ldc, int nrhs) {
     ensure_tf32_copy(ctx, H);
     auto T = get_template(ctx, H, 0, false);
     const int n = H.width();
@@ -419,6 +415,93 @@ void multiply_dense_tf32(HMatrix& H, double alpha, const double* B, int ldb, dou
     HMB_CUDA(cudaMemcpyAsync(&h_err, err.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
     HMB_CUDA(cudaStreamSynchronize(st));
     HMB_REQUIRE(h_err == 0, HM_ERR_TIMEOUT, "a tensor-core wait ran out (no progress)");
+}
+
+// The mma.sync form: persistent 64 x 64 tiles over all right-hand sides.
+void dense_tf32_mma(Context& ctx, HMatrix& H, double alpha, const double* B, int ldb, double beta,
+                    double* Cout, int ldc, int nrhs) {
+    if (nrhs <= 8) {   // below the tile width the FP64 kernels are bandwidth-bound anyway
+        run_jobs(ctx, {MatJob{&H, 0, false, alpha, beta, B, ldb, Cout, ldc, nrhs}});
+    } else {
+        run_jobs(ctx, {MatJob{&H, 0, false, alpha, beta, B, ldb, Cout, ldc, nrhs}}, true);
+    }
+    HMB_CUDA(cudaStreamSynchronize(ctx.stream));
+}
+
+// Right-hand-side bucket of the tuning table: 16, 32, 64, 128, ...
+int rhs_bucket(int nrhs) {
+    int b = 16;
+    while (b < nrhs) b *= 2;
+    return b;
+}
+
+// Times both forms on the matrix into a scratch output (beta = 0, three
+// runs each after one untimed run) and returns the faster (1 tcgen05,
+// 2 mma.sync).
+int tune_tf32(Context& ctx, HMatrix& H, const double* B, int ldb, int nrhs) {
+    HostScope hs(ctx, "tf32_autotune");
+    const int m = H.height();
+    DeviceBuffer<double> scratch;
+    scratch.allocate((size_t)std::max(m, 1) * nrhs, ctx.stream);
+    cudaEvent_t e0, e1;
+    HMB_CUDA(cudaEventCreate(&e0));
+    HMB_CUDA(cudaEventCreate(&e1));
+    float best_ms = 0.0f;
+    int best = 2;
+    for (int which = 1; which <= 2; ++which) {
+        auto run = [&] {
+            if (which == 1) dense_tf32_tc(ctx, H, 1.0, B, ldb, 0.0, scratch.get(), std::max(m, 1), nrhs);
+            else dense_tf32_mma(ctx, H, 1.0, B, ldb, 0.0, scratch.get(), std::max(m, 1), nrhs);
+        };
+        run();
+        HMB_CUDA(cudaEventRecord(e0, ctx.stream));
+        for (int r = 0; r < 3; ++r) run();
+        HMB_CUDA(cudaEventRecord(e1, ctx.stream));
+        HMB_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.0f;
+        HMB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (which == 1 || ms < best_ms) {
+            best_ms = ms;
+            best = which;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return best;
+}
+
+}  // namespace
+
+int tf32_kernel_choice(Context& ctx, HMatrix& H, const double* B, int ldb, int nrhs) {
+    bool tc_ok = nrhs <= kM;
+    for (size_t b = 0; tc_ok && b < H.S->blocks.size(); ++b)
+        tc_ok = H.S->blocks[b].kind != KIND_LOWRANK || H.rank[b] <= 256;
+    if (!tc_ok) return 2;
+    if (ctx.tf32_kernel != 0) return ctx.tf32_kernel;
+    get_template(ctx, H, 0, false);   // makes H.group
+    const auto key = std::make_pair(H.group->hash, rhs_bucket(nrhs));
+    auto f = ctx.tf32_tuned.find(key);
+    if (f != ctx.tf32_tuned.end()) return f->second;
+    const int w = tune_tf32(ctx, H, B, ldb, nrhs);
+    ctx.tf32_tuned[key] = w;
+    return w;
+}
+
+void multiply_dense_tf32(HMatrix& H, double alpha, const double* B, int ldb, double beta,
+                         double* Cout, int ldc, int nrhs) {
+    Context& ctx = *H.ctx;
+    HMB_REQUIRE(nrhs >= 0, HM_ERR_ARGUMENT, "nrhs must be >= 0");
+    HMB_REQUIRE(ldb >= std::max(1, H.width()) && ldc >= std::max(1, H.height()), HM_ERR_ARGUMENT,
+                "leading dimension too small");
+    if (nrhs == 0 || H.height() == 0) return;
+    const int which = tf32_kernel_choice(ctx, H, B, ldb, nrhs);
+    if (which == 1) {
+        HMB_REQUIRE(nrhs <= kM, HM_ERR_UNSUPPORTED,
+                    "the tcgen05 product handles at most 64 right-hand sides per call");
+        dense_tf32_tc(ctx, H, alpha, B, ldb, beta, Cout, ldc, nrhs);
+    } else {
+        dense_tf32_mma(ctx, H, alpha, B, ldb, beta, Cout, ldc, nrhs);
+    }
 }
 
 }  // namespace hmb

@@ -119,14 +119,22 @@ HM_API int hm_multiply_dense_host(hm_matrix h, int transpose, double alpha,
 
 /*
  * Mixed-precision form of hm_multiply_dense (no transpose): block data read
- * from an FP32 copy rounded to TF32 (made on first use), products on the
- * tensor cores (tcgen05.mma kind::tf32) with FP32 accumulation, C in FP64.
- * DEVICE pointers; nrhs <= 64 per call; synchronizes the stream.  Relative
- * error against the FP64 product is about 1e-3 (TF32 has an 11-bit
- * significand).  The reference computes only in the matrix's own precision.
+ * from an FP32 copy rounded to TF32 (made on first use), inputs rounded to
+ * TF32, products on the tensor cores with FP32 accumulation, C in FP64.
+ * DEVICE pointers; synchronizes the stream.  Relative error against the
+ * FP64 product is about 1e-3 (TF32 has an 11-bit significand).  The
+ * reference computes only in the matrix's own precision.
+ * Two kernel forms: 1 = tcgen05.mma kind::tf32 with tensor-memory
+ * accumulators (nrhs <= 64, ranks <= 256), 2 = persistent 64 x 64 tiles of
+ * mma.sync m16n8k8 TF32 (any nrhs; below 9 columns the FP64 kernels run).
+ * hm_set_tf32_kernel(ctx, 0) (the default) times both on the first product
+ * of each (layout, column bucket 16/32/64/...) and keeps the faster;
+ * hm_tf32_kernel_choice reports (and if need be tunes) the form used.
  */
 HM_API int hm_multiply_dense_tf32(hm_matrix h, double alpha, const double* B, int ldb,
                                   double beta, double* C, int ldc, int nrhs);
+HM_API int hm_set_tf32_kernel(hm_context ctx, int which);
+HM_API int hm_tf32_kernel_choice(hm_matrix h, const double* B, int ldb, int nrhs, int* which);
 
 /*
  * H*H products with randomized low-rank compression.

@@ -64,6 +64,8 @@ SIGNATURES = {
     "hm_multiply_hmat_update": [_P, _D, _P, _D, _P],
     "hm_estimate_two_norm": [_P, _D, _D, _PD],
     "hm_schulz_invert": [_P, _I, _D, _D, _D, _PI, _PD, _I, _PI],
+    "hm_schulz_invert_mixed": [_P, _I, _D, _D, _D, _D, _PI, _PI, _PD, _I, _PI],
+    "hm_set_low_precision": [_P, _I],
     "hm_copy": [_P, C.POINTER(_P)],
     "hm_transpose": [_P, C.POINTER(_P)],
     "hm_scale": [_P, _D],

@@ -500,6 +500,33 @@ int hm_schulz_invert(hm_matrix h, int num_iterations, double theta, double confi
     });
 }
 
+int hm_schulz_invert_mixed(hm_matrix h, int num_iterations, double theta, double confidence,
+                           double stop_tol, double mixed_switch, int* iterations,
+                           int* low_iterations, double* trace, int trace_cap, int* trace_len) {
+    return guarded([&] {
+        HMB_REQUIRE(h, HM_ERR_ARGUMENT, "h is NULL");
+        HMB_REQUIRE(h->h.height() == h->h.width(), HM_ERR_ARGUMENT,
+                    "Cannot invert non-square matrices");
+        HMB_REQUIRE(theta > 1.0, HM_ERR_ARGUMENT, "Theta must be > 1");
+        HMB_REQUIRE(confidence > 0.0, HM_ERR_ARGUMENT, "Confidence must be positive");
+        HMB_REQUIRE(mixed_switch >= 0.0, HM_ERR_ARGUMENT, "mixed_switch must be >= 0");
+        SchulzResult r = schulz_invert(owner_of(h)->c, h->h, num_iterations, theta, confidence,
+                                       stop_tol, mixed_switch);
+        if (iterations) *iterations = r.iterations;
+        if (low_iterations) *low_iterations = r.low_iterations;
+        if (trace_len) *trace_len = (int)r.trace.size();
+        if (trace)
+            for (int i = 0; i < trace_cap && i < (int)r.trace.size(); ++i) trace[i] = r.trace[i];
+    });
+}
+
+int hm_set_low_precision(hm_context ctx, int on) {
+    return guarded([&] {
+        HMB_REQUIRE(ctx, HM_ERR_ARGUMENT, "ctx is NULL");
+        ctx->c.low_precision = on != 0;
+    });
+}
+
 int hm_copy(hm_matrix src, hm_matrix* dst) {
     return guarded([&] {
         HMB_REQUIRE(src && dst, HM_ERR_ARGUMENT, "NULL argument");

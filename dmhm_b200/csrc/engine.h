@@ -72,6 +72,12 @@ struct Context {
     std::vector<std::shared_ptr<struct LayoutGroup>> layouts;
     // Symbolic H*H plans of recent products (hh.cu).
     std::shared_ptr<struct HHPlanCache> hh_cache;
+    // Low-precision phase: H*H products draw their range samples (B Omega,
+    // A (B Omega)) on the TF32 tensor cores and round their blocks in FP32
+    // (QR, core SVD); orthogonalisation of the samples, the projections and
+    // everything else stay FP64.  Set by mixed-precision Schulz for its
+    // early iterations, or by the caller for whole products.
+    bool low_precision = false;
     // Kernels of the TF32 dense product: 0 autotuned per (layout, column
     // bucket), 1 tcgen05 (at most 64 columns, ranks <= 256), 2 mma.sync.
     int tf32_kernel = 0;

@@ -760,7 +760,7 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
                 jobs.push_back({&B, t.b, false, t.alpha, 0.0, S0 + t.s_omega, Bb.n, S0 + t.s_x,
                                 Bb.m, t.k});
             }
-            run_jobs(ctx, jobs);
+            run_jobs(ctx, jobs, ctx.low_precision);
         }
         // Y = A X
         {
@@ -770,7 +770,7 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
                 const Block& Ba = S.blocks[t.a];
                 jobs.push_back({&A, t.a, false, 1.0, 0.0, S0 + t.s_x, Ba.n, S0 + t.s_y, Ba.m, t.k});
             }
-            run_jobs(ctx, jobs);
+            run_jobs(ctx, jobs, ctx.low_precision);
         }
         // Q = orth(Y)
         {

@@ -13,6 +13,12 @@
 // reflectors applied back.  The truncated result is the same best rank-r
 // approximation the reference computes (its factors differ only by the
 // usual sign / rotation freedom of an SVD).
+//
+// Every device routine is written for an arithmetic type R: double (the
+// reference's precision) or float, the low-precision form used by the early
+// iterations of a mixed-precision Schulz run (inputs and outputs stay FP64;
+// stacks, reflectors, core and rotations are FP32 in the work area and in
+// shared memory).
 #include "lowrank.h"
 
 #include <algorithm>
@@ -24,26 +30,51 @@ namespace {
 constexpr int kT = 256;
 constexpr int kW = kT / 32;
 constexpr int kMaxK = 128;         // largest stacked rank handled
-constexpr long long kSmemDoubles = 8192;   // 64 KB: M and J up to 64 x 64
+constexpr long long kSmemBytes = 65536;   // M and J up to 64 x 64 FP64
 constexpr int kJacobiSweeps = 40;  // bounded; converges in ~6-12
-constexpr double kJacobiTol = 1e-15;
 
-__device__ __forceinline__ double warp_sum(double v) {
+// Per-precision constants: Jacobi's orthogonality threshold (relative to the
+// column norms), the squared-norm level below which a column counts as
+// rounding noise (relative to ||M||_F^2), and the smallest resolvable
+// relative truncation tolerance.
+template <typename R> struct Prec;
+template <> struct Prec<double> {
+    static constexpr double jtol = 1e-15, tiny = 1e-32, tol_floor = 0.0;
+};
+template <> struct Prec<float> {
+    static constexpr float jtol = 1e-6f, tiny = 1e-12f;
+    static constexpr double tol_floor = 1e-6;
+};
+
+__device__ __forceinline__ double r_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float r_sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double r_rsqrt(double x) { return rsqrt(x); }
+__device__ __forceinline__ float r_rsqrt(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double r_fma(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float r_fma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double r_abs(double x) { return fabs(x); }
+__device__ __forceinline__ float r_abs(float x) { return fabsf(x); }
+__device__ __forceinline__ double r_copysign(double a, double b) { return copysign(a, b); }
+__device__ __forceinline__ float r_copysign(float a, float b) { return copysignf(a, b); }
+
+template <typename R>
+__device__ __forceinline__ R warp_sum(R v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
 
-__device__ double block_sum(double v, double* red) {
+template <typename R>
+__device__ R block_sum(R v, R* red) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     v = warp_sum(v);
     if (lane == 0) red[warp] = v;
     __syncthreads();
-    double t = threadIdx.x < kW ? red[threadIdx.x] : 0.0;
+    R t = threadIdx.x < kW ? red[threadIdx.x] : R(0);
     if (warp == 0) t = warp_sum(t);
     if (threadIdx.x == 0) red[kW] = t;
     __syncthreads();
-    double r = red[kW];
+    R r = red[kW];
     __syncthreads();
     return r;
 }
@@ -51,21 +82,22 @@ __device__ double block_sum(double v, double* red) {
 // In-place Householder QR (LAPACK dgeqr2 conventions: beta = -sign(alpha)
 // ||x||, v(1) = 1 implicit, tau = (beta - alpha) / beta; tau = 0 when the
 // column below the diagonal is zero).
-__device__ void cta_qr(double* A, int m, int n, int ld, double* tau, double* red) {
+template <typename R>
+__device__ void cta_qr(R* A, int m, int n, int ld, R* tau, R* red) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int kk = min(m, n);
     for (int j = 0; j < kk; ++j) {
-        double* col = A + j + (long long)j * ld;
+        R* col = A + j + (long long)j * ld;
         const int len = m - j;
-        double s = 0.0;
+        R s = 0;
         for (int i = 1 + threadIdx.x; i < len; i += kT) s += col[i] * col[i];
         s = block_sum(s, red);
-        const double alpha = col[0];
-        double t = 0.0, beta = alpha;
-        if (s != 0.0) {
-            beta = -copysign(sqrt(alpha * alpha + s), alpha);
+        const R alpha = col[0];
+        R t = 0, beta = alpha;
+        if (s != R(0)) {
+            beta = -r_copysign(r_sqrt(alpha * alpha + s), alpha);
             t = (beta - alpha) / beta;
-            const double scal = 1.0 / (alpha - beta);
+            const R scal = R(1) / (alpha - beta);
             for (int i = 1 + threadIdx.x; i < len; i += kT) col[i] *= scal;
         }
         __syncthreads();
@@ -74,14 +106,14 @@ __device__ void cta_qr(double* A, int m, int n, int ld, double* tau, double* red
             tau[j] = t;
         }
         __syncthreads();
-        if (t != 0.0) {
+        if (t != R(0)) {
             for (int c = j + 1 + warp; c < n; c += kW) {
-                double* cc = A + j + (long long)c * ld;
-                const double c0 = cc[0];
-                double w = 0.0;
+                R* cc = A + j + (long long)c * ld;
+                const R c0 = cc[0];
+                R w = 0;
                 for (int i = 1 + lane; i < len; i += 32) w += col[i] * cc[i];
                 w = warp_sum(w) + c0;
-                const double tw = t * w;
+                const R tw = t * w;
                 __syncwarp();
                 if (lane == 0) cc[0] = c0 - tw;
                 for (int i = 1 + lane; i < len; i += 32) cc[i] -= tw * col[i];
@@ -92,24 +124,26 @@ __device__ void cta_qr(double* A, int m, int n, int ld, double* tau, double* red
 }
 
 // B := Q B with Q = H_0 H_1 ... H_{kk-1} from cta_qr (B is m x p).
-__device__ void cta_apply_q(const double* A, int m, int kk, int lda, const double* tau,
-                            double* B, int p, int ldb) {
+// (arithmetic in R; B may be stored in another type)
+template <typename R, typename RB>
+__device__ void cta_apply_q(const R* A, int m, int kk, int lda, const R* tau, RB* B, int p,
+                            int ldb) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int j = kk - 1; j >= 0; --j) {
-        const double t = tau[j];
-        if (t == 0.0) continue;
-        const double* v = A + j + (long long)j * lda;
+        const R t = tau[j];
+        if (t == R(0)) continue;
+        const R* v = A + j + (long long)j * lda;
         const int len = m - j;
         for (int c = warp; c < p; c += kW) {
-            double* bc = B + j + (long long)c * ldb;
-            const double b0 = bc[0];
-            double w = 0.0;
-            for (int i = 1 + lane; i < len; i += 32) w += v[i] * bc[i];
+            RB* bc = B + j + (long long)c * ldb;
+            const R b0 = (R)bc[0];
+            R w = 0;
+            for (int i = 1 + lane; i < len; i += 32) w += v[i] * (R)bc[i];
             w = warp_sum(w) + b0;
-            const double tw = t * w;
+            const R tw = t * w;
             __syncwarp();
-            if (lane == 0) bc[0] = b0 - tw;
-            for (int i = 1 + lane; i < len; i += 32) bc[i] -= tw * v[i];
+            if (lane == 0) bc[0] = (RB)(b0 - tw);
+            for (int i = 1 + lane; i < len; i += 32) bc[i] = (RB)((R)bc[i] - tw * v[i]);
         }
         __syncthreads();
     }
@@ -127,15 +161,15 @@ __device__ __forceinline__ int rr_pos(int i, int step, int n) {
 // the squared Frobenius norm of M) are left alone: rotating noise against
 // noise never settles, and such columns carry no singular value above
 // rounding level.
-__device__ void cta_jacobi(double* M, int rows, int cols, double* J, int* flag, double* red,
-                           double* nrm) {
+template <typename R>
+__device__ void cta_jacobi(R* M, int rows, int cols, R* J, int* flag, R* red, R* nrm) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int e = threadIdx.x; e < cols * cols; e += kT)
-        J[e] = (e % cols == e / cols) ? 1.0 : 0.0;
-    double fro = 0.0;
-    for (long long e = threadIdx.x; e < (long long)rows * cols; e += kT) fro = fma(M[e], M[e], fro);
+        J[e] = (e % cols == e / cols) ? R(1) : R(0);
+    R fro = 0;
+    for (long long e = threadIdx.x; e < (long long)rows * cols; e += kT) fro = r_fma(M[e], M[e], fro);
     fro = block_sum(fro, red);
-    const double tiny = 1e-32 * fro;
+    const R tiny = R(Prec<R>::tiny) * fro;
     __syncthreads();
     if (cols < 2) return;
     const int n = cols + (cols & 1);
@@ -146,9 +180,9 @@ __device__ void cta_jacobi(double* M, int rows, int cols, double* J, int* flag, 
     const int hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
     for (int sweep = 0; sweep < kJacobiSweeps; ++sweep) {
         for (int c = warp; c < cols; c += kW) {
-            const double* g = M + (long long)c * rows;
-            double sq = 0.0;
-            for (int i = lane; i < rows; i += 32) sq = fma(g[i], g[i], sq);
+            const R* g = M + (long long)c * rows;
+            R sq = 0;
+            for (int i = lane; i < rows; i += 32) sq = r_fma(g[i], g[i], sq);
             sq = warp_sum(sq);
             if (lane == 0) nrm[c] = sq;
         }
@@ -166,38 +200,38 @@ __device__ void cta_jacobi(double* M, int rows, int cols, double* J, int* flag, 
                 }
                 const bool live = k < n / 2 && p < cols && q < cols;
                 if (p > q) { int t = p; p = q; q = t; }
-                double* gp = M + (long long)p * rows;
-                double* gq = M + (long long)q * rows;
-                double c = 0.0;
+                R* gp = M + (long long)p * rows;
+                R* gq = M + (long long)q * rows;
+                R c = 0;
                 if (live)
-                    for (int i = hl; i < rows; i += 16) c = fma(gp[i], gq[i], c);
+                    for (int i = hl; i < rows; i += 16) c = r_fma(gp[i], gq[i], c);
 #pragma unroll
                 for (int o = 8; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-                const double a = live ? nrm[p] : 0.0, b = live ? nrm[q] : 0.0;
-                if (live && c != 0.0 && a > tiny && b > tiny &&
-                    c * c > (kJacobiTol * kJacobiTol) * (a * b)) {
+                const R a = live ? nrm[p] : R(0), b = live ? nrm[q] : R(0);
+                constexpr R jt2 = Prec<R>::jtol * Prec<R>::jtol;
+                if (live && c != R(0) && a > tiny && b > tiny && c * c > jt2 * (a * b)) {
                     // t = tan of the rotation angle, the smaller root of
                     // t^2 + 2 zeta t - 1 = 0 with zeta = (b - a) / (2c),
                     // written as 2|c| / (|b - a| + sqrt((b - a)^2 + 4c^2))
-                    const double d = b - a;
-                    const double t = copysign(2.0 * fabs(c), d * c) /
-                                     (fabs(d) + sqrt(fma(d, d, 4.0 * c * c)));
-                    const double cs = rsqrt(fma(t, t, 1.0)), sn = cs * t;
+                    const R d = b - a;
+                    const R t = r_copysign(R(2) * r_abs(c), d * c) /
+                                (r_abs(d) + r_sqrt(r_fma(d, d, R(4) * c * c)));
+                    const R cs = r_rsqrt(r_fma(t, t, R(1))), sn = cs * t;
                     for (int i = hl; i < rows; i += 16) {
-                        const double x = gp[i], y = gq[i];
+                        const R x = gp[i], y = gq[i];
                         gp[i] = cs * x - sn * y;
                         gq[i] = sn * x + cs * y;
                     }
-                    double* jp = J + (long long)p * cols;
-                    double* jq = J + (long long)q * cols;
+                    R* jp = J + (long long)p * cols;
+                    R* jq = J + (long long)q * cols;
                     for (int i = hl; i < cols; i += 16) {
-                        const double x = jp[i], y = jq[i];
+                        const R x = jp[i], y = jq[i];
                         jp[i] = cs * x - sn * y;
                         jq[i] = sn * x + cs * y;
                     }
                     if (hl == 0) {
-                        nrm[p] = fma(-t, c, a);
-                        nrm[q] = fma(t, c, b);
+                        nrm[p] = r_fma(-t, c, a);
+                        nrm[q] = r_fma(t, c, b);
                         *flag = 1;
                     }
                 }
@@ -211,22 +245,22 @@ __device__ void cta_jacobi(double* M, int rows, int cols, double* J, int* flag, 
 }
 
 // order[0..cols) = column indices of M by decreasing norm (ties by index).
-__device__ void cta_order_columns(const double* M, int rows, int cols, double* norms,
-                                  int* order) {
+template <typename R>
+__device__ void cta_order_columns(const R* M, int rows, int cols, R* norms, int* order) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int c = warp; c < cols; c += kW) {
-        const double* g = M + (long long)c * rows;
-        double s = 0.0;
-        for (int i = lane; i < rows; i += 32) s = fma(g[i], g[i], s);
+        const R* g = M + (long long)c * rows;
+        R s = 0;
+        for (int i = lane; i < rows; i += 32) s = r_fma(g[i], g[i], s);
         s = warp_sum(s);
         if (lane == 0) norms[c] = s;
     }
     __syncthreads();
     for (int j = threadIdx.x; j < cols; j += kT) {
-        const double sj = norms[j];
+        const R sj = norms[j];
         int pos = 0;
         for (int i = 0; i < cols; ++i) {
-            const double si = norms[i];
+            const R si = norms[i];
             pos += (si > sj || (si == sj && i < j)) ? 1 : 0;
         }
         order[pos] = j;
@@ -234,20 +268,21 @@ __device__ void cta_order_columns(const double* M, int rows, int cols, double* n
     __syncthreads();
 }
 
+template <typename R>
 struct RoundShared {
-    double red[kW + 1];
-    double norms[kMaxK];
-    double nrm[kMaxK];    // Jacobi's running squared column norms
+    R red[kW + 1];
+    R norms[kMaxK];
+    R nrm[kMaxK];    // Jacobi's running squared column norms
     int order[kMaxK];
     int flag;
 };
 
 // One rounding operation, executed by the whole CTA.  `dyn` holds the core
-// and the rotations in shared memory when they fit in `smem_doubles` doubles.
-__device__ void do_round(const RoundOp& op_in, double* dyn, long long smem_doubles,
-                         RoundShared& sh) {
-    double* red = sh.red;
-    double* norms = sh.norms;
+// and the rotations in shared memory when they fit in `smem_elems` elements.
+template <typename R>
+__device__ void do_round(const RoundOp& op_in, R* dyn, long long smem_elems, RoundShared<R>& sh) {
+    R* red = sh.red;
+    R* norms = sh.norms;
     int* order = sh.order;
     RoundOp op = op_in;
     if (op.r1_dev) op.r1 = min(op.r1, *op.r1_dev);
@@ -283,20 +318,20 @@ __device__ void do_round(const RoundOp& op_in, double* dyn, long long smem_doubl
     const int ku = ortho ? op.r1 : min(m, k);
     const int kv = dense ? n : min(n, k);
     // The core and the rotations live in shared memory when they fit in
-    // `smem_doubles`; the stacked factors in the (L1-cached) work area.
+    // `smem_elems`; the stacked factors in the (L1-cached) work area.
     const long long need_mj = (long long)ku * kv + (long long)kv * kv;
-    const bool mj_smem = need_mj <= smem_doubles;
-    double* w = op.work;
-    double* Ucat = w;
+    const bool mj_smem = need_mj <= smem_elems;
+    R* w = reinterpret_cast<R*>(op.work);
+    R* Ucat = w;
     if (!ortho) w += (long long)m * k;
-    double* Vcat = w;
+    R* Vcat = w;
     if (!dense) w += (long long)n * k;
-    double* tauU = w;
+    R* tauU = w;
     w += k;
-    double* tauV = w;
+    R* tauV = w;
     w += k;
-    double* M;
-    double* J;
+    R* M;
+    R* J;
     if (mj_smem) {
         M = dyn;
         J = dyn + (long long)ku * kv;
@@ -314,13 +349,13 @@ __device__ void do_round(const RoundOp& op_in, double* dyn, long long smem_doubl
         const int r2 = op.r2;
         for (long long e = tid; e < (long long)m * k; e += kT) {
             int i = (int)(e % m), c = (int)(e / m);
-            Ucat[e] = c < r2 ? op.beta * op.u2[i + (long long)c * op.ldu2]
-                             : op.alpha * op.u1[i + (long long)(c - r2) * op.ldu1];
+            Ucat[e] = (R)(c < r2 ? op.beta * op.u2[i + (long long)c * op.ldu2]
+                                 : op.alpha * op.u1[i + (long long)(c - r2) * op.ldu1]);
         }
         for (long long e = tid; e < (long long)n * k; e += kT) {
             int i = (int)(e % n), c = (int)(e / n);
-            Vcat[e] = c < r2 ? op.v2[i + (long long)c * op.ldv2]
-                             : op.v1[i + (long long)(c - r2) * op.ldv1];
+            Vcat[e] = (R)(c < r2 ? op.v2[i + (long long)c * op.ldv2]
+                                 : op.v1[i + (long long)(c - r2) * op.ldv1]);
         }
     } else if (dense) {
         for (long long e = tid; e < (long long)m * n; e += kT) {
@@ -330,12 +365,12 @@ __device__ void do_round(const RoundOp& op_in, double* dyn, long long smem_doubl
                 for (int l = 0; l < op.r2; ++l)
                     v = fma(op.beta * op.u2[i + (long long)l * op.ldu2],
                             op.v2[c + (long long)l * op.ldv2], v);
-            Ucat[e] = v;
+            Ucat[e] = (R)v;
         }
     } else {  // ortho: Q1 is used in place; Z is copied
         for (long long e = tid; e < (long long)n * k; e += kT) {
             int i = (int)(e % n), c = (int)(e / n);
-            Vcat[e] = op.v1[i + (long long)c * op.ldv1];
+            Vcat[e] = (R)op.v1[i + (long long)c * op.ldv1];
         }
     }
     __syncthreads();
@@ -347,14 +382,14 @@ __device__ void do_round(const RoundOp& op_in, double* dyn, long long smem_doubl
     // ---- core M = R_u R_v^T (ku x kv) -------------------------------------
     for (int e = tid; e < ku * kv; e += kT) {
         const int i = e % ku, l = e / ku;
-        double v = 0.0;
+        R v = 0;
         if (ortho) {
-            v = (i >= l) ? Vcat[l + (long long)i * n] : 0.0;      // R_v^T
+            v = (i >= l) ? Vcat[l + (long long)i * n] : R(0);     // R_v^T
         } else if (dense) {
-            v = (l >= i) ? Ucat[i + (long long)l * m] : 0.0;      // R_u (ku x n)
+            v = (l >= i) ? Ucat[i + (long long)l * m] : R(0);     // R_u (ku x n)
         } else {
             for (int p = max(i, l); p < k; ++p)
-                v = fma(Ucat[i + (long long)p * m], Vcat[l + (long long)p * n], v);
+                v = r_fma(Ucat[i + (long long)p * m], Vcat[l + (long long)p * n], v);
         }
         M[i + (long long)l * ku] = v;
     }
@@ -366,14 +401,16 @@ __device__ void do_round(const RoundOp& op_in, double* dyn, long long smem_doubl
 
     // ---- outputs -------------------------------------------------------------
     // columns kept: at most rout and the core's size; with a tolerance, the
-    // singular values above tol * sigma_0 (norms holds squared values)
+    // singular values above tol * sigma_0 (norms holds squared values); in
+    // FP32 the tolerance is at least the precision's resolvable level
     int keep = min(rout, min(ku, kv));
     if (op.tol > 0.0 && keep > 0) {
         const double s0 = norms[order[0]];
-        const double t2 = op.tol * op.tol;
+        const double tol = op.tol > Prec<R>::tol_floor ? op.tol : Prec<R>::tol_floor;
+        const double t2 = tol * tol;
         int c = 0;
         if (s0 >= t2 * t2)
-            while (c < keep && norms[order[c]] > t2 * s0) ++c;
+            while (c < keep && (double)norms[order[c]] > t2 * s0) ++c;
         keep = c;
     }
     if (tid == 0 && op.rank_out) *op.rank_out = keep;
@@ -382,20 +419,20 @@ __device__ void do_round(const RoundOp& op_in, double* dyn, long long smem_doubl
             int i = (int)(e % m), c = (int)(e / m);
             double v = 0.0;
             if (c < keep) {
-                const double* g = M + (long long)order[c] * ku;
-                for (int p = 0; p < ku; ++p) v = fma(op.u1[i + (long long)p * op.ldu1], g[p], v);
+                const R* g = M + (long long)order[c] * ku;
+                for (int p = 0; p < ku; ++p) v = fma(op.u1[i + (long long)p * op.ldu1], (double)g[p], v);
             }
             op.uo[e] = v;
         }
     } else {
         for (long long e = tid; e < (long long)m * rout; e += kT) {
             int i = (int)(e % m), c = (int)(e / m);
-            op.uo[e] = (i < ku && c < keep) ? M[i + (long long)order[c] * ku] : 0.0;
+            op.uo[e] = (i < ku && c < keep) ? (double)M[i + (long long)order[c] * ku] : 0.0;
         }
     }
     for (long long e = tid; e < (long long)n * rout; e += kT) {
         int i = (int)(e % n), c = (int)(e / n);
-        op.vo[e] = (i < kv && c < keep) ? J[i + (long long)order[c] * kv] : 0.0;
+        op.vo[e] = (i < kv && c < keep) ? (double)J[i + (long long)order[c] * kv] : 0.0;
     }
     __syncthreads();
     if (!ortho) cta_apply_q(Ucat, m, min(m, k), m, tauU, op.uo, rout, m);
@@ -404,16 +441,18 @@ __device__ void do_round(const RoundOp& op_in, double* dyn, long long smem_doubl
 
 // One CTA per worker; worker w runs ops [begin[w], begin[w+1]) in order (a
 // C block's whole operation list, each op reading the previous one's output).
-__global__ void __launch_bounds__(kT)
+template <typename R>
+__global__ void __launch_bounds__(kT, 4)
 round_worker_kernel(const RoundOp* __restrict__ ops, const int* __restrict__ begin,
-                    const int* __restrict__ workers, long long smem_doubles) {
-    extern __shared__ double dyn[];
-    __shared__ RoundShared sh;
+                    const int* __restrict__ workers, long long smem_elems) {
+    extern __shared__ __align__(16) unsigned char round_dyn[];
+    R* dyn = reinterpret_cast<R*>(round_dyn);
+    __shared__ RoundShared<R> sh;
     const int w = workers[blockIdx.x];
     const int b0 = begin[w], b1 = begin[w + 1];
     for (int i = b0; i < b1; ++i) {
         const RoundOp op = ops[i];
-        do_round(op, dyn, smem_doubles, sh);
+        do_round(op, dyn, smem_elems, sh);
         __syncthreads();
     }
 }
@@ -463,15 +502,11 @@ long long round_smem_need(const RoundOp& op) {
     return (ortho ? 0 : op.m * k) + (dense ? 0 : op.n * k) + 2 * k + ku * kv + kv * kv;
 }
 
-void launch_round_workers(Context& ctx, const std::vector<RoundOp>& ops,
-                          const std::vector<int>& begin, const char* name) {
-    if (ops.empty() || begin.size() < 2) return;
-    for (const RoundOp& op : ops) {
-        int k = op.kind == ROUND_DENSE ? op.n : op.r1 + (op.kind == ROUND_GENERAL ? op.r2 : 0);
-        if (op.kind == ROUND_SET || op.kind == ROUND_CONCAT) k = 0;
-        HMB_REQUIRE(k <= kMaxK, HM_ERR_UNSUPPORTED,
-                    "low-rank rounding of more than 128 stacked columns");
-    }
+namespace {
+
+template <typename R>
+void launch_round_typed(Context& ctx, const std::vector<RoundOp>& ops,
+                        const std::vector<int>& begin, const char* name) {
     // One launch.  The core and the rotations of an op live in shared memory
     // when they fit the launch's size, otherwise in the (L1-cached) global
     // work area; the size is the largest need of the non-dense ops (dense
@@ -487,7 +522,7 @@ void launch_round_workers(Context& ctx, const std::vector<RoundOp>& ops,
         const long long need = ku * kv + kv * kv;
         if (!dense || need <= 3072) smem = std::max(smem, need);
     }
-    smem = std::min(smem, kSmemDoubles);
+    smem = std::min<long long>(smem, kSmemBytes / (long long)sizeof(R));
     const int nw = (int)begin.size() - 1;
     std::vector<int> workers(nw);
     for (int w = 0; w < nw; ++w) workers[w] = w;
@@ -495,9 +530,9 @@ void launch_round_workers(Context& ctx, const std::vector<RoundOp>& ops,
     cudaGetDevice(&dev);
     static int attr_dev = -1;
     if (attr_dev != dev) {
-        HMB_CUDA(cudaFuncSetAttribute(round_worker_kernel,
+        HMB_CUDA(cudaFuncSetAttribute(round_worker_kernel<R>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(kSmemDoubles * sizeof(double))));
+                                      (int)kSmemBytes));
         attr_dev = dev;
     }
     DeviceBuffer<RoundOp> d;
@@ -506,9 +541,24 @@ void launch_round_workers(Context& ctx, const std::vector<RoundOp>& ops,
     db.upload(begin, ctx.stream);
     dw.upload(workers, ctx.stream);
     LaunchScope ls(ctx, name);
-    round_worker_kernel<<<(unsigned)nw, kT, smem * sizeof(double), ctx.stream>>>(
+    round_worker_kernel<R><<<(unsigned)nw, kT, smem * sizeof(R), ctx.stream>>>(
         d.get(), db.get(), dw.get(), smem);
     HMB_CHECK_LAUNCH();
+}
+
+}  // namespace
+
+void launch_round_workers(Context& ctx, const std::vector<RoundOp>& ops,
+                          const std::vector<int>& begin, const char* name) {
+    if (ops.empty() || begin.size() < 2) return;
+    for (const RoundOp& op : ops) {
+        int k = op.kind == ROUND_DENSE ? op.n : op.r1 + (op.kind == ROUND_GENERAL ? op.r2 : 0);
+        if (op.kind == ROUND_SET || op.kind == ROUND_CONCAT) k = 0;
+        HMB_REQUIRE(k <= kMaxK, HM_ERR_UNSUPPORTED,
+                    "low-rank rounding of more than 128 stacked columns");
+    }
+    if (ctx.low_precision) launch_round_typed<float>(ctx, ops, begin, name);
+    else launch_round_typed<double>(ctx, ops, begin, name);
 }
 
 void launch_qr_formq(Context& ctx, const std::vector<QrOp>& ops, const char* name) {

@@ -12,6 +12,7 @@
 #include "schulz.h"
 
 #include <cmath>
+#include <limits>
 
 #include "dense_ops.h"
 #include "hh.h"
@@ -333,7 +334,7 @@ double estimate_two_norm(Context& ctx, HMatrix& A, double theta, double confiden
 // SchulzInvert
 // ---------------------------------------------------------------------------
 SchulzResult schulz_invert(Context& ctx, HMatrix& A, int num_iterations, double theta,
-                           double confidence, double stop_tol) {
+                           double confidence, double stop_tol, double mixed_switch) {
     SchulzResult res;
     bool stop = false;
     if (num_iterations <= 0) {
@@ -346,15 +347,34 @@ SchulzResult schulz_invert(Context& ctx, HMatrix& A, int num_iterations, double 
     auto X = std::make_unique<HMatrix>();
     hmat_transpose(ctx, A, *X);
     hmat_scale(ctx, *X, alpha);
+    // Mixed precision: an iteration runs its two products in the
+    // low-precision phase while the last ||I - X A|| estimate is above
+    // mixed_switch (without stop checks: all but the last three
+    // iterations).  Newton-Schulz corrects the perturbation of a low-precision
+    // step (e_{k+1} ~ e_k^2 + its rounding level), so the FP64 iterations that
+    // follow reach the FP64 method's accuracy; the estimates themselves are
+    // always FP64.
+    const bool was_low = ctx.low_precision;
+    struct Restore {
+        Context& c;
+        bool v;
+        ~Restore() { c.low_precision = v; }
+    } restore{ctx, was_low};
+    double last = std::numeric_limits<double>::infinity();
     int k = 0;
     for (; k < num_iterations; ++k) {
+        const bool low = mixed_switch > 0.0 &&
+                         (stop ? last > mixed_switch : k + 3 < num_iterations);
+        ctx.low_precision = low || was_low;
+        if (low) ++res.low_iterations;
         HMatrix Z;
         hh_multiply(ctx, *X, A, -1.0, 0.0, Z, true);
         if (stop) {
             hmat_add_diagonal(ctx, Z, 1.0);
             const double ez = estimate_two_norm(ctx, Z, theta, confidence);
             res.trace.push_back(ez);
-            if (std::fabs(ez) < stop_tol) {
+            last = std::fabs(ez);
+            if (std::fabs(ez) < stop_tol && !low) {
                 hmat_add_diagonal(ctx, Z, 1.0);
                 auto Xn = std::make_unique<HMatrix>();
                 hh_multiply(ctx, Z, *X, 1.0, 0.0, *Xn, true);

@@ -8,6 +8,7 @@ namespace hmb {
 
 struct SchulzResult {
     int iterations = 0;
+    int low_iterations = 0;      // iterations run in the low-precision phase
     std::vector<double> trace;   // [est ||A||, est ||I - X_k A|| per stop check]
 };
 
@@ -15,7 +16,9 @@ double estimate_two_norm(Context& ctx, HMatrix& A, double theta, double confiden
 // Drops the trailing zero columns that tolerance truncation leaves in the
 // low-rank blocks (synchronizes to read the ranks back).
 void compact_ranks(Context& ctx, HMatrix& H);
+// mixed_switch > 0: mixed precision (iterations in the low-precision phase
+// while the last ||I - X A|| estimate is above mixed_switch).
 SchulzResult schulz_invert(Context& ctx, HMatrix& A, int num_iterations, double theta,
-                           double confidence, double stop_tol);
+                           double confidence, double stop_tol, double mixed_switch = 0.0);
 
 }  // namespace hmb

@@ -66,6 +66,11 @@ class Context:
     def set_compression_tolerance(self, tol: float):
         check(lib().hm_set_compression_tolerance(self._h, float(tol)))
 
+    def set_low_precision(self, on: bool):
+        """Low-precision phase for this context's H*H products: range samples
+        on the TF32 tensor cores, block roundings in FP32."""
+        check(lib().hm_set_low_precision(self._h, int(bool(on))))
+
     def compression_tolerance(self) -> float:
         v = C.c_double()
         check(lib().hm_get_compression_tolerance(self._h, C.byref(v)))
@@ -386,6 +391,23 @@ class _HMatBase:
                                      float(confidence), float(stopTol), C.byref(its), trace,
                                      cap, C.byref(n)))
         return its.value, [trace[i] for i in range(min(n.value, cap))]
+
+    def SchulzInvertMixed(self, numIterations: int, theta: float = 1.5,
+                          confidence: float = 6.0, stopTol: float = 1e-4,
+                          mixedSwitch: float = 1e-2):
+        """Mixed-precision SchulzInvert: iterations run their H*H products in
+        the low-precision phase (TF32 range samples, FP32 roundings) while
+        the last ||I - X_k A|| estimate is above mixedSwitch, then FP64.
+
+        Returns (iterations run, low-precision iterations, trace)."""
+        its, low = C.c_int(), C.c_int()
+        cap = 64
+        trace = (C.c_double * cap)()
+        n = C.c_int()
+        check(lib().hm_schulz_invert_mixed(self._h, int(numIterations), float(theta),
+                                           float(confidence), float(stopTol), float(mixedSwitch),
+                                           C.byref(its), C.byref(low), trace, cap, C.byref(n)))
+        return its.value, low.value, [trace[i] for i in range(min(n.value, cap))]
 
 
 def _handle_of(obj) -> C.c_void_p:

@@ -168,6 +168,26 @@ HM_API int hm_schulz_invert(hm_matrix h, int num_iterations, double theta,
                             double confidence, double stop_tol, int* iterations,
                             double* trace, int trace_cap, int* trace_len);
 
+/*
+ * Mixed-precision SchulzInvert (same iteration and stop test as
+ * hm_schulz_invert).  While the last ||I - X_k A|| estimate is above
+ * mixed_switch (without the stop test: all but the last three iterations),
+ * an iteration runs its two H*H products in the low-precision phase (range
+ * samples on the TF32 tensor cores, block roundings in FP32); the others,
+ * the norm estimates and the sample orthogonalisation are FP64.
+ * mixed_switch = 0 is hm_schulz_invert.  low_iterations receives the number
+ * of low-precision iterations.  The reference has only the FP64 method.
+ */
+HM_API int hm_schulz_invert_mixed(hm_matrix h, int num_iterations, double theta,
+                                  double confidence, double stop_tol, double mixed_switch,
+                                  int* iterations, int* low_iterations, double* trace,
+                                  int trace_cap, int* trace_len);
+/* Low-precision phase for the context's H*H products (on != 0): range
+   samples in TF32, roundings in FP32 (relative block error about 1e-6 from
+   the roundings, up to about 1e-3 in blocks whose spectrum reaches below
+   TF32's resolution).  Off by default. */
+HM_API int hm_set_low_precision(hm_context ctx, int on);
+
 /* CopyFrom (src/HMat2d/HMat2d.cpp:331-391); AdjointFrom / TransposeFrom for
    real scalars (HMat2d.cpp:479-614); *dst == NULL creates a new handle. */
 HM_API int hm_copy(hm_matrix src, hm_matrix* dst);

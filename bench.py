@@ -489,28 +489,36 @@ def schulz_leg(device, with_reference):
     return out
 
 
-SCHULZ_MODES = dict(sizes=(64, 64), levels=5, rank=16, oversample=4, seed=1, stop_tol=1e-8,
-                    tol=1e-10)
+SCHULZ_MODES = dict(sizes=(128, 128), levels=5, rank=16, oversample=4, seed=1, stop_tol=1e-8,
+                    tol=1e-10, mixed_switch=0.1,
+                    train=(((64, 64), 4, 6), ((128, 128), 5, 3)))
 
 
 def schulz_modes_leg(device):
-    """SchulzInvert(-1, 1.5, 6, stopTol 1e-8) on the 64 x 64 five-point
-    operator (N = 4096, 16-point leaves, maxRank 16), three ways, each from a
-    fresh context: the plain method (fixed rank maxRank, the reference's
-    HMat2d semantics), tolerance truncation at 1e-10 (CompressionTolerance),
-    and tolerance truncation with learned sample counts (the rank predictor
-    trained, on the GPU, on the kept ranks logged by a 6-iteration run of the
-    same operator family with another coefficient seed).  Each reports wall
-    seconds (the iteration reads one norm estimate back per step), iterations,
-    the attained ||I - X A|| estimate, the residual ||X A p - p|| / ||p|| on
-    probe vectors, and the sample counts drawn."""
+    """SchulzInvert(-1, 1.5, 6, stopTol 1e-8) on the 128 x 128 five-point
+    operator (N = 16384, 64-point leaves, maxRank 16, oversample 4), each
+    mode from a fresh context:
+      plain_fp64        the reference's HMat2d method (fixed rank maxRank),
+      mixed             the same with the early iterations in the
+                        low-precision phase (TF32 range samples, FP32
+                        roundings) while ||I - X A|| > 0.1, then FP64,
+      tolerance_1e-10   tolerance truncation (CompressionTolerance),
+      mixed_tolerance   both,
+      learned_mixed     both, with learned sample counts (the rank predictor
+                        trained on the GPU on the kept ranks logged by short
+                        tolerance runs at 64 x 64 and 128 x 128 on another
+                        coefficient field).
+    Each reports wall seconds (the iteration reads one norm estimate back per
+    step), iterations (low-precision ones), the final ||I - X A|| estimate,
+    the residual ||X A p - p|| / ||p|| and the relative difference of X p
+    from the plain FP64 inverse on probe vectors."""
     import dmhm_b200 as D
     cfg = SCHULZ_MODES
     sz, L, r = cfg["sizes"], cfg["levels"], cfg["rank"]
 
-    def make(seed, tol, log=False):
-        coef = D.operators.uniform_coefficients(sz, seed)
-        S = D.operators.stencil(sz, coef, L)
+    def make(sizes, levels, seed, tol, log=False):
+        coef = D.operators.uniform_coefficients(sizes, seed)
+        S = D.operators.stencil(sizes, coef, levels)
         ctx = D.Context(device)
         ctx.set_oversample(cfg["oversample"])
         ctx.set_compression_tolerance(tol)
@@ -518,24 +526,39 @@ def schulz_modes_leg(device):
             ctx.rank_log_enable(True)
         return ctx, S
 
-    # training data: kept ranks of a short run on another coefficient field
+    # training data: kept ranks of short runs on another coefficient field
     t0 = time.perf_counter()
-    ctx, S = make(cfg["seed"] + 100, cfg["tol"], log=True)
-    H = D.HMat2d(S, L, r, True, *sz, ctx=ctx)
-    H.SchulzInvert(6, 1.5, 6.0, 1e-30)
-    x, t = ctx.rank_log(clear=True)
+    xs, ts = [], []
+    for tsz, tl, tits in cfg["train"]:
+        ctx, S = make(tsz, tl, cfg["seed"] + 100, cfg["tol"], log=True)
+        H = D.HMat2d(S, tl, r, True, *tsz, ctx=ctx)
+        H.SchulzInvert(tits, 1.5, 6.0, 1e-30)
+        x, t = ctx.rank_log(clear=True)
+        xs.append(x)
+        ts.append(t)
+        del H, ctx
+    x, t = np.concatenate(xs), np.concatenate(ts)
+    ctx, _ = make(sz, L, cfg["seed"] + 100, cfg["tol"])
     model = D.RankModel(ctx, seed=7)
     loss0, _ = model.loss_grad(x, t)
     loss = model.train(x, t, epochs=800, lr=1e-2)
     params = model.params()
     train_s = time.perf_counter() - t0
     out = {"workload": "SchulzInvert(-1, theta 1.5, confidence 6, stopTol 1e-8), HMat2d<double> "
-                       "64x64 five-point operator, numLevels 5, maxRank 16, oversample 4",
+                       "128x128 five-point operator, numLevels 5 (64-point leaves), maxRank 16, "
+                       "oversample 4",
            "training": {"rows": int(x.shape[0]), "loss_initial": loss0, "loss_final": loss,
-                        "epochs": 800, "seconds": train_s}}
-    for mode, tol, learned in (("plain_fp64", 0.0, False), ("tolerance_1e-10", cfg["tol"], False),
-                               ("learned_1e-10", cfg["tol"], True)):
-        ctx, S = make(cfg["seed"], tol)
+                        "epochs": 800, "seconds": train_s,
+                        "runs": [f"{a[0][0]}x{a[0][1]} numLevels {a[1]}, {a[2]} iterations"
+                                 for a in cfg["train"]]}}
+    P = np.random.default_rng(5).standard_normal((sz[0] * sz[1], 4))
+    ref_xp = None
+    modes = (("plain_fp64", 0.0, False, 0.0), ("mixed", 0.0, False, cfg["mixed_switch"]),
+             ("tolerance_1e-10", cfg["tol"], False, 0.0),
+             ("mixed_tolerance_1e-10", cfg["tol"], False, cfg["mixed_switch"]),
+             ("learned_mixed_1e-10", cfg["tol"], True, cfg["mixed_switch"]))
+    for mode, tol, learned, switch in modes:
+        ctx, S = make(sz, L, cfg["seed"], tol)
         if learned:
             m = D.RankModel(ctx, seed=7)
             m.set_params(params)
@@ -543,16 +566,23 @@ def schulz_modes_leg(device):
         H = D.HMat2d(S, L, r, True, *sz, ctx=ctx)
         ctx.synchronize()
         t0 = time.perf_counter()
-        its, trace = H.SchulzInvert(-1, 1.5, 6.0, cfg["stop_tol"])
+        its, low, trace = H.SchulzInvertMixed(-1, 1.5, 6.0, cfg["stop_tol"], switch)
         ctx.synchronize()
         secs = time.perf_counter() - t0
         A = D.HMat2d(S, L, r, True, *sz, ctx=ctx)
-        P = np.random.default_rng(5).standard_normal((A.Width(), 4))
+        xp = H.Multiply(1.0, P)
         res = np.linalg.norm(H.Multiply(1.0, A.Multiply(1.0, P)) - P) / np.linalg.norm(P)
-        out[mode] = {"seconds": secs, "iterations": its, "final_norm_estimate": trace[-1],
+        if ref_xp is None:
+            ref_xp = xp
+        out[mode] = {"seconds": secs, "iterations": its, "low_precision_iterations": low,
+                     "final_norm_estimate": trace[-1],
                      "relative_residual_XAp_minus_p": float(res),
+                     "rel_diff_vs_plain_fp64": float(np.linalg.norm(xp - ref_xp) /
+                                                     np.linalg.norm(ref_xp)),
                      "rank_sum": H.BlockCensus()["rank_sum"], "sampling": ctx.rank_stats()}
-    out["speedup_learned_vs_plain"] = out["plain_fp64"]["seconds"] / out["learned_1e-10"]["seconds"]
+        del H, A, ctx
+    base = out["plain_fp64"]["seconds"]
+    out["speedup_vs_plain_fp64"] = {k: base / out[k]["seconds"] for k, *_ in modes}
     return out
 
 

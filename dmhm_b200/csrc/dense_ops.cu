@@ -99,11 +99,15 @@ gemm_ops_kernel(const GemmOp* __restrict__ ops, const int* __restrict__ tile_op,
 
 // One CTA per worker: ops [begin[w], begin[w+1]) in order, all tiles of each.
 __global__ void __launch_bounds__(kT)
-gemm_worker_kernel(const GemmOp* __restrict__ ops, const int* __restrict__ begin) {
+gemm_worker_kernel(const GemmOp* __restrict__ ops, const int* __restrict__ begin,
+                   const RelocBases bases) {
     __shared__ double sA[16][65];
     __shared__ double sB[16][65];
     for (int i = begin[blockIdx.x]; i < begin[blockIdx.x + 1]; ++i) {
-        const GemmOp op = ops[i];
+        GemmOp op = ops[i];
+        op.A = reloc(op.A, bases);
+        op.B = reloc(op.B, bases);
+        op.C = reloc(op.C, bases);
         const int tiles = ((op.m + 63) / 64) * ((op.n + 63) / 64);
         for (int t = 0; t < tiles; ++t) {
             gemm_tile(op, t, sA, sB);
@@ -137,16 +141,27 @@ void launch_gemm_ops(Context& ctx, const std::vector<GemmOp>& ops, const char* n
     HMB_CHECK_LAUNCH();
 }
 
+void upload_gemm_list(Context& ctx, const std::vector<GemmOp>& ops, const std::vector<int>& begin,
+                      GemmList& out) {
+    out.nw = 0;
+    if (ops.empty() || begin.size() < 2) return;
+    out.ops.upload(ops, ctx.stream);
+    out.begin.upload(begin, ctx.stream);
+    out.nw = (int)begin.size() - 1;
+}
+
+void launch_gemm_list(Context& ctx, const GemmList& L, const RelocBases& bases, const char* name) {
+    if (L.nw == 0) return;
+    LaunchScope ls(ctx, name);
+    gemm_worker_kernel<<<(unsigned)L.nw, kT, 0, ctx.stream>>>(L.ops.get(), L.begin.get(), bases);
+    HMB_CHECK_LAUNCH();
+}
+
 void launch_gemm_workers(Context& ctx, const std::vector<GemmOp>& ops,
                          const std::vector<int>& begin, const char* name) {
-    if (ops.empty() || begin.size() < 2) return;
-    DeviceBuffer<GemmOp> d_ops;
-    DeviceBuffer<int> d_b;
-    d_ops.upload(ops, ctx.stream);
-    d_b.upload(begin, ctx.stream);
-    LaunchScope ls(ctx, name);
-    gemm_worker_kernel<<<(unsigned)(begin.size() - 1), kT, 0, ctx.stream>>>(d_ops.get(), d_b.get());
-    HMB_CHECK_LAUNCH();
+    GemmList L;
+    upload_gemm_list(ctx, ops, begin, L);
+    launch_gemm_list(ctx, L, RelocBases{}, name);
 }
 
 }  // namespace hmb

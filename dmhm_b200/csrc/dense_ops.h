@@ -3,6 +3,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "reloc.h"
 
 namespace hmb {
 
@@ -23,5 +24,15 @@ void launch_gemm_ops(Context& ctx, const std::vector<GemmOp>& ops, const char* n
 // worker may update the same C); different workers write disjoint C.
 void launch_gemm_workers(Context& ctx, const std::vector<GemmOp>& ops,
                          const std::vector<int>& begin, const char* name);
+// The same from a device-resident list whose pointers may be tagged offsets
+// (reloc.h).
+struct GemmList {
+    DeviceBuffer<GemmOp> ops;
+    DeviceBuffer<int> begin;
+    int nw = 0;
+};
+void upload_gemm_list(Context& ctx, const std::vector<GemmOp>& ops, const std::vector<int>& begin,
+                      GemmList& out);
+void launch_gemm_list(Context& ctx, const GemmList& L, const RelocBases& bases, const char* name);
 
 }  // namespace hmb

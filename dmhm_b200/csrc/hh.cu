@@ -460,12 +460,27 @@ std::vector<double> probe_errors(Context& ctx, const Structure& S, const HMatrix
 // oversampling; generator positions are kept as draw counts from the
 // starting state.  Plans are cached per context (the last kHHPlans), so the
 // iterations of SchulzInvert, whose ranks repeat, plan once.
+// Per-block operation lists of a plan in position-independent form (pointer
+// fields are tagged offsets into the product's buffers, see reloc.h): built
+// by the first product that uses the plan, replayed by the next ones.
+// Indices of the base table: doubles 0 W arena, 1 A, 2 B, 3 C, 4 state
+// slots, 5 C's previous storage, 6 rounding work; ints 0 per-op ranks,
+// 1 kept ranks of the sampled products.
+struct BlockCache {
+    RoundList rounds;
+    GemmList gemms;
+    long long pa_used = 0, wk_used = 0;
+    double tol = 0.0;
+    bool a_is_b = false;
+};
+
 struct SymPlan {
     std::vector<WTask> w;
     PerBlock<LOp> lops;
     PerBlock<DOp> dops;
     uint64_t serial_steps = 0;
     std::vector<int> crank, state_rank, op_kind;
+    std::shared_ptr<BlockCache> blocks;
 };
 
 struct SymKey {
@@ -941,143 +956,197 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
     // One worker (CTA) per C leaf block runs that block's operations in the
     // reference's order; blocks proceed independently.  Low-rank states of a
     // block with several operations alternate between two scratch slots; the
-    // last operation writes into C.
-    Arena pa, wk;
-    std::vector<long long> slot0(S.blocks.size(), -1), slot1(S.blocks.size(), -1);
-    std::vector<long long> wslot(S.blocks.size(), -1);
-    for (int c : S.leaves) {
-        const Block& Cb = S.blocks[c];
-        const int nops = P.lops.size(c);
-        if (Cb.kind != KIND_LOWRANK || nops == 0) continue;
-        int mr = 0;
-        for (int j = 0; j + 1 < nops; ++j) mr = std::max(mr, state_rank[P.lops.begin[c] + j]);
-        if (nops > 1) {
-            slot0[c] = pa.take((long long)(Cb.m + Cb.n) * mr);
-            slot1[c] = pa.take((long long)(Cb.m + Cb.n) * mr);
-        }
-    }
-    DeviceBuffer<double> parena;
-    parena.allocate((size_t)std::max<long long>(pa.used, 2), st);
-    double* P0 = parena.get();
-    std::vector<RoundOp> rops;
-    std::vector<int> rbegin{0};
-    std::vector<long long> rwork;   // per op: offset into the work arena
-    // truncating runs: every op leaves its output rank in rk, the next op of
-    // the block (and a sampled W's kept rank) set its input ranks on the device
+    // last operation writes into C.  The lists depend only on the plan (and
+    // the truncation tolerance): built once, cached with it, then replayed.
     const bool dyn = ctx.compression_tol > 0.0;
+    const bool a_is_b = A.data.get() == B.data.get();
+    std::shared_ptr<BlockCache> bc = plan->blocks;
+    if (bc && (bc->tol != ctx.compression_tol || bc->a_is_b != a_is_b)) bc.reset();
+    DeviceBuffer<double> parena, wbuf;
     DeviceBuffer<int> rk;
     if (dyn) rk.allocate(std::max<size_t>(1, P.lops.ops.size()), st);
-    std::vector<GemmOp> gops;
-    std::vector<int> gbegin{0};
-    for (int c : S.leaves) {
-        const Block& Cb = S.blocks[c];
-        if (Cb.kind == KIND_LOWRANK) {
+    auto bases_now = [&]() {
+        RelocBases b{};
+        b.d[0] = W0;
+        b.d[1] = const_cast<double*>(A.data.get());
+        b.d[2] = const_cast<double*>(B.data.get());
+        b.d[3] = C.data.get();
+        b.d[4] = parena.get();
+        b.d[5] = c_old_data.get();
+        b.d[6] = wbuf.get();
+        b.i[0] = rk.get();
+        b.i[1] = kept.get();
+        return b;
+    };
+    if (bc) {
+        HostScope replay(ctx, "hh_block_lists_replayed");
+        parena.allocate((size_t)std::max<long long>(bc->pa_used, 2), st);
+        if (bc->rounds.nw > 0) wbuf.allocate((size_t)std::max<long long>(bc->wk_used, 2), st);
+    } else {
+        Arena pa, wk;
+        std::vector<long long> slot0(S.blocks.size(), -1), slot1(S.blocks.size(), -1);
+        std::vector<long long> wslot(S.blocks.size(), -1);
+        for (int c : S.leaves) {
+            const Block& Cb = S.blocks[c];
             const int nops = P.lops.size(c);
-            const LOp* ops = P.lops.of(c);
-            const int obase = P.lops.begin[c];
-            if (nops == 0) continue;
-            const double* cu = nullptr;
-            const double* cv = nullptr;
-            int cr = 0;
-            if (!fresh) {
-                cu = c_old_data.get() + c_old_off[c];
-                cv = cu + (long long)Cb.m * c_old_rank[c];
-                cr = c_old_rank[c];
+            if (Cb.kind != KIND_LOWRANK || nops == 0) continue;
+            int mr = 0;
+            for (int j = 0; j + 1 < nops; ++j) mr = std::max(mr, state_rank[P.lops.begin[c] + j]);
+            if (nops > 1) {
+                slot0[c] = pa.take((long long)(Cb.m + Cb.n) * mr);
+                slot1[c] = pa.take((long long)(Cb.m + Cb.n) * mr);
             }
-            long long wmax = 0;
-            const size_t first = rops.size();
-            int prev = -1;   // op whose output is (cu, cv)
-            for (int j = 0; j < nops; ++j) {
-                const LOp& op = ops[j];
-                const int rnew = state_rank[obase + j];
-                if (op.type == L_RESET) {
-                    cr = 0;
-                    prev = -1;
-                    continue;
-                }
-                double* ou = (j + 1 == nops) ? C.U(c)
-                                                    : P0 + ((j & 1) ? slot1[c] : slot0[c]);
-                double* ov = ou + (long long)Cb.m * rnew;
-                const WTask& t = P.w[op.w];
-                RoundOp r{};
-                r.kind = op_kind[obase + j];
-                r.m = Cb.m;
-                r.n = Cb.n;
-                r.alpha = 1.0;
-                r.beta = op.beta;
-                r.rout = rnew;
-                r.uo = ou;
-                r.vo = ov;
-                if (op.type == L_DDC) {
-                    r.u1 = t.D;
-                    r.ldu1 = t.m;
-                } else {
-                    r.u1 = t.U ? t.U + op.row0 : nullptr;
-                    r.v1 = t.V ? t.V + op.col0 : nullptr;
-                    r.ldu1 = t.ldU;
-                    r.ldv1 = t.ldV;
-                    r.r1 = t.r;
-                }
-                r.u2 = cu;
-                r.v2 = cv;
-                r.tol = ctx.compression_tol;
-                r.r2 = (op.type == L_SET || (op.type == L_DDC && op.beta == 0.0)) ? 0 : cr;
-                r.ldu2 = Cb.m;
-                r.ldv2 = Cb.n;
-                if (dyn) {
-                    r.rank_out = rk.get() + rops.size();
-                    if (r.r2 > 0 && prev >= 0) r.r2_dev = rk.get() + prev;
-                    if (op.type != L_DDC && hh_pos[op.w] >= 0) r.r1_dev = kept.get() + hh_pos[op.w];
-                }
-                prev = -1;
-                if (rnew > 0 && Cb.m > 0 && Cb.n > 0) {
-                    prev = (int)rops.size();
-                    rops.push_back(r);
-                    wmax = std::max(wmax, round_work_size(r));
-                }
-                cu = ou;
-                cv = ov;
-                cr = rnew;
-            }
-            if (rops.size() > first) {
-                const long long w0 = wk.take(wmax);
-                for (size_t i = first; i < rops.size(); ++i) rwork.push_back(w0);
-                rbegin.push_back((int)rops.size());
-            }
-        } else {
-            const size_t first = gops.size();
-            if (!fresh)
-                gops.push_back({c_old_data.get() + c_old_off[c], nullptr, C.D(c), 1.0, 0.0, Cb.m,
-                                Cb.n, -1, Cb.m, 0, Cb.m, 0, 0});
-            for (int j = 0; j < P.dops.size(c); ++j) {
-                const DOp& op = P.dops.of(c)[j];
-                if (op.type == D_DD) {
-                    const Block& Ba = S.blocks[op.a];
-                    const Block& Bb = S.blocks[op.b];
-                    gops.push_back({A.D(op.a), B.D(op.b), C.D(c), op.alpha, op.beta, Cb.m, Cb.n,
-                                    Ba.n, Ba.m, Bb.m, Cb.m, 0, 0});
-                } else {
-                    const WTask& t = P.w[op.w];
-                    if (t.r == 0)
-                        gops.push_back({C.D(c), nullptr, C.D(c), op.beta, 0.0, Cb.m, Cb.n, -1,
-                                        Cb.m, 0, Cb.m, 0, 0});
-                    else
-                        gops.push_back({t.U + op.row0, t.V + op.col0, C.D(c), 1.0, op.beta, Cb.m,
-                                        Cb.n, t.r, t.ldU, t.ldV, Cb.m, 0, 1});
-                }
-            }
-            if (gops.size() > first && Cb.m > 0 && Cb.n > 0) gbegin.push_back((int)gops.size());
-            else gops.resize(first);
         }
-    }
-    DeviceBuffer<double> wbuf;
-    if (!rops.empty()) {
-        wbuf.allocate((size_t)std::max<long long>(wk.used, 2), st);
-        for (size_t i = 0; i < rops.size(); ++i) rops[i].work = wbuf.get() + rwork[i];
+        parena.allocate((size_t)std::max<long long>(pa.used, 2), st);
+        double* P0 = parena.get();
+        std::vector<RoundOp> rops;
+        std::vector<int> rbegin{0};
+        std::vector<long long> rwork;   // per op: offset into the work arena
+        // truncating runs: every op leaves its output rank in rk, the next op of
+        // the block (and a sampled W's kept rank) set its input ranks on the device
+        std::vector<GemmOp> gops;
+        std::vector<int> gbegin{0};
+        for (int c : S.leaves) {
+            const Block& Cb = S.blocks[c];
+            if (Cb.kind == KIND_LOWRANK) {
+                const int nops = P.lops.size(c);
+                const LOp* ops = P.lops.of(c);
+                const int obase = P.lops.begin[c];
+                if (nops == 0) continue;
+                const double* cu = nullptr;
+                const double* cv = nullptr;
+                int cr = 0;
+                if (!fresh) {
+                    cu = c_old_data.get() + c_old_off[c];
+                    cv = cu + (long long)Cb.m * c_old_rank[c];
+                    cr = c_old_rank[c];
+                }
+                long long wmax = 0;
+                const size_t first = rops.size();
+                int prev = -1;   // op whose output is (cu, cv)
+                for (int j = 0; j < nops; ++j) {
+                    const LOp& op = ops[j];
+                    const int rnew = state_rank[obase + j];
+                    if (op.type == L_RESET) {
+                        cr = 0;
+                        prev = -1;
+                        continue;
+                    }
+                    double* ou = (j + 1 == nops) ? C.U(c)
+                                                        : P0 + ((j & 1) ? slot1[c] : slot0[c]);
+                    double* ov = ou + (long long)Cb.m * rnew;
+                    const WTask& t = P.w[op.w];
+                    RoundOp r{};
+                    r.kind = op_kind[obase + j];
+                    r.m = Cb.m;
+                    r.n = Cb.n;
+                    r.alpha = 1.0;
+                    r.beta = op.beta;
+                    r.rout = rnew;
+                    r.uo = ou;
+                    r.vo = ov;
+                    if (op.type == L_DDC) {
+                        r.u1 = t.D;
+                        r.ldu1 = t.m;
+                    } else {
+                        r.u1 = t.U ? t.U + op.row0 : nullptr;
+                        r.v1 = t.V ? t.V + op.col0 : nullptr;
+                        r.ldu1 = t.ldU;
+                        r.ldv1 = t.ldV;
+                        r.r1 = t.r;
+                    }
+                    r.u2 = cu;
+                    r.v2 = cv;
+                    r.tol = ctx.compression_tol;
+                    r.r2 = (op.type == L_SET || (op.type == L_DDC && op.beta == 0.0)) ? 0 : cr;
+                    r.ldu2 = Cb.m;
+                    r.ldv2 = Cb.n;
+                    if (dyn) {
+                        r.rank_out = rk.get() + rops.size();
+                        if (r.r2 > 0 && prev >= 0) r.r2_dev = rk.get() + prev;
+                        if (op.type != L_DDC && hh_pos[op.w] >= 0) r.r1_dev = kept.get() + hh_pos[op.w];
+                    }
+                    prev = -1;
+                    if (rnew > 0 && Cb.m > 0 && Cb.n > 0) {
+                        prev = (int)rops.size();
+                        rops.push_back(r);
+                        wmax = std::max(wmax, round_work_size(r));
+                    }
+                    cu = ou;
+                    cv = ov;
+                    cr = rnew;
+                }
+                if (rops.size() > first) {
+                    const long long w0 = wk.take(wmax);
+                    for (size_t i = first; i < rops.size(); ++i) rwork.push_back(w0);
+                    rbegin.push_back((int)rops.size());
+                }
+            } else {
+                const size_t first = gops.size();
+                if (!fresh)
+                    gops.push_back({c_old_data.get() + c_old_off[c], nullptr, C.D(c), 1.0, 0.0, Cb.m,
+                                    Cb.n, -1, Cb.m, 0, Cb.m, 0, 0});
+                for (int j = 0; j < P.dops.size(c); ++j) {
+                    const DOp& op = P.dops.of(c)[j];
+                    if (op.type == D_DD) {
+                        const Block& Ba = S.blocks[op.a];
+                        const Block& Bb = S.blocks[op.b];
+                        gops.push_back({A.D(op.a), B.D(op.b), C.D(c), op.alpha, op.beta, Cb.m, Cb.n,
+                                        Ba.n, Ba.m, Bb.m, Cb.m, 0, 0});
+                    } else {
+                        const WTask& t = P.w[op.w];
+                        if (t.r == 0)
+                            gops.push_back({C.D(c), nullptr, C.D(c), op.beta, 0.0, Cb.m, Cb.n, -1,
+                                            Cb.m, 0, Cb.m, 0, 0});
+                        else
+                            gops.push_back({t.U + op.row0, t.V + op.col0, C.D(c), 1.0, op.beta, Cb.m,
+                                            Cb.n, t.r, t.ldU, t.ldV, Cb.m, 0, 1});
+                    }
+                }
+                if (gops.size() > first && Cb.m > 0 && Cb.n > 0) gbegin.push_back((int)gops.size());
+                else gops.resize(first);
+            }
+        }
+        if (!rops.empty()) {
+            wbuf.allocate((size_t)std::max<long long>(wk.used, 2), st);
+            for (size_t i = 0; i < rops.size(); ++i) rops[i].work = wbuf.get() + rwork[i];
+        }
+
+        // position-independent copy for the cache
+        Relocator rel;
+        rel.add(0, W0, wa.used);
+        rel.add(1, A.data.get(), A.total);
+        rel.add(2, B.data.get(), B.total);
+        rel.add(3, C.data.get(), C.total);
+        rel.add(4, parena.get(), pa.used);
+        rel.add(5, c_old_data.get(), (long long)c_old_data.size());
+        rel.add(6, wbuf.get(), wk.used);
+        rel.add(0, rk.get(), (long long)rk.size());
+        rel.add(1, kept.get(), (long long)kept.size());
+        std::vector<RoundOp> trops = rops;
+        std::vector<GemmOp> tgops = gops;
+        bool ok = true;
+        for (RoundOp& r : trops) {
+            ok = ok && rel.tag(r.u1) && rel.tag(r.v1) && rel.tag(r.u2) && rel.tag(r.v2) &&
+                 rel.tag(r.uo) && rel.tag(r.vo) && rel.tag(r.work) && rel.tag(r.rank_out) &&
+                 rel.tag(r.r1_dev) && rel.tag(r.r2_dev);
+        }
+        for (GemmOp& g : tgops) ok = ok && rel.tag(g.A) && rel.tag(g.B) && rel.tag(g.C);
+        bc = std::make_shared<BlockCache>();
+        upload_round_list(ctx, ok ? trops : rops, rbegin, bc->rounds);
+        upload_gemm_list(ctx, ok ? tgops : gops, gbegin, bc->gemms);
+        bc->pa_used = pa.used;
+        bc->wk_used = wk.used;
+        bc->tol = ctx.compression_tol;
+        bc->a_is_b = a_is_b;
+        // lists that point outside the registered buffers run once, uncached
+        if (ok) plan->blocks = bc;
+        else HostScope uncached(ctx, "hh_block_lists_uncached");
     }
     hs.reset(new HostScope(ctx, "hh_block_launch"));
-    launch_round_workers(ctx, rops, rbegin, "block_round");
-    launch_gemm_workers(ctx, gops, gbegin, "dense_update");
+    const RelocBases bases = bases_now();
+    launch_round_list(ctx, bc->rounds, bases, "block_round");
+    launch_gemm_list(ctx, bc->gemms, bases, "dense_update");
     // low-rank C blocks whose final rank is 0 or that received no operation
     // need nothing: their storage is empty.
     ctx.serial_state = serial_after;

@@ -61,7 +61,7 @@ struct StagingRing {
     char* buf = nullptr;
     size_t cap = 0, head = 0;
 };
-constexpr size_t kStagingBytes = size_t(64) << 20;
+constexpr size_t kStagingBytes = size_t(128) << 20;
 std::mutex g_staging_mu;
 std::map<cudaStream_t, StagingRing> g_staging;
 

@@ -444,14 +444,25 @@ __device__ void do_round(const RoundOp& op_in, R* dyn, long long smem_elems, Rou
 template <typename R>
 __global__ void __launch_bounds__(kT, 4)
 round_worker_kernel(const RoundOp* __restrict__ ops, const int* __restrict__ begin,
-                    const int* __restrict__ workers, long long smem_elems) {
+                    const int* __restrict__ workers, long long smem_elems,
+                    const RelocBases bases) {
     extern __shared__ __align__(16) unsigned char round_dyn[];
     R* dyn = reinterpret_cast<R*>(round_dyn);
     __shared__ RoundShared<R> sh;
     const int w = workers[blockIdx.x];
     const int b0 = begin[w], b1 = begin[w + 1];
     for (int i = b0; i < b1; ++i) {
-        const RoundOp op = ops[i];
+        RoundOp op = ops[i];
+        op.u1 = reloc(op.u1, bases);
+        op.v1 = reloc(op.v1, bases);
+        op.u2 = reloc(op.u2, bases);
+        op.v2 = reloc(op.v2, bases);
+        op.uo = reloc(op.uo, bases);
+        op.vo = reloc(op.vo, bases);
+        op.work = reloc(op.work, bases);
+        op.rank_out = reloc(op.rank_out, bases);
+        op.r1_dev = reloc(op.r1_dev, bases);
+        op.r2_dev = reloc(op.r2_dev, bases);
         do_round(op, dyn, smem_elems, sh);
         __syncthreads();
     }
@@ -493,39 +504,13 @@ void launch_round_ops(Context& ctx, std::vector<RoundOp>& ops, const char* name)
     launch_round_workers(ctx, ops, begin, name);
 }
 
-long long round_smem_need(const RoundOp& op) {
-    if (op.kind == ROUND_SET || op.kind == ROUND_CONCAT) return 0;
-    const bool ortho = op.kind == ROUND_ORTHO, dense = op.kind == ROUND_DENSE;
-    const long long k = dense ? op.n : op.r1 + (op.kind == ROUND_GENERAL ? op.r2 : 0);
-    const long long ku = ortho ? op.r1 : std::min<long long>(op.m, k);
-    const long long kv = dense ? op.n : std::min<long long>(op.n, k);
-    return (ortho ? 0 : op.m * k) + (dense ? 0 : op.n * k) + 2 * k + ku * kv + kv * kv;
-}
 
 namespace {
 
 template <typename R>
-void launch_round_typed(Context& ctx, const std::vector<RoundOp>& ops,
-                        const std::vector<int>& begin, const char* name) {
-    // One launch.  The core and the rotations of an op live in shared memory
-    // when they fit the launch's size, otherwise in the (L1-cached) global
-    // work area; the size is the largest need of the non-dense ops (dense
-    // compressions with larger cores take the global path), so that more
-    // CTAs share an SM.
-    long long smem = 0;
-    for (const RoundOp& op : ops) {
-        if (op.kind == ROUND_SET || op.kind == ROUND_CONCAT) continue;
-        const bool dense = op.kind == ROUND_DENSE;
-        const long long k = dense ? op.n : op.r1 + (op.kind == ROUND_GENERAL ? op.r2 : 0);
-        const long long ku = op.kind == ROUND_ORTHO ? op.r1 : std::min<long long>(op.m, k);
-        const long long kv = dense ? op.n : std::min<long long>(op.n, k);
-        const long long need = ku * kv + kv * kv;
-        if (!dense || need <= 3072) smem = std::max(smem, need);
-    }
-    smem = std::min<long long>(smem, kSmemBytes / (long long)sizeof(R));
-    const int nw = (int)begin.size() - 1;
-    std::vector<int> workers(nw);
-    for (int w = 0; w < nw; ++w) workers[w] = w;
+void launch_round_typed(Context& ctx, const RoundList& L, const RelocBases& bases,
+                        const char* name) {
+    const long long smem = sizeof(R) == 8 ? L.smem_double : L.smem_float;
     int dev = 0;
     cudaGetDevice(&dev);
     static int attr_dev = -1;
@@ -535,30 +520,56 @@ void launch_round_typed(Context& ctx, const std::vector<RoundOp>& ops,
                                       (int)kSmemBytes));
         attr_dev = dev;
     }
-    DeviceBuffer<RoundOp> d;
-    d.upload(ops, ctx.stream);
-    DeviceBuffer<int> db, dw;
-    db.upload(begin, ctx.stream);
-    dw.upload(workers, ctx.stream);
     LaunchScope ls(ctx, name);
-    round_worker_kernel<R><<<(unsigned)nw, kT, smem * sizeof(R), ctx.stream>>>(
-        d.get(), db.get(), dw.get(), smem);
+    round_worker_kernel<R><<<(unsigned)L.nw, kT, smem * sizeof(R), ctx.stream>>>(
+        L.ops.get(), L.begin.get(), L.workers.get(), smem, bases);
     HMB_CHECK_LAUNCH();
 }
 
 }  // namespace
 
-void launch_round_workers(Context& ctx, const std::vector<RoundOp>& ops,
-                          const std::vector<int>& begin, const char* name) {
+void upload_round_list(Context& ctx, const std::vector<RoundOp>& ops,
+                       const std::vector<int>& begin, RoundList& out) {
+    out.nw = 0;
     if (ops.empty() || begin.size() < 2) return;
+    // The core and the rotations of an op live in shared memory when they
+    // fit the launch's size, otherwise in the (L1-cached) global work area;
+    // the size is the largest need of the non-dense ops (dense compressions
+    // with larger cores take the global path), so that more CTAs share an SM.
+    long long need_max = 0;
     for (const RoundOp& op : ops) {
-        int k = op.kind == ROUND_DENSE ? op.n : op.r1 + (op.kind == ROUND_GENERAL ? op.r2 : 0);
-        if (op.kind == ROUND_SET || op.kind == ROUND_CONCAT) k = 0;
+        if (op.kind == ROUND_SET || op.kind == ROUND_CONCAT) continue;
+        const bool dense = op.kind == ROUND_DENSE;
+        const long long k = dense ? op.n : op.r1 + (op.kind == ROUND_GENERAL ? op.r2 : 0);
         HMB_REQUIRE(k <= kMaxK, HM_ERR_UNSUPPORTED,
                     "low-rank rounding of more than 128 stacked columns");
+        const long long ku = op.kind == ROUND_ORTHO ? op.r1 : std::min<long long>(op.m, k);
+        const long long kv = dense ? op.n : std::min<long long>(op.n, k);
+        const long long need = ku * kv + kv * kv;
+        if (!dense || need <= 3072) need_max = std::max(need_max, need);
     }
-    if (ctx.low_precision) launch_round_typed<float>(ctx, ops, begin, name);
-    else launch_round_typed<double>(ctx, ops, begin, name);
+    out.smem_double = std::min<long long>(need_max, kSmemBytes / 8);
+    out.smem_float = std::min<long long>(need_max, kSmemBytes / 4);
+    out.nw = (int)begin.size() - 1;
+    std::vector<int> workers(out.nw);
+    for (int w = 0; w < out.nw; ++w) workers[w] = w;
+    out.ops.upload(ops, ctx.stream);
+    out.begin.upload(begin, ctx.stream);
+    out.workers.upload(workers, ctx.stream);
+}
+
+void launch_round_list(Context& ctx, const RoundList& L, const RelocBases& bases,
+                       const char* name) {
+    if (L.nw == 0) return;
+    if (ctx.low_precision) launch_round_typed<float>(ctx, L, bases, name);
+    else launch_round_typed<double>(ctx, L, bases, name);
+}
+
+void launch_round_workers(Context& ctx, const std::vector<RoundOp>& ops,
+                          const std::vector<int>& begin, const char* name) {
+    RoundList L;
+    upload_round_list(ctx, ops, begin, L);
+    launch_round_list(ctx, L, RelocBases{}, name);
 }
 
 void launch_qr_formq(Context& ctx, const std::vector<QrOp>& ops, const char* name) {

@@ -3,6 +3,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "reloc.h"
 
 namespace hmb {
 
@@ -36,6 +37,19 @@ struct RoundOp {
     const int* r1_dev;
     const int* r2_dev;
 };
+
+// A device-resident list of rounding ops in worker order (see
+// launch_round_workers).
+struct RoundList {
+    DeviceBuffer<RoundOp> ops;
+    DeviceBuffer<int> begin, workers;
+    int nw = 0;
+    long long smem_double = 0, smem_float = 0;   // shared elements per CTA
+};
+void upload_round_list(Context& ctx, const std::vector<RoundOp>& ops,
+                       const std::vector<int>& begin, RoundList& out);
+void launch_round_list(Context& ctx, const RoundList& L, const RelocBases& bases,
+                       const char* name);
 
 // Scratch doubles one op needs (0 for SET / CONCAT).
 long long round_work_size(const RoundOp& op);

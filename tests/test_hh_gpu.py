@@ -109,3 +109,36 @@ def test_errors():
     B = build(D, other, c)
     with pytest.raises(D.HMError):
         A.Multiply(1.0, B)                  # different structures
+
+
+@pytest.mark.parametrize("case", ["c1", "c3d"])
+def test_cached_lists_replay(case):
+    """The second product with the same plan replays the cached
+    position-independent block lists against new buffers: same generator
+    state, same result, also when the factors change from A * A to A * B
+    with the same ranks."""
+    fx = load(case)
+    P = fx["probes"]
+    c = fresh_ctx(fx)
+    A = build(D, fx, c)
+    A.SetToRandom()
+    B = build(D, fx, c, "coefB" if "coefB" in fx else "coef")
+    B.SetToRandom()
+    st = c.lcg_states()
+    C1 = A.Multiply(0.5, B).Multiply(1.0, P)
+    c.set_lcg_states(*st)
+    C2 = A.Multiply(0.5, B).Multiply(1.0, P)
+    assert np.array_equal(C1, C2)
+    c.set_lcg_states(*st)
+    AA1 = A.Multiply(0.5, A).Multiply(1.0, P)
+    c.set_lcg_states(*st)
+    AA2 = A.Multiply(0.5, A).Multiply(1.0, P)
+    assert np.array_equal(AA1, AA2)
+    # a fresh context (no cached lists) agrees with the replays
+    c2 = fresh_ctx(fx)
+    A2 = build(D, fx, c2)
+    A2.SetToRandom()
+    B2 = build(D, fx, c2, "coefB" if "coefB" in fx else "coef")
+    B2.SetToRandom()
+    c2.set_lcg_states(*st)
+    assert np.array_equal(A2.Multiply(0.5, B2).Multiply(1.0, P), C1)

@@ -586,6 +586,99 @@ def schulz_modes_leg(device):
     return out
 
 
+HELMHOLTZ = dict(count=48, sides=(32, 48, 64, 96, 128), k_range=(2.0, 10.0), rank=24,
+                 oversample=4, rhs=8, stop_tol=1e-8, mixed_switch=0.1, seed=21, leaf_target=32,
+                 streams=8, dense_check_max_n=2304)
+
+
+def helmholtz_levels(side, target):
+    """numLevels whose leaf (side / 2^(L-1))^2 points is closest to `target`
+    (both axes must halve evenly down to the leaves)."""
+    best = None
+    for L in range(1, 12):
+        if side % (1 << (L - 1)):
+            break
+        leaf = (side >> (L - 1)) ** 2
+        if best is None or abs(leaf - target) < abs(best[1] - target):
+            best = (L, leaf)
+    return best[0]
+
+
+def helmholtz_batch_leg(device, count=None, max_side=None):
+    """Batch of independent HMat2d<std::complex<double>> instances: shifted
+    five-point Helmholtz-like operators (diagonal 4 + 0.2i - (k h)^2,
+    off-diagonals -1, h = 1/(side+1), k uniform in [2, 10), sides drawn from
+    {32, 48, 64, 96, 128}, leaf size closest to 32 points, maxRank 24),
+    each inverted by mixed-precision SchulzInvert to ||I - X A|| < 1e-8 and
+    applied to 8 random complex right-hand sides.  Instances run
+    concurrently, one context (CUDA stream) per host thread.  Reports
+    instances and right-hand-side solves per second over the whole batch
+    (wall clock from the first build to the last result), and per instance
+    the residual ||A X b - b|| / ||b|| and, for N <= 2304, the relative error
+    of X b against a dense solve of the same operator."""
+    import concurrent.futures as cf
+    import dmhm_b200 as D
+    from dmhm_b200 import operators as O
+    cfg = HELMHOLTZ
+    count = count or cfg["count"]
+    rng = np.random.default_rng(cfg["seed"])
+    inst = []
+    for i in range(cfg["count"]):
+        side = int(rng.choice(cfg["sides"]))
+        k = float(rng.uniform(*cfg["k_range"]))
+        inst.append((i, side, k))
+    if max_side:
+        inst = [t for t in inst if t[1] <= max_side]
+    inst = inst[:count]
+    nthreads = min(cfg["streams"], len(inst))
+    ctxs = [D.Context(device) for _ in range(nthreads)]
+    for c in ctxs:
+        c.set_oversample(cfg["oversample"])
+
+    def solve(job):
+        slot, (i, side, k) = job
+        ctx = ctxs[slot]
+        L = helmholtz_levels(side, cfg["leaf_target"])
+        S = O.helmholtz((side, side), k, L)
+        t0 = time.perf_counter()
+        X = D.HMat2d(S, L, cfg["rank"], True, side, side, ctx=ctx)
+        its, low, trace = X.SchulzInvertMixed(-1, 1.5, 6.0, cfg["stop_tol"], cfg["mixed_switch"])
+        r = np.random.default_rng(1000 + i)
+        B = r.standard_normal((S.height, cfg["rhs"])) + 1j * r.standard_normal((S.height, cfg["rhs"]))
+        Y = X.Multiply(1.0, B)
+        secs = time.perf_counter() - t0
+        A = D.HMat2d(S, L, cfg["rank"], True, side, side, ctx=ctx)
+        res = float(np.linalg.norm(A.Multiply(1.0, Y) - B) / np.linalg.norm(B))
+        out = {"instance": i, "side": side, "k": k, "levels": L, "N": S.height,
+               "iterations": its, "low_precision_iterations": low, "final_norm_estimate": trace[-1],
+               "seconds": secs, "residual_AXb_minus_b": res}
+        if S.height <= cfg["dense_check_max_n"]:
+            Ad = O.dense_from_sparse(S)
+            ref = np.linalg.solve(Ad, B)
+            out["rel_err_vs_dense_solve"] = float(np.linalg.norm(Y - ref) / np.linalg.norm(ref))
+        del X, A
+        return out
+
+    jobs = [(j % nthreads, t) for j, t in enumerate(inst)]
+    # one thread per context: each thread takes the jobs of its slot in order
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=nthreads) as ex:
+        futs = [ex.submit(lambda s=s: [solve(j) for j in jobs if j[0] == s]) for s in range(nthreads)]
+        results = sorted((r for f in futs for r in f.result()), key=lambda r: r["instance"])
+    wall = time.perf_counter() - t0
+    for c in ctxs:
+        c.synchronize()
+    return {"workload": f"{len(inst)} HMat2d<complex<double>> Helmholtz-like instances "
+                        f"(sides {sorted(set(t[1] for t in inst))}, maxRank {cfg['rank']}, "
+                        f"oversample {cfg['oversample']}), mixed SchulzInvert to 1e-8, "
+                        f"{cfg['rhs']} complex right-hand sides each, {nthreads} streams",
+            "instances_per_s": len(inst) / wall, "rhs_solves_per_s": len(inst) * cfg["rhs"] / wall,
+            "wall_s": wall, "max_residual": max(r["residual_AXb_minus_b"] for r in results),
+            "max_rel_err_vs_dense": max((r["rel_err_vs_dense_solve"] for r in results
+                                         if "rel_err_vs_dense_solve" in r), default=None),
+            "instances": results}
+
+
 def cpu_baseline(coef, X, nbytes):
     if not os.path.exists(REF_DRIVER):
         return {"value": None, "unit": "GB/s", "cores": 1, "kind": "reference",

@@ -55,6 +55,10 @@ SIGNATURES = {
     "hm_get_lcg_states": [_P, _PU64, _PU64],
     "hm_natural_to_hierarchical_map": [_I, _PI, _I, _PI],
     "hm_create_from_csr": [_P, _I, _PI, _I, _I, _I, _PI64, _PI32, _PD, C.POINTER(_P)],
+    "hm_create_from_csr_complex": [_P, _I, _PI, _I, _I, _I, _PI64, _PI32, _PD, C.POINTER(_P)],
+    "hm_is_complex": [_P, _PI],
+    "hm_multiply_dense_complex": [_P, _I, _D, _D, _P, _I, _D, _D, _P, _I, _I],
+    "hm_multiply_dense_complex_host": [_P, _I, _D, _D, _PD, _I, _D, _D, _PD, _I, _I],
     "hm_destroy": [_P],
     "hm_info": [_P, _PI, _PI, _PI, _PI, _PI64, _PI64],
     "hm_set_to_random": [_P],

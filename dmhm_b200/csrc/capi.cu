@@ -366,6 +366,105 @@ int hm_create_from_csr(hm_context ctx, int dim, const int* sizes, int num_levels
     });
 }
 
+int hm_create_from_csr_complex(hm_context ctx, int dim, const int* sizes, int num_levels,
+                               int max_rank, int strongly_admissible, const int64_t* row_offsets,
+                               const int32_t* col_indices, const double* values, hm_matrix* out) {
+    return guarded([&] {
+        HMB_REQUIRE(ctx && sizes && row_offsets && out, HM_ERR_ARGUMENT, "NULL argument");
+        HMB_REQUIRE(max_rank >= 0, HM_ERR_ARGUMENT, "max_rank must be >= 0");
+        *out = nullptr;
+        HMB_CUDA(cudaSetDevice(ctx->c.device));
+        auto* m = new_handle(ctx);
+        try {
+            m->h.S = build_structure(dim, sizes, num_levels, strongly_admissible != 0, 2);
+            m->h.max_rank = 2 * max_rank;
+            const int n = m->h.S->N / 2;
+            const int64_t nnz = row_offsets[n];
+            HMB_REQUIRE(nnz == 0 || (col_indices && values), HM_ERR_ARGUMENT,
+                        "NULL CSR arrays");
+            // real form: entry a + bi at (i, j) -> [[a, -b], [b, a]] at rows
+            // 2i, 2i+1 and columns 2j, 2j+1 (zero parts dropped)
+            std::vector<int64_t> rows((size_t)2 * n + 1, 0);
+            std::vector<int32_t> cols;
+            std::vector<double> vals;
+            cols.reserve((size_t)nnz * 4);
+            vals.reserve((size_t)nnz * 4);
+            for (int i = 0; i < n; ++i)
+                for (int half = 0; half < 2; ++half) {
+                    for (int64_t k = row_offsets[i]; k < row_offsets[i + 1]; ++k) {
+                        const int j = col_indices[k];
+                        HMB_REQUIRE(j >= 0 && j < n, HM_ERR_ARGUMENT,
+                                    "CSR column index out of range");
+                        const double a = values[2 * k], b = values[2 * k + 1];
+                        const double re_col = half == 0 ? a : b;    // column 2j
+                        const double im_col = half == 0 ? -b : a;   // column 2j + 1
+                        if (re_col != 0.0) {
+                            cols.push_back(2 * j);
+                            vals.push_back(re_col);
+                        }
+                        if (im_col != 0.0) {
+                            cols.push_back(2 * j + 1);
+                            vals.push_back(im_col);
+                        }
+                    }
+                    rows[(size_t)2 * i + half + 1] = (int64_t)cols.size();
+                }
+            import_csr(m->h, rows.data(), cols.data(), vals.data());
+        } catch (...) {
+            delete_handle(m);
+            throw;
+        }
+        *out = m;
+    });
+}
+
+int hm_is_complex(hm_matrix h, int* is_complex) {
+    return guarded([&] {
+        HMB_REQUIRE(h && is_complex, HM_ERR_ARGUMENT, "NULL argument");
+        owner_of(h);
+        *is_complex = h->h.S && h->h.S->dof == 2 ? 1 : 0;
+    });
+}
+
+int hm_multiply_dense_complex(hm_matrix h, int op, double alpha_re, double alpha_im,
+                              const double* B, int ldb, double beta_re, double beta_im, double* C,
+                              int ldc, int nrhs) {
+    return guarded([&] {
+        HMB_REQUIRE(h && (nrhs == 0 || (B && C)), HM_ERR_ARGUMENT, "NULL argument");
+        owner_of(h);
+        multiply_dense_complex(h->h, op, alpha_re, alpha_im, B, ldb, beta_re, beta_im, C, ldc,
+                               nrhs);
+    });
+}
+
+int hm_multiply_dense_complex_host(hm_matrix h, int op, double alpha_re, double alpha_im,
+                                   const double* B, int ldb, double beta_re, double beta_im,
+                                   double* C, int ldc, int nrhs) {
+    return guarded([&] {
+        HMB_REQUIRE(h && (nrhs == 0 || (B && C)), HM_ERR_ARGUMENT, "NULL argument");
+        Context& ctx = owner_of(h)->c;
+        HMB_REQUIRE(h->h.S && h->h.S->dof == 2, HM_ERR_ARGUMENT, "not a complex H-matrix");
+        const int n = h->h.height() / 2;
+        HMB_REQUIRE(ldb >= std::max(1, n) && ldc >= std::max(1, n), HM_ERR_ARGUMENT,
+                    "leading dimension too small");
+        if (nrhs == 0) return;
+        const size_t col = (size_t)n * 2 * sizeof(double);
+        DeviceBuffer<double> dB, dC;
+        dB.allocate((size_t)2 * n * nrhs, ctx.stream);
+        dC.allocate((size_t)2 * n * nrhs, ctx.stream);
+        HMB_CUDA(cudaMemcpy2DAsync(dB.get(), col, B, (size_t)ldb * 2 * sizeof(double), col, nrhs,
+                                   cudaMemcpyHostToDevice, ctx.stream));
+        if (beta_re != 0.0 || beta_im != 0.0)
+            HMB_CUDA(cudaMemcpy2DAsync(dC.get(), col, C, (size_t)ldc * 2 * sizeof(double), col,
+                                       nrhs, cudaMemcpyHostToDevice, ctx.stream));
+        multiply_dense_complex(h->h, op, alpha_re, alpha_im, dB.get(), n, beta_re, beta_im,
+                               dC.get(), n, nrhs);
+        HMB_CUDA(cudaMemcpy2DAsync(C, (size_t)ldc * 2 * sizeof(double), dC.get(), col, col, nrhs,
+                                   cudaMemcpyDeviceToHost, ctx.stream));
+        HMB_CUDA(cudaStreamSynchronize(ctx.stream));
+    });
+}
+
 int hm_destroy(hm_matrix h) {
     return guarded([&] {
         if (!h) return;

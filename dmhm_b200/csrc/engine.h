@@ -205,6 +205,12 @@ void ensure_tf32_copy(Context& ctx, HMatrix& H);
 void multiply_dense_tf32(HMatrix& H, double alpha, const double* B, int ldb, double beta,
                          double* C, int ldc, int nrhs);
 
+// Complex H-matrix (real form, structure dof 2) times complex dense blocks
+// (interleaved re, im; leading dimensions in complex elements), device
+// pointers: op 0 C = alpha A B + beta C, 1 with A^T, 2 with A^H (complex.cu).
+void multiply_dense_complex(HMatrix& H, int op, double ar, double ai, const double* B, int ldb,
+                            double br, double bi, double* C, int ldc, int nrhs);
+
 // Device kernels driven from the host side (launchers).
 void launch_fill_random(Context& ctx, HMatrix& H);
 

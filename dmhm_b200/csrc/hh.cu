@@ -608,7 +608,9 @@ std::shared_ptr<SymPlan> get_plan(Context& ctx, const HMatrix& A, const HMatrix&
             return hit.second;
         }
     }
-    auto plan = make_plan(A, B, C, alpha, beta, fresh, maxRankC, ctx.oversample);
+    // complex matrices (real form, 2 rows per point): oversample complex
+    // directions = 2 x oversample real ones
+    auto plan = make_plan(A, B, C, alpha, beta, fresh, maxRankC, ctx.oversample * A.S->dof);
     E.emplace_back(std::move(key), plan);
     if (E.size() > kHHPlans) E.erase(E.begin());
     return plan;
@@ -745,7 +747,7 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
             WTask& t = P.w[hh[i]];
             int rp = (int)std::ceil(pred[i] * t.r) + ctx.rank_margin;
             rp = std::max(1, std::min(rp, t.r));
-            t.k = std::min(k_plain[i], rp + ctx.oversample);
+            t.k = std::min(k_plain[i], rp + ctx.oversample * S.dof);
             t.kq = std::min(S.blocks[t.a].m, t.k);
         }
     }

@@ -22,6 +22,8 @@
 #include "lowrank.h"
 
 #include <algorithm>
+#include <mutex>
+#include <set>
 
 namespace hmb {
 
@@ -511,14 +513,17 @@ template <typename R>
 void launch_round_typed(Context& ctx, const RoundList& L, const RelocBases& bases,
                         const char* name) {
     const long long smem = sizeof(R) == 8 ? L.smem_double : L.smem_float;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    static int attr_dev = -1;
-    if (attr_dev != dev) {
-        HMB_CUDA(cudaFuncSetAttribute(round_worker_kernel<R>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)kSmemBytes));
-        attr_dev = dev;
+    {
+        // once per device (contexts on several host threads may get here at once)
+        int dev = 0;
+        cudaGetDevice(&dev);
+        static std::mutex mu;
+        static std::set<int> done;
+        std::lock_guard<std::mutex> lock(mu);
+        if (done.insert(dev).second)
+            HMB_CUDA(cudaFuncSetAttribute(round_worker_kernel<R>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)kSmemBytes));
     }
     LaunchScope ls(ctx, name);
     round_worker_kernel<R><<<(unsigned)L.nw, kT, smem * sizeof(R), ctx.stream>>>(

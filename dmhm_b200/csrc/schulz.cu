@@ -286,7 +286,10 @@ double estimate_two_norm(Context& ctx, HMatrix& A, double theta, double confiden
     HMB_REQUIRE(theta > 1.0, HM_ERR_ARGUMENT, "theta must be > 1");
     HMB_REQUIRE(confidence > 0.0, HM_ERR_ARGUMENT, "confidence must be positive");
     const int n = A.height();
-    const int k = (int)std::ceil(std::log(0.8 * std::sqrt((double)n) * std::pow(10.0, confidence)) /
+    // power steps from the matrix's own height (complex rows for the real
+    // form of a complex matrix, as the reference's complex instantiation)
+    const int nk = n / A.S->dof;
+    const int k = (int)std::ceil(std::log(0.8 * std::sqrt((double)nk) * std::pow(10.0, confidence)) /
                                  std::log(theta));
     cudaStream_t st = ctx.stream;
     DeviceBuffer<double> x, y, partial, scal;

@@ -26,6 +26,7 @@ void fill_box(Structure& S, int id, int level, const int* coord,
         b.size[k] = k < S.dim ? size[k] : 1;
         b.count *= b.size[k];
     }
+    b.count *= S.dof;
     b.offset = offset;
     b.first_child = -1;
     b.leaf0 = S.num_clusters();
@@ -67,15 +68,16 @@ bool Structure::in_subtree(int b, int root) const {
 
 bool same_structure(const Structure& a, const Structure& b) {
     return a.dim == b.dim && a.num_levels == b.num_levels && a.strong == b.strong &&
+           a.dof == b.dof &&
            a.sizes[0] == b.sizes[0] && a.sizes[1] == b.sizes[1] && a.sizes[2] == b.sizes[2];
 }
 
-std::shared_ptr<Structure> build_structure(int dim, const int* sizes,
-                                           int num_levels, bool strong) {
+std::shared_ptr<Structure> build_structure(int dim, const int* sizes, int num_levels,
+                                           bool strong, int dof) {
     // H-matrices over the same grid share one structure object.
     static std::mutex mu;
     static std::map<std::vector<int>, std::weak_ptr<Structure>> cache;
-    std::vector<int> key{dim, num_levels, strong ? 1 : 0};
+    std::vector<int> key{dim, num_levels, strong ? 1 : 0, dof};
     for (int k = 0; k < dim; ++k) key.push_back(sizes[k]);
     {
         std::lock_guard<std::mutex> lock(mu);
@@ -83,14 +85,14 @@ std::shared_ptr<Structure> build_structure(int dim, const int* sizes,
         if (it != cache.end())
             if (auto sp = it->second.lock()) return sp;
     }
-    auto S = build_structure_uncached(dim, sizes, num_levels, strong);
+    auto S = build_structure_uncached(dim, sizes, num_levels, strong, dof);
     std::lock_guard<std::mutex> lock(mu);
     cache[key] = S;
     return S;
 }
 
-std::shared_ptr<Structure> build_structure_uncached(int dim, const int* sizes,
-                                                    int num_levels, bool strong) {
+std::shared_ptr<Structure> build_structure_uncached(int dim, const int* sizes, int num_levels,
+                                                    bool strong, int dof) {
     HMB_REQUIRE(dim == 2 || dim == 3, HM_ERR_ARGUMENT, "dim must be 2 or 3");
     HMB_REQUIRE(num_levels >= 1 && num_levels <= 16, HM_ERR_ARGUMENT,
                 "num_levels must be in [1, 16]");
@@ -99,7 +101,9 @@ std::shared_ptr<Structure> build_structure_uncached(int dim, const int* sizes,
     S->num_levels = num_levels;
     S->strong = strong;
     S->q = 1 << dim;
-    long long N = 1;
+    HMB_REQUIRE(dof == 1 || dof == 2, HM_ERR_ARGUMENT, "dof must be 1 or 2");
+    S->dof = dof;
+    long long N = dof;
     for (int k = 0; k < 3; ++k) {
         S->sizes[k] = k < dim ? sizes[k] : 1;
         HMB_REQUIRE(S->sizes[k] >= 1, HM_ERR_ARGUMENT, "grid sizes must be >= 1");

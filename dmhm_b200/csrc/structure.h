@@ -39,7 +39,11 @@ struct Structure {
     int num_levels = 1;
     bool strong = true;
     int q = 4;        // children per side of a node: 2^dim
-    int N = 0;
+    // Unknowns per grid point: 1, or 2 for the real form of a complex matrix
+    // (point p owns rows dof*p .. dof*p + dof - 1; box offsets, counts and
+    // block sizes are in rows)
+    int dof = 1;
+    int N = 0;        // rows = dof * grid points
 
     std::vector<Box> boxes;     // box 0 = the whole grid
     std::vector<int> leaf_box;  // leaf cluster -> box id (hierarchical order)
@@ -57,10 +61,10 @@ struct Structure {
 
 // Builds the structure (shared by all H-matrices over the same grid and
 // parameters); throws hmb::Error on bad arguments.
-std::shared_ptr<Structure> build_structure(int dim, const int* sizes,
-                                           int num_levels, bool strong);
-std::shared_ptr<Structure> build_structure_uncached(int dim, const int* sizes,
-                                                    int num_levels, bool strong);
+std::shared_ptr<Structure> build_structure(int dim, const int* sizes, int num_levels,
+                                           bool strong, int dof = 1);
+std::shared_ptr<Structure> build_structure_uncached(int dim, const int* sizes, int num_levels,
+                                                    bool strong, int dof = 1);
 bool same_structure(const Structure& a, const Structure& b);
 
 // map[natural] = hierarchical index (x fastest in the natural order).

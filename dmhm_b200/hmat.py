@@ -209,10 +209,16 @@ class _HMatBase:
             raise _lib.HMError(1, "sparse matrix does not match the grid")
         rows = np.ascontiguousarray(S.rowOffsets, dtype=np.int64)
         cols = np.ascontiguousarray(S.columnIndices, dtype=np.int32)
-        vals = np.ascontiguousarray(S.nonzeros, dtype=np.float64)
         sz = _as_i32(list(sizes))
         h = C.c_void_p()
-        check(lib().hm_create_from_csr(
+        if np.iscomplexobj(S.nonzeros):
+            # HMat2d<std::complex<double>>: interleaved (re, im) values
+            vals = np.ascontiguousarray(S.nonzeros, dtype=np.complex128).view(np.float64)
+            create = lib().hm_create_from_csr_complex
+        else:
+            vals = np.ascontiguousarray(S.nonzeros, dtype=np.float64)
+            create = lib().hm_create_from_csr
+        check(create(
             self.ctx.handle, self.dim, sz.ctypes.data_as(_lib._PI), int(numLevels),
             int(maxRank), int(bool(stronglyAdmissible)), rows.ctypes.data_as(_lib._PI64),
             cols.ctypes.data_as(_lib._PI32), vals.ctypes.data_as(_lib._PD), C.byref(h)))
@@ -240,11 +246,20 @@ class _HMatBase:
                             counts, C.byref(nbytes)))
         return h.value, w.value, L.value, r.value, list(counts), nbytes.value
 
+    @property
+    def is_complex(self) -> bool:
+        """Scalar = std::complex<double> (stored in real form on the device)."""
+        v = C.c_int()
+        check(lib().hm_is_complex(self._h, C.byref(v)))
+        return bool(v.value)
+
     def Height(self) -> int:
-        return self._info()[0]
+        h = self._info()[0]
+        return h // 2 if self.is_complex else h
 
     def Width(self) -> int:
-        return self._info()[1]
+        w = self._info()[1]
+        return w // 2 if self.is_complex else w
 
     def NumLevels(self) -> int:
         return self._info()[2]
@@ -269,7 +284,29 @@ class _HMatBase:
         check(lib().hm_set_to_random(self._h))
 
     # -- H * dense ------------------------------------------------------------
+    def _apply_complex(self, op: int, alpha, B, beta, Cout):
+        """Complex Multiply / TransposeMultiply / AdjointMultiply (op 0 / 1 /
+        2) on host arrays through the engine's complex entry."""
+        n = self.Height()
+        Bn = np.asarray(B, dtype=np.complex128)
+        vec = Bn.ndim == 1
+        B2 = np.asfortranarray(Bn.reshape(-1, 1) if vec else Bn)
+        if B2.shape[0] != n:
+            raise _lib.HMError(1, "nonconformal multiply")
+        k = B2.shape[1]
+        if Cout is None:
+            C2 = np.zeros((n, k), dtype=np.complex128, order="F")
+        else:
+            C2 = np.asfortranarray(np.asarray(Cout, dtype=np.complex128).reshape(n, k))
+        a, b = complex(alpha), complex(beta)
+        check(lib().hm_multiply_dense_complex_host(
+            self._h, op, a.real, a.imag, B2.ctypes.data_as(_lib._PD), n, b.real, b.imag,
+            C2.ctypes.data_as(_lib._PD), n, k))
+        return C2[:, 0].copy() if vec else C2
+
     def _apply(self, transpose: int, alpha: float, B, beta: float, Cout):
+        if self.is_complex:
+            return self._apply_complex(transpose, alpha, B, beta, Cout)
         n = self.Height() if transpose else self.Width()
         m = self.Width() if transpose else self.Height()
         if _is_cuda_tensor(B):
@@ -332,7 +369,10 @@ class _HMatBase:
         return self._apply(1, alpha, B, 0.0 if beta is None else beta, C)
 
     def AdjointMultiply(self, alpha, B, beta=None, C=None):
-        """AdjointMultiply: equal to TransposeMultiply for real scalars."""
+        """AdjointMultiply: C := alpha H^H B (+ beta C); equal to
+        TransposeMultiply for real scalars."""
+        if self.is_complex:
+            return self._apply_complex(2, alpha, B, 0.0 if beta is None else beta, C)
         return self.TransposeMultiply(alpha, B, beta, C)
 
     def _multiply_hmat(self, alpha, B, beta, Cm):

@@ -91,6 +91,38 @@ HM_API int hm_create_from_csr(hm_context ctx, int dim, const int* sizes,
                        int num_levels, int max_rank, int strongly_admissible,
                        const int64_t* row_offsets, const int32_t* col_indices,
                        const double* values, hm_matrix* out);
+/*
+ * HMat2d<std::complex<double>> / HMat3d<std::complex<double>> (explicit
+ * instantiations, src/HMat2d/HMat2d.cpp:1321-1324) from a complex CSR in
+ * hierarchical order: values[2k], values[2k+1] = real, imaginary part of
+ * nonzero k (the memory of std::complex<double>[]).  Stored on the device in
+ * real form (two rows per grid point, entry a + bi as [[a, -b], [b, a]], a
+ * complex rank-r block as a real rank-2r block), so every H-matrix entry of
+ * this header (products, H*H, SchulzInvert, EstimateTwoNorm, copy,
+ * transpose = AdjointFrom, real Scale / AddConstantToDiagonal) applies to it
+ * unchanged, on real vectors of twice the length, which are the complex
+ * vectors in interleaved storage; hm_info reports that real form.  H*H
+ * products draw 2 x Oversample() real samples per complex direction.
+ */
+HM_API int hm_create_from_csr_complex(hm_context ctx, int dim, const int* sizes, int num_levels,
+                                      int max_rank, int strongly_admissible,
+                                      const int64_t* row_offsets, const int32_t* col_indices,
+                                      const double* values, hm_matrix* out);
+HM_API int hm_is_complex(hm_matrix h, int* is_complex);
+/*
+ * Complex Multiply / TransposeMultiply / AdjointMultiply against dense
+ * blocks (src/HMat2d/MultiplyDense-incl.hpp:12-260 for Scalar =
+ * std::complex<double>): C := alpha op(A) B + beta C, op 0 = A, 1 = A^T,
+ * 2 = A^H; B, C interleaved complex, leading dimensions in complex elements;
+ * DEVICE pointers (stream-ordered) or HOST pointers (copies, synchronizes).
+ */
+HM_API int hm_multiply_dense_complex(hm_matrix h, int op, double alpha_re, double alpha_im,
+                                     const double* B, int ldb, double beta_re, double beta_im,
+                                     double* C, int ldc, int nrhs);
+HM_API int hm_multiply_dense_complex_host(hm_matrix h, int op, double alpha_re,
+                                          double alpha_im, const double* B, int ldb,
+                                          double beta_re, double beta_im, double* C, int ldc,
+                                          int nrhs);
 HM_API int hm_destroy(hm_matrix h);
 
 /* Height, width, number of levels, max rank, and the block census:

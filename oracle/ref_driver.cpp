@@ -11,6 +11,8 @@
  *   schulz  SchulzInvert       (src/HMat2d/Invert-incl.hpp:127-196; 3-D :127-186)
  *   lcg     first draws of the serial generator (src/core/random.cpp:13-119,
  *           include/dmhm/core/random.hpp:238-445)
+ *   cmatvec / chh / cschulz   the same on HMat2d<std::complex<double>> over a
+ *           shifted Helmholtz-like operator (RunComplex below)
  *
  * The operator is the grid stencil the workloads use: a 5-point (2-D) or
  * 7-point (3-D) operator in natural x-fastest order, diagonal 2*d*c_i + shift,
@@ -24,6 +26,7 @@
 #include "dmhm.hpp"
 #include <cstdio>
 #include <cstdlib>
+#include <complex>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -45,12 +48,13 @@ struct DriverArgs
     std::string cmd;
     int dim, nx, ny, nz, levels, rank, oversample, strong, random;
     int nrhs, repeat, iters, count, useB;
-    double shift, alpha, theta, conf, stopTol;
+    double shift, alpha, theta, conf, stopTol, kwave, absorption;
     std::string coef, coefB, x, out;
     DriverArgs()
     : dim(2), nx(32), ny(32), nz(1), levels(4), rank(8), oversample(4),
       strong(1), random(0), nrhs(1), repeat(1), iters(-1), count(16), useB(0),
-      shift(0.1), alpha(1.0), theta(1.5), conf(6.0), stopTol(1e-4) { }
+      shift(0.1), alpha(1.0), theta(1.5), conf(6.0), stopTol(1e-4), kwave(5.0),
+      absorption(0.2) { }
 };
 
 std::vector<double> ReadDoubles(const std::string& path, size_t n)
@@ -318,6 +322,84 @@ int Run(const DriverArgs& a)
     return 0;
 }
 
+// Complex-double path (HMat2d<std::complex<double>>, explicitly instantiated
+// at src/HMat2d/HMat2d.cpp:1321-1324) on the shifted five-point
+// Helmholtz-like operator: diagonal 4 + absorption i - (k h)^2 with
+// h = 1 / (nx + 1), off-diagonals -1, natural x-fastest order permuted to the
+// hierarchical order.  Commands: cmatvec (y = A x), chh (C = A A applied to
+// the probes), cschulz (SchulzInvert applied to the probes).  Complex vectors
+// are read and written as interleaved (re, im) float64.
+int RunComplex(const DriverArgs& a)
+{
+    typedef std::complex<double> C;
+    const int N = a.nx * a.ny;
+    Vector<int> map;
+    HMat2d<C>::BuildNaturalToHierarchicalMap(map, a.nx, a.ny, a.levels);
+    Vector<int> inv(N);
+    for (int i = 0; i < N; ++i) inv[map[i]] = i;
+    const double h = 1.0 / (a.nx + 1);
+    const C diag(4.0 - (a.kwave * h) * (a.kwave * h), a.absorption);
+    Sparse<C> S;
+    S.height = N; S.width = N; S.symmetric = false;
+    for (int i = 0; i < N; ++i)
+    {
+        S.rowOffsets.PushBack(S.nonzeros.Size());
+        const int nat = inv[i];
+        const int x = nat % a.nx, y = nat / a.nx;
+        int nb[4]; int nn = 0;
+        if (x > 0) nb[nn++] = nat - 1;
+        if (x < a.nx - 1) nb[nn++] = nat + 1;
+        if (y > 0) nb[nn++] = nat - a.nx;
+        if (y < a.ny - 1) nb[nn++] = nat + a.nx;
+        for (int k = 0; k < nn; ++k)
+        {
+            S.nonzeros.PushBack(C(-1.0, 0.0));
+            S.columnIndices.PushBack(map[nb[k]]);
+        }
+        S.nonzeros.PushBack(diag);
+        S.columnIndices.PushBack(map[nat]);
+    }
+    S.rowOffsets.PushBack(S.nonzeros.Size());
+    SetOversample(a.oversample);
+    HMat2d<C> A(S, a.levels, a.rank, a.strong != 0, a.nx, a.ny);
+    std::vector<double> raw = ReadDoubles(a.x, (size_t)2 * N * a.nrhs);
+    Dense<C> P(N, a.nrhs), R;
+    for (int j = 0; j < a.nrhs; ++j)
+        for (int i = 0; i < N; ++i)
+            P.Set(i, j, C(raw[2 * (i + (size_t)j * N)], raw[2 * (i + (size_t)j * N) + 1]));
+    double t0 = Now();
+    int its = 0;
+    if (a.cmd == "cmatvec")
+        A.Multiply(C(1.0, 0.0), P, R);
+    else if (a.cmd == "chh")
+    {
+        HMat2d<C> B;
+        A.Multiply(C(1.0, 0.0), A, B);
+        B.Multiply(C(1.0, 0.0), P, R);
+    }
+    else if (a.cmd == "cschulz")
+    {
+        HMat2d<C> X;
+        X.CopyFrom(A);
+        X.SchulzInvert(a.iters, a.theta, a.conf, a.stopTol);
+        X.Multiply(C(1.0, 0.0), P, R);
+    }
+    else { fprintf(stderr, "unknown command %s\n", a.cmd.c_str()); return 2; }
+    const double seconds = Now() - t0;
+    std::vector<double> out((size_t)2 * N * a.nrhs);
+    for (int j = 0; j < a.nrhs; ++j)
+        for (int i = 0; i < N; ++i)
+        {
+            const C v = R.Get(i, j);
+            out[2 * (i + (size_t)j * N)] = v.real();
+            out[2 * (i + (size_t)j * N) + 1] = v.imag();
+        }
+    if (!a.out.empty()) WriteDoubles(a.out + ".bin", out);
+    printf("{\"cmd\": \"%s\", \"N\": %d, \"seconds\": %.9g, \"iterations\": %d}\n",
+           a.cmd.c_str(), N, seconds, its);
+    return 0;
+}
+
 int RunLcg(const DriverArgs& a)
 {
     // Draw `count` serial uniforms, then `count` Gaussians of a vector and a
@@ -370,6 +452,8 @@ int main(int argc, char* argv[])
         else if (k == "--theta") a.theta = atof(v);
         else if (k == "--conf") a.conf = atof(v);
         else if (k == "--stopTol") a.stopTol = atof(v);
+        else if (k == "--kwave") a.kwave = atof(v);
+        else if (k == "--absorption") a.absorption = atof(v);
         else if (k == "--coef") a.coef = v;
         else if (k == "--coefB") a.coefB = v;
         else if (k == "--x") a.x = v;
@@ -383,6 +467,7 @@ int main(int argc, char* argv[])
     try
     {
         if (a.cmd == "lcg") rc = RunLcg(a);
+        else if (a.cmd[0] == 'c') rc = RunComplex(a);
         else if (a.dim == 2) rc = Run<HMat2d<double> >(a);
         else rc = Run<HMat3d<double> >(a);
     }

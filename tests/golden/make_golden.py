@@ -7,6 +7,7 @@ touch the reference; the fixtures let the GPU tests check parity without it.
 
     python tests/golden/make_golden.py            # all cases
     python tests/golden/make_golden.py c1 ragged  # some cases
+    python tests/golden/make_golden.py cplx       # the complex-double case
 """
 from __future__ import annotations
 
@@ -106,6 +107,41 @@ def make_case(name, spec, tmp):
     print(name, "ok", sorted(out))
 
 
+# complex cases (HMat2d<std::complex<double>>, shifted Helmholtz-like operator)
+COMPLEX_CASES = {
+    "cplx": dict(sizes=(32, 32), levels=3, rank=12, oversample=4, kwave=6.0, seed=11, probes=2),
+}
+
+
+def make_complex_case(name, spec, tmp):
+    sizes = spec["sizes"]
+    N = int(np.prod(sizes))
+    rng = np.random.default_rng(spec["seed"])
+    k = spec["probes"]
+    P = rng.standard_normal((N, k)) + 1j * rng.standard_normal((N, k))
+    ppath = os.path.join(tmp, "cp.bin")
+    np.asfortranarray(P).T.copy().view(np.float64).tofile(ppath)   # column-major, interleaved
+    base = ["--nx", sizes[0], "--ny", sizes[1], "--levels", spec["levels"],
+            "--rank", spec["rank"], "--oversample", spec["oversample"],
+            "--kwave", spec["kwave"], "--x", ppath, "--nrhs", k]
+    out = dict(sizes=np.array(sizes), levels=spec["levels"], rank=spec["rank"],
+               oversample=spec["oversample"], kwave=spec["kwave"], probes=P)
+    o = os.path.join(tmp, "co")
+
+    def cmat(v):
+        return v.view(np.complex128).reshape(k, N).T.copy()
+
+    _, y = run(["cmatvec"] + base, o)
+    out["matvec"] = cmat(y)
+    _, y = run(["chh"] + base, o)
+    out["hh_AA"] = cmat(y)
+    info, y = run(["cschulz"] + base + ["--iters", -1, "--stopTol", 1e-8], o)
+    out["schulz_stop"] = cmat(y)
+    out["schulz_stop_seconds"] = info["seconds"]
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name, "ok", sorted(out))
+
+
 def make_lcg(tmp):
     o = os.path.join(tmp, "lcg")
     run(["lcg", "--count", 9], o)
@@ -117,11 +153,13 @@ def make_lcg(tmp):
 def main(argv):
     subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-j8"], check=True,
                    capture_output=True)
-    names = argv or list(CASES) + ["lcg"]
+    names = argv or list(CASES) + list(COMPLEX_CASES) + ["lcg"]
     with tempfile.TemporaryDirectory() as tmp:
         for n in names:
             if n == "lcg":
                 make_lcg(tmp)
+            elif n in COMPLEX_CASES:
+                make_complex_case(n, COMPLEX_CASES[n], tmp)
             else:
                 make_case(n, CASES[n], tmp)
 

@@ -84,3 +84,19 @@ def test_schulz_iterations(case, its):
     assert abs(trace[0] - fx[key + "_trace"][0]) < 1e-13 * trace[0]
     # fixed-rank truncation inside each H*H amplifies rounding differences
     assert relerr(O.multiply_dense(X, 1.0, fx["probes"]), fx[key]) < 1e-8
+
+
+def test_complex_fixture_against_dense():
+    """The reference's complex-double results (tests/golden/cplx.npz) against
+    dense complex algebra of the same operator: products exact, the Schulz
+    inverse within 1e-8 of the dense inverse on the probes."""
+    import numpy as np
+    from dmhm_b200 import operators as O
+    fx = load("cplx")
+    sizes = tuple(int(s) for s in fx["sizes"])
+    S = O.helmholtz(sizes, float(fx["kwave"]), int(fx["levels"]))
+    A = O.dense_from_sparse(S)
+    P = fx["probes"]
+    assert relerr(fx["matvec"], A @ P) < 1e-14
+    assert relerr(fx["hh_AA"], A @ (A @ P)) < 1e-14
+    assert relerr(fx["schulz_stop"], np.linalg.solve(A, P)) < 1e-8

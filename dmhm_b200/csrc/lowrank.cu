@@ -83,33 +83,43 @@ __device__ R block_sum(R v, R* red) {
 
 // In-place Householder QR (LAPACK dgeqr2 conventions: beta = -sign(alpha)
 // ||x||, v(1) = 1 implicit, tau = (beta - alpha) / beta; tau = 0 when the
-// column below the diagonal is zero).
+// column below the diagonal is zero).  Column c belongs to warp c % kW for
+// the whole factorization: the owner of column j has applied reflectors
+// 0..j-1 to it and forms reflector j with warp reductions only; one barrier
+// per column publishes it; every warp then applies it to its own columns.
 template <typename R>
 __device__ void cta_qr(R* A, int m, int n, int ld, R* tau, R* red) {
+    (void)red;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int kk = min(m, n);
     for (int j = 0; j < kk; ++j) {
         R* col = A + j + (long long)j * ld;
         const int len = m - j;
-        R s = 0;
-        for (int i = 1 + threadIdx.x; i < len; i += kT) s += col[i] * col[i];
-        s = block_sum(s, red);
-        const R alpha = col[0];
-        R t = 0, beta = alpha;
-        if (s != R(0)) {
-            beta = -r_copysign(r_sqrt(alpha * alpha + s), alpha);
-            t = (beta - alpha) / beta;
-            const R scal = R(1) / (alpha - beta);
-            for (int i = 1 + threadIdx.x; i < len; i += kT) col[i] *= scal;
+        if (warp == j % kW) {
+            __syncwarp();   // this warp's last update of column j used other lanes' rows
+            R s = 0;
+            for (int i = 1 + lane; i < len; i += 32) s += col[i] * col[i];
+            s = warp_sum(s);
+            const R alpha = col[0];
+            R t = 0, beta = alpha;
+            if (s != R(0)) {
+                beta = -r_copysign(r_sqrt(alpha * alpha + s), alpha);
+                t = (beta - alpha) / beta;
+                const R scal = R(1) / (alpha - beta);
+                for (int i = 1 + lane; i < len; i += 32) col[i] *= scal;
+            }
+            __syncwarp();
+            if (lane == 0) {
+                col[0] = beta;
+                tau[j] = t;
+            }
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            col[0] = beta;
-            tau[j] = t;
-        }
-        __syncthreads();
+        const R t = tau[j];
         if (t != R(0)) {
-            for (int c = j + 1 + warp; c < n; c += kW) {
+            // first column > j owned by this warp
+            int c = j + 1 + ((warp - (j + 1) % kW + kW) % kW);
+            for (; c < n; c += kW) {
                 R* cc = A + j + (long long)c * ld;
                 const R c0 = cc[0];
                 R w = 0;
@@ -121,23 +131,26 @@ __device__ void cta_qr(R* A, int m, int n, int ld, R* tau, R* red) {
                 for (int i = 1 + lane; i < len; i += 32) cc[i] -= tw * col[i];
             }
         }
-        __syncthreads();
     }
+    __syncthreads();
 }
 
-// B := Q B with Q = H_0 H_1 ... H_{kk-1} from cta_qr (B is m x p).
-// (arithmetic in R; B may be stored in another type)
+// B := Q B with Q = H_0 H_1 ... H_{kk-1} from cta_qr (B is m x p;
+// arithmetic in R, B may be stored in another type).  Column c of B is
+// updated by warp c % kW through all reflectors, so no barrier is needed
+// between them.
 template <typename R, typename RB>
 __device__ void cta_apply_q(const R* A, int m, int kk, int lda, const R* tau, RB* B, int p,
                             int ldb) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int j = kk - 1; j >= 0; --j) {
-        const R t = tau[j];
-        if (t == R(0)) continue;
-        const R* v = A + j + (long long)j * lda;
-        const int len = m - j;
-        for (int c = warp; c < p; c += kW) {
-            RB* bc = B + j + (long long)c * ldb;
+    for (int c = warp; c < p; c += kW) {
+        RB* bcol = B + (long long)c * ldb;
+        for (int j = kk - 1; j >= 0; --j) {
+            const R t = tau[j];
+            if (t == R(0)) continue;
+            const R* v = A + j + (long long)j * lda;
+            const int len = m - j;
+            RB* bc = bcol + j;
             const R b0 = (R)bc[0];
             R w = 0;
             for (int i = 1 + lane; i < len; i += 32) w += v[i] * (R)bc[i];
@@ -146,9 +159,10 @@ __device__ void cta_apply_q(const R* A, int m, int kk, int lda, const R* tau, RB
             __syncwarp();
             if (lane == 0) bc[0] = (RB)(b0 - tw);
             for (int i = 1 + lane; i < len; i += 32) bc[i] = (RB)((R)bc[i] - tw * v[i]);
+            __syncwarp();
         }
-        __syncthreads();
     }
+    __syncthreads();
 }
 
 __device__ __forceinline__ int rr_pos(int i, int step, int n) {

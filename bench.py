@@ -298,6 +298,9 @@ def gpu_arm(args):
     if not args.no_schulz:
         line["schulz"] = schulz_leg(local, rank == 0 and not args.no_cpu_baseline)
         line["schulz_modes"] = schulz_modes_leg(local)
+    if args.helmholtz_count > 0:
+        line["helmholtz_batch"] = helmholtz_batch_leg(local, args.helmholtz_count,
+                                                      args.helmholtz_max_side or None)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
@@ -698,6 +701,10 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-schulz", action="store_true")
+    # complex Helmholtz batch: a bounded sample by default (the full 48
+    # instances take tens of minutes: --helmholtz-count 48 --helmholtz-max-side 0)
+    ap.add_argument("--helmholtz-count", type=int, default=8)
+    ap.add_argument("--helmholtz-max-side", type=int, default=48)
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)

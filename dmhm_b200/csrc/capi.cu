@@ -253,6 +253,7 @@ int hm_context_destroy(hm_context ctx) {
         // stream goes away
         ctx->c.layouts.clear();
         ctx->c.hh_cache.reset();
+        for (auto& b : ctx->c.scratch_bufs) b.reset();
         ctx->c.counters.reset();
         ctx->c.errword.reset();
         cudaStreamSynchronize(ctx->c.stream);

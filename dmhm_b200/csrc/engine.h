@@ -82,6 +82,11 @@ struct Context {
     // bucket), 1 tcgen05 (at most 64 columns, ranks <= 256), 2 mma.sync.
     int tf32_kernel = 0;
     std::map<std::pair<uint64_t, int>, int> tf32_tuned;
+    // Grow-only device scratch reused by consecutive H*H products on this
+    // context's stream (W arena, sampling arena, state slots, rounding work):
+    // a product's kernels finish before the next product's start.
+    double* scratch(int slot, long long n);
+    DeviceBuffer<double> scratch_bufs[4];
     // Device word set by kernels whose bounded waits gave up (zero = fine).
     int* error_word();
     DeviceBuffer<int> errword;

@@ -714,11 +714,8 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
                 break;
         }
     }
-    DeviceBuffer<double> warena, sarena;
-    warena.allocate((size_t)std::max<long long>(wa.used, 2), st);
-    sarena.allocate((size_t)std::max<long long>(sa.used, 2), st);
-    double* W0 = warena.get();
-    double* S0 = sarena.get();
+    double* W0 = ctx.scratch(0, wa.used);
+    double* S0 = ctx.scratch(1, sa.used);
     for (WTask& t : P.w) {
         if (t.u_off >= 0) t.U = W0 + t.u_off;
         if (t.v_off >= 0) t.V = W0 + t.v_off;
@@ -964,7 +961,8 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
     const bool a_is_b = A.data.get() == B.data.get();
     std::shared_ptr<BlockCache> bc = plan->blocks;
     if (bc && (bc->tol != ctx.compression_tol || bc->a_is_b != a_is_b)) bc.reset();
-    DeviceBuffer<double> parena, wbuf;
+    double* parena = nullptr;   // state slots (scratch 2)
+    double* wbuf = nullptr;     // rounding work (scratch 3)
     DeviceBuffer<int> rk;
     if (dyn) rk.allocate(std::max<size_t>(1, P.lops.ops.size()), st);
     auto bases_now = [&]() {
@@ -973,17 +971,17 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
         b.d[1] = const_cast<double*>(A.data.get());
         b.d[2] = const_cast<double*>(B.data.get());
         b.d[3] = C.data.get();
-        b.d[4] = parena.get();
+        b.d[4] = parena;
         b.d[5] = c_old_data.get();
-        b.d[6] = wbuf.get();
+        b.d[6] = wbuf;
         b.i[0] = rk.get();
         b.i[1] = kept.get();
         return b;
     };
     if (bc) {
         HostScope replay(ctx, "hh_block_lists_replayed");
-        parena.allocate((size_t)std::max<long long>(bc->pa_used, 2), st);
-        if (bc->rounds.nw > 0) wbuf.allocate((size_t)std::max<long long>(bc->wk_used, 2), st);
+        parena = ctx.scratch(2, bc->pa_used);
+        if (bc->rounds.nw > 0) wbuf = ctx.scratch(3, bc->wk_used);
     } else {
         Arena pa, wk;
         std::vector<long long> slot0(S.blocks.size(), -1), slot1(S.blocks.size(), -1);
@@ -999,8 +997,8 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
                 slot1[c] = pa.take((long long)(Cb.m + Cb.n) * mr);
             }
         }
-        parena.allocate((size_t)std::max<long long>(pa.used, 2), st);
-        double* P0 = parena.get();
+        parena = ctx.scratch(2, pa.used);
+        double* P0 = parena;
         std::vector<RoundOp> rops;
         std::vector<int> rbegin{0};
         std::vector<long long> rwork;   // per op: offset into the work arena
@@ -1110,8 +1108,8 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
             }
         }
         if (!rops.empty()) {
-            wbuf.allocate((size_t)std::max<long long>(wk.used, 2), st);
-            for (size_t i = 0; i < rops.size(); ++i) rops[i].work = wbuf.get() + rwork[i];
+            wbuf = ctx.scratch(3, wk.used);
+            for (size_t i = 0; i < rops.size(); ++i) rops[i].work = wbuf + rwork[i];
         }
 
         // position-independent copy for the cache
@@ -1120,9 +1118,9 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
         rel.add(1, A.data.get(), A.total);
         rel.add(2, B.data.get(), B.total);
         rel.add(3, C.data.get(), C.total);
-        rel.add(4, parena.get(), pa.used);
+        rel.add(4, parena, pa.used);
         rel.add(5, c_old_data.get(), (long long)c_old_data.size());
-        rel.add(6, wbuf.get(), wk.used);
+        rel.add(6, wbuf, wk.used);
         rel.add(0, rk.get(), (long long)rk.size());
         rel.add(1, kept.get(), (long long)kept.size());
         std::vector<RoundOp> trops = rops;

@@ -6,6 +6,7 @@
 // are laid out in depth-first order so that a subtree's data is contiguous.
 #include <algorithm>
 
+#include <deque>
 #include <map>
 #include <mutex>
 #include <cstring>
@@ -54,16 +55,29 @@ void HMatrix::upload_table() {
 
 namespace {
 
-// Pinned staging ring of one stream: copies take [head, head + bytes); when
-// the ring is full the host waits for the stream once (all copies that read
-// the ring are then done) and starts over.
+// Pinned staging ring of one stream: copies take [head, head + bytes) and
+// record an event after their cudaMemcpyAsync; before a range of the ring is
+// written again, the host waits for the events of the copies that read it
+// (normally long done), never for the whole stream.
+struct StagedCopy {
+    size_t begin, end;
+    cudaEvent_t done;
+};
 struct StagingRing {
     char* buf = nullptr;
     size_t cap = 0, head = 0;
+    std::deque<StagedCopy> pending;   // in ring order
+    std::vector<cudaEvent_t> spare;
 };
 constexpr size_t kStagingBytes = size_t(128) << 20;
 std::mutex g_staging_mu;
 std::map<cudaStream_t, StagingRing> g_staging;
+
+void retire_front(StagingRing& R) {
+    HMB_CUDA(cudaEventSynchronize(R.pending.front().done));
+    R.spare.push_back(R.pending.front().done);
+    R.pending.pop_front();
+}
 
 }  // namespace
 
@@ -86,13 +100,36 @@ void staged_h2d(void* dst, const void* src, size_t bytes, cudaStream_t s) {
     }
     const size_t need = (bytes + 255) & ~size_t(255);
     if (R.head + need > R.cap) {
-        HMB_CUDA(cudaStreamSynchronize(s));
+        // the tail [head, cap) is skipped this lap: copies of earlier laps
+        // still pending there are the oldest and are retired first
+        while (!R.pending.empty() && R.pending.front().begin >= R.head) retire_front(R);
         R.head = 0;
     }
+    // copies of the previous lap that read the range about to be written
+    while (!R.pending.empty() && R.pending.front().begin < R.head + need &&
+           R.pending.front().end > R.head)
+        retire_front(R);
     char* p = R.buf + R.head;
     std::memcpy(p, src, bytes);
-    R.head += need;
     HMB_CUDA(cudaMemcpyAsync(dst, p, bytes, cudaMemcpyHostToDevice, s));
+    cudaEvent_t ev;
+    if (!R.spare.empty()) {
+        ev = R.spare.back();
+        R.spare.pop_back();
+    } else {
+        HMB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    }
+    HMB_CUDA(cudaEventRecord(ev, s));
+    R.pending.push_back({R.head, R.head + need, ev});
+    R.head += need;
+    // retire copies that are already done (keeps the pending list short)
+    for (int i = 0; i < 8 && R.pending.size() > 1; ++i) {
+        const cudaError_t q = cudaEventQuery(R.pending.front().done);
+        if (q == cudaErrorNotReady) break;
+        HMB_CUDA(q);
+        R.spare.push_back(R.pending.front().done);
+        R.pending.pop_front();
+    }
 }
 
 // Drops the staging ring of a stream that is about to be destroyed.
@@ -101,6 +138,8 @@ void release_staging(cudaStream_t s) {
     auto it = g_staging.find(s);
     if (it == g_staging.end()) return;
     cudaStreamSynchronize(s);
+    for (const StagedCopy& c : it->second.pending) cudaEventDestroy(c.done);
+    for (cudaEvent_t e : it->second.spare) cudaEventDestroy(e);
     if (it->second.buf) cudaFreeHost(it->second.buf);
     g_staging.erase(it);
 }

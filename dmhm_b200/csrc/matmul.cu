@@ -1235,6 +1235,13 @@ int* Context::error_word() {
     return errword.get();
 }
 
+double* Context::scratch(int slot, long long n) {
+    DeviceBuffer<double>& b = scratch_bufs[slot];
+    n = std::max<long long>(n, 2);
+    if ((long long)b.size() < n) b.allocate((size_t)(n + n / 4), stream);
+    return b.get();
+}
+
 int* Context::zeroed_counters(long long n) {
     if (n > counters_cap) {
         const long long cap = std::max<long long>(n, 2 * counters_cap);

@@ -419,6 +419,39 @@ int hm_create_from_csr_complex(hm_context ctx, int dim, const int* sizes, int nu
     });
 }
 
+int hm_packed_size(hm_matrix h, size_t* bytes) {
+    return guarded([&] {
+        HMB_REQUIRE(h && bytes, HM_ERR_ARGUMENT, "NULL argument");
+        owner_of(h);
+        *bytes = packed_size(h->h);
+    });
+}
+
+int hm_pack(hm_matrix h, void* buffer, size_t capacity, size_t* written) {
+    return guarded([&] {
+        HMB_REQUIRE(h && buffer, HM_ERR_ARGUMENT, "NULL argument");
+        owner_of(h);
+        const size_t n = pack(h->h, static_cast<unsigned char*>(buffer), capacity);
+        if (written) *written = n;
+    });
+}
+
+int hm_unpack(hm_context ctx, int dim, const void* buffer, size_t size, hm_matrix* out) {
+    return guarded([&] {
+        HMB_REQUIRE(ctx && buffer && out, HM_ERR_ARGUMENT, "NULL argument");
+        *out = nullptr;
+        HMB_CUDA(cudaSetDevice(ctx->c.device));
+        auto* m = new_handle(ctx);
+        try {
+            unpack(ctx->c, dim, static_cast<const unsigned char*>(buffer), size, m->h);
+        } catch (...) {
+            delete_handle(m);
+            throw;
+        }
+        *out = m;
+    });
+}
+
 int hm_is_complex(hm_matrix h, int* is_complex) {
     return guarded([&] {
         HMB_REQUIRE(h && is_complex, HM_ERR_ARGUMENT, "NULL argument");

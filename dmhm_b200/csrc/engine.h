@@ -216,6 +216,11 @@ void multiply_dense_tf32(HMatrix& H, double alpha, const double* B, int ldb, dou
 void multiply_dense_complex(HMatrix& H, int op, double ar, double ai, const double* B, int ldb,
                             double br, double bi, double* C, int ldc, int nrhs);
 
+// The reference's Pack / Unpack wire format (pack.cpp).
+size_t packed_size(const HMatrix& H);
+size_t pack(const HMatrix& H, unsigned char* out, size_t cap);
+void unpack(Context& ctx, int dim, const unsigned char* buf, size_t size, HMatrix& H);
+
 // Device kernels driven from the host side (launchers).
 void launch_fill_random(Context& ctx, HMatrix& H);
 

@@ -279,6 +279,30 @@ class _HMatBase:
         """SampleRank (hmat2d.hpp:32-33)."""
         return approxRank + self.ctx.oversample()
 
+    # -- wire format (src/HMat2d/Pack-incl.hpp) -------------------------------
+    def PackedSize(self) -> int:
+        n = C.c_size_t()
+        check(lib().hm_packed_size(self._h, C.byref(n)))
+        return n.value
+
+    def Pack(self) -> bytes:
+        """The reference's byte layout of this H-matrix (Pack)."""
+        n = self.PackedSize()
+        buf = C.create_string_buffer(n)
+        w = C.c_size_t()
+        check(lib().hm_pack(self._h, buf, n, C.byref(w)))
+        return buf.raw[:w.value]
+
+    @classmethod
+    def Unpack(cls, packed: bytes, ctx: Optional[Context] = None):
+        """H-matrix from the reference's byte layout (the HMat2d(const
+        Vector<byte>&) constructor)."""
+        ctx = _ctx(ctx)
+        buf = C.create_string_buffer(bytes(packed), len(packed))
+        h = C.c_void_p()
+        check(lib().hm_unpack(ctx.handle, cls.dim, buf, len(packed), C.byref(h)))
+        return cls(ctx=ctx, _handle=h)
+
     def SetToRandom(self):
         """SetToRandom (src/HMat2d/SetToRandom-incl.hpp:14-55)."""
         check(lib().hm_set_to_random(self._h))

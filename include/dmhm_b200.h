@@ -109,6 +109,20 @@ HM_API int hm_create_from_csr_complex(hm_context ctx, int dim, const int* sizes,
                                       const int64_t* row_offsets, const int32_t* col_indices,
                                       const double* values, hm_matrix* out);
 HM_API int hm_is_complex(hm_matrix h, int* is_complex);
+
+/*
+ * The reference's wire format: PackedSize / Pack / Unpack and the
+ * HMat2d(const Vector<byte>&) constructor (src/HMat2d/Pack-incl.hpp:16-364;
+ * HMat3d: src/HMat3d/Pack-incl.hpp).  Byte-identical to what the reference
+ * writes on the same host (native-endian ints, one-byte bools, column-major
+ * doubles), so matrices move between the two in both directions.
+ * hm_unpack builds the block structure from the header (dim = 2 for HMat2d,
+ * 3 for HMat3d) and rejects a block tree that does not match it, symmetric
+ * matrices (NODE_SYMMETRIC) and non-root sub-matrices.  Real matrices only.
+ */
+HM_API int hm_packed_size(hm_matrix h, size_t* bytes);
+HM_API int hm_pack(hm_matrix h, void* buffer, size_t capacity, size_t* written);
+HM_API int hm_unpack(hm_context ctx, int dim, const void* buffer, size_t size, hm_matrix* out);
 /*
  * Complex Multiply / TransposeMultiply / AdjointMultiply against dense
  * blocks (src/HMat2d/MultiplyDense-incl.hpp:12-260 for Scalar =

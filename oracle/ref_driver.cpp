@@ -304,6 +304,36 @@ int Run(const DriverArgs& a)
         std::vector<double> tr = trace;
         WriteDoubles(a.out + ".trace.bin", tr);
     }
+    else if (a.cmd == "pack")
+    {
+        // the reference's wire format (src/HMat2d/Pack-incl.hpp:37-61);
+        // bytes written to <out>.pack
+        std::vector<byte> packed;
+        Vector<byte> buf;
+        A->Pack(buf);
+        packed.assign(&buf[0], &buf[0] + buf.Size());
+        FILE* f = fopen((a.out + ".pack").c_str(), "wb");
+        if (!f) { fprintf(stderr, "cannot write pack\n"); return 2; }
+        fwrite(&packed[0], 1, packed.size(), f);
+        fclose(f);
+        extraInt = (int)packed.size();
+    }
+    else if (a.cmd == "unpack_matvec")
+    {
+        // Unpack <coefB> (raw bytes of a packed matrix) and multiply the probes
+        FILE* f = fopen(a.coefB.c_str(), "rb");
+        if (!f) { fprintf(stderr, "cannot open %s\n", a.coefB.c_str()); return 2; }
+        std::vector<byte> raw;
+        int ch;
+        while ((ch = fgetc(f)) != EOF) raw.push_back((byte)ch);
+        fclose(f);
+        Vector<byte> buf(raw.size());
+        for (size_t i = 0; i < raw.size(); ++i) buf[i] = raw[i];
+        HMat U;
+        U.Unpack(buf);
+        std::vector<double> P = ReadDoubles(a.x, (size_t)N * a.nrhs);
+        ApplyToProbes(U, P, N, a.nrhs, result);
+    }
     else if (a.cmd == "norm")
     {
         double t0 = Now();

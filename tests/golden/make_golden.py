@@ -142,6 +142,45 @@ def make_complex_case(name, spec, tmp):
     print(name, "ok", sorted(out))
 
 
+# the reference's Pack wire format: (case, SetToRandom?)
+PACK_CASES = (("ragged", 1), ("c3d", 0))
+
+
+def make_pack(tmp):
+    """Pack bytes written by the reference for two fixture matrices (a
+    SetToRandom 2-D matrix and a sparse-built 3-D one), with the reference's
+    own matvec of the packed matrices' Unpack on the fixture probes."""
+    out = {}
+    for name, random in PACK_CASES:
+        spec = CASES[name]
+        sizes = spec["sizes"]
+        dim = len(sizes)
+        N = int(np.prod(sizes))
+        rng = np.random.default_rng(spec["seed"])
+        coef = 1.0 + rng.random(N)
+        rng.random(N)                                  # coefB
+        P = rng.standard_normal((N, spec["probes"]))
+        cpath, ppath = os.path.join(tmp, "pc.bin"), os.path.join(tmp, "pp.bin")
+        coef.tofile(cpath)
+        np.asfortranarray(P).T.copy().tofile(ppath)
+        base = ["--dim", dim, "--nx", sizes[0], "--ny", sizes[1],
+                "--nz", sizes[2] if dim == 3 else 1, "--levels", spec["levels"],
+                "--rank", spec["rank"], "--oversample", spec["oversample"],
+                "--strong", spec["strong"], "--coef", cpath, "--random", random]
+        o = os.path.join(tmp, "pk")
+        r = subprocess.run([DRIVER, "pack"] + [str(a) for a in base] + ["--out", o],
+                           capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(r.stderr)
+        packed = np.fromfile(o + ".pack", dtype=np.uint8)
+        _, y = run(["unpack_matvec"] + base + ["--coefB", o + ".pack", "--x", ppath,
+                                                "--nrhs", spec["probes"]], o)
+        out[name + "_pack"] = packed
+        out[name + "_unpack_matvec"] = y.reshape(spec["probes"], N).T.copy()
+    np.savez_compressed(os.path.join(HERE, "pack.npz"), **out)
+    print("pack ok", sorted(out))
+
+
 def make_lcg(tmp):
     o = os.path.join(tmp, "lcg")
     run(["lcg", "--count", 9], o)
@@ -153,11 +192,13 @@ def make_lcg(tmp):
 def main(argv):
     subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-j8"], check=True,
                    capture_output=True)
-    names = argv or list(CASES) + list(COMPLEX_CASES) + ["lcg"]
+    names = argv or list(CASES) + list(COMPLEX_CASES) + ["lcg", "pack"]
     with tempfile.TemporaryDirectory() as tmp:
         for n in names:
             if n == "lcg":
                 make_lcg(tmp)
+            elif n == "pack":
+                make_pack(tmp)
             elif n in COMPLEX_CASES:
                 make_complex_case(n, COMPLEX_CASES[n], tmp)
             else:

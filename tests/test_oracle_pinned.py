@@ -100,3 +100,43 @@ def test_complex_fixture_against_dense():
     assert relerr(fx["matvec"], A @ P) < 1e-14
     assert relerr(fx["hh_AA"], A @ (A @ P)) < 1e-14
     assert relerr(fx["schulz_stop"], np.linalg.solve(A, P)) < 1e-8
+
+
+def _walk_pack(raw, pos, H):
+    """Parses one block of the reference's Pack layout
+    (src/HMat2d/Pack-incl.hpp:183-240) against the oracle's block tree and
+    returns the position after it."""
+    import struct
+    t = struct.unpack_from("<i", raw, pos)[0]
+    pos += 4
+    if H.kind == O.NODE:
+        assert t == 0
+        for c in H.children:
+            pos = _walk_pack(raw, pos, c)
+    elif H.kind == O.LOW_RANK:
+        assert t == 2
+        r = struct.unpack_from("<i", raw, pos)[0]
+        pos += 4 + 8 * (H.height + H.width) * r
+    else:
+        assert t == 3
+        assert struct.unpack_from("<i", raw, pos)[0] == 0      # GENERAL
+        pos += 4 + 8 * H.height * H.width
+    return pos
+
+
+@pytest.mark.parametrize("case", ["ragged", "c3d"])
+def test_pack_fixture_layout(case):
+    """The reference's Pack bytes follow the documented layout over the
+    oracle's block tree and are consumed exactly."""
+    import struct
+    pk = load("pack")
+    fx = load(case)
+    raw = pk[case + "_pack"].tobytes()
+    dim = len(fx["sizes"])
+    L, r = struct.unpack_from("<ii", raw, 0)
+    assert (L, r) == (int(fx["levels"]), int(fx["rank"]))
+    header = 4 * 4 + 2 + 4 * 4 * dim     # 4 ints, 2 bools, per axis 2 sizes + 2 coordinates
+    # PackedSize counts one int more than the header holds: 4 zero bytes end
+    # the buffer (Pack-incl.hpp:32)
+    end = _walk_pack(raw, header, oracle_hmat(fx))
+    assert end + 4 == len(raw) and raw[end:] == bytes(4)

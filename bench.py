@@ -264,9 +264,13 @@ def gpu_arm(args):
     kbytes = kernel_bytes(kname, census, N, NRHS, H)
     achieved = kbytes / (per_launch_ms * 1e-3) / 1e9
 
-    # end to end through the C ABI with host buffers
-    Xp = np.asfortranarray(Xh)
-    Yp = np.zeros((N, NRHS), order="F")
+    # end to end through the C ABI with host buffers (pinned host memory,
+    # column-major N x k: the transposed view of a pinned k x N tensor)
+    Xpin = torch.empty((NRHS, N), dtype=torch.float64, pin_memory=True)
+    Ypin = torch.zeros((NRHS, N), dtype=torch.float64, pin_memory=True)
+    Xp = Xpin.numpy().T
+    Yp = Ypin.numpy().T
+    Xp[:] = Xh
     e2e_steps = max(3, args.steps // 2)
     H.Multiply(1.0, Xp)
     ctx.synchronize()

@@ -199,6 +199,27 @@ class HMatBase {
         Check(hm_multiply_hmat_update(Need(), alpha, B.Need(), beta, C.Need()));
     }
 
+    // Wire format (PackedSize / Pack / Unpack, src/HMat2d/Pack-incl.hpp:27-153):
+    // the reference's bytes, readable by the reference's Unpack and back.
+    std::size_t PackedSize() const {
+        std::size_t n = 0;
+        Check(hm_packed_size(Need(), &n));
+        return n;
+    }
+    std::size_t Pack(std::vector<unsigned char>& packed) const {
+        packed.resize(PackedSize());
+        std::size_t written = 0;
+        Check(hm_pack(Need(), packed.data(), packed.size(), &written));
+        return written;
+    }
+    std::size_t Unpack(const std::vector<unsigned char>& packed) {
+        hm_matrix h = nullptr;
+        Check(hm_unpack(Context(), Dim, packed.data(), packed.size(), &h));
+        if (h_) hm_destroy(h_);
+        h_ = h;
+        return packed.size();
+    }
+
     void CopyFrom(const HMatBase& B) { Check(hm_copy(B.Need(), &h_)); }
     void AdjointFrom(const HMatBase& B) { Check(hm_transpose(B.Need(), &h_)); }
     void TransposeFrom(const HMatBase& B) { Check(hm_transpose(B.Need(), &h_)); }
@@ -249,6 +270,16 @@ class HMat2d : public HMatBase<Scalar, 2> {
                       Scalar stopTol = 1e-4) {
         Check(hm_schulz_invert(this->Need(), numIterations, theta, confidence, stopTol, nullptr,
                                nullptr, 0, nullptr));
+    }
+    // Mixed-precision SchulzInvert (no reference counterpart): iterations in
+    // the low-precision phase while ||I - X A|| > mixedSwitch, then FP64;
+    // returns the number of low-precision iterations.
+    int SchulzInvertMixed(int numIterations, Scalar theta = 1.5, Scalar confidence = 6,
+                          Scalar stopTol = 1e-4, Scalar mixedSwitch = 0.1) {
+        int its = 0, low = 0;
+        Check(hm_schulz_invert_mixed(this->Need(), numIterations, theta, confidence, stopTol,
+                                     mixedSwitch, &its, &low, nullptr, 0, nullptr));
+        return low;
     }
 };
 

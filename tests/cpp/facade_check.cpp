@@ -90,6 +90,16 @@ int main(int argc, char** argv) {
     X.Multiply(1.0, B, Cd);
     write_bin(dir + "/schulz3.bin", Cd.LockedBuffer(), (size_t)N * k);
     std::printf("norm estimate %.17g\n", hmat_tools::EstimateTwoNorm(A, 1.5, 6.0));
+    // wire format round trip: X packed, unpacked into a fresh matrix, packed again
+    std::vector<unsigned char> p1, p2;
+    X.Pack(p1);
+    HMat2d<double> Y;
+    Y.Unpack(p1);
+    Y.Pack(p2);
+    if (p1 != p2 || p1.size() != X.PackedSize()) {
+        std::fprintf(stderr, "pack round trip differs\n");
+        return 1;
+    }
     Finalize();
     return 0;
 }

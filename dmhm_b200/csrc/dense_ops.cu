@@ -90,10 +90,13 @@ __device__ void gemm_tile(const GemmOp& op, int tile, double (*sA)[65], double (
 // One CTA per (op, 64x64 output tile).
 __global__ void __launch_bounds__(kT)
 gemm_ops_kernel(const GemmOp* __restrict__ ops, const int* __restrict__ tile_op,
-                const int* __restrict__ tile_id) {
+                const int* __restrict__ tile_id, const RelocBases bases) {
     __shared__ double sA[16][65];
     __shared__ double sB[16][65];
-    const GemmOp op = ops[tile_op[blockIdx.x]];
+    GemmOp op = ops[tile_op[blockIdx.x]];
+    op.A = reloc(op.A, bases);
+    op.B = reloc(op.B, bases);
+    op.C = reloc(op.C, bases);
     gemm_tile(op, tile_id[blockIdx.x], sA, sB);
 }
 
@@ -118,7 +121,8 @@ gemm_worker_kernel(const GemmOp* __restrict__ ops, const int* __restrict__ begin
 
 }  // namespace
 
-void launch_gemm_ops(Context& ctx, const std::vector<GemmOp>& ops, const char* name) {
+void upload_gemm_tiles(Context& ctx, const std::vector<GemmOp>& ops, GemmTileList& out) {
+    out.ntiles = 0;
     std::vector<int> tile_op, tile_id;
     for (size_t o = 0; o < ops.size(); ++o) {
         const GemmOp& g = ops[o];
@@ -130,15 +134,25 @@ void launch_gemm_ops(Context& ctx, const std::vector<GemmOp>& ops, const char* n
         }
     }
     if (tile_op.empty()) return;
-    DeviceBuffer<GemmOp> d_ops;
-    DeviceBuffer<int> d_to, d_ti;
-    d_ops.upload(ops, ctx.stream);
-    d_to.upload(tile_op, ctx.stream);
-    d_ti.upload(tile_id, ctx.stream);
+    out.ops.upload(ops, ctx.stream);
+    out.tile_op.upload(tile_op, ctx.stream);
+    out.tile_id.upload(tile_id, ctx.stream);
+    out.ntiles = (int)tile_op.size();
+}
+
+void launch_gemm_tiles(Context& ctx, const GemmTileList& L, const RelocBases& bases,
+                       const char* name) {
+    if (L.ntiles == 0) return;
     LaunchScope ls(ctx, name);
-    gemm_ops_kernel<<<(unsigned)tile_op.size(), kT, 0, ctx.stream>>>(d_ops.get(), d_to.get(),
-                                                                     d_ti.get());
+    gemm_ops_kernel<<<(unsigned)L.ntiles, kT, 0, ctx.stream>>>(L.ops.get(), L.tile_op.get(),
+                                                               L.tile_id.get(), bases);
     HMB_CHECK_LAUNCH();
+}
+
+void launch_gemm_ops(Context& ctx, const std::vector<GemmOp>& ops, const char* name) {
+    GemmTileList L;
+    upload_gemm_tiles(ctx, ops, L);
+    launch_gemm_tiles(ctx, L, RelocBases{}, name);
 }
 
 void upload_gemm_list(Context& ctx, const std::vector<GemmOp>& ops, const std::vector<int>& begin,

@@ -19,6 +19,16 @@ struct GemmOp {
 
 // Launches all ops in one kernel; ops must write disjoint C matrices.
 void launch_gemm_ops(Context& ctx, const std::vector<GemmOp>& ops, const char* name);
+// The same from a device-resident list (one CTA per 64 x 64 tile of every
+// op) whose pointers may be tagged offsets (reloc.h).
+struct GemmTileList {
+    DeviceBuffer<GemmOp> ops;
+    DeviceBuffer<int> tile_op, tile_id;
+    int ntiles = 0;
+};
+void upload_gemm_tiles(Context& ctx, const std::vector<GemmOp>& ops, GemmTileList& out);
+void launch_gemm_tiles(Context& ctx, const GemmTileList& L, const RelocBases& bases,
+                       const char* name);
 
 // One CTA per worker w running ops [begin[w], begin[w+1]) in order (ops of one
 // worker may update the same C); different workers write disjoint C.

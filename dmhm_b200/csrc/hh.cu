@@ -469,6 +469,8 @@ std::vector<double> probe_errors(Context& ctx, const Structure& S, const HMatrix
 struct BlockCache {
     RoundList rounds;
     GemmList gemms;
+    GemmTileList leaf1, leaf2;   // leaf products (bases: 0 W arena, 1 A, 2 B)
+    bool leaves_cached = false;
     long long pa_used = 0, wk_used = 0;
     double tol = 0.0;
     bool a_is_b = false;
@@ -480,6 +482,7 @@ struct SymPlan {
     PerBlock<DOp> dops;
     uint64_t serial_steps = 0;
     std::vector<int> crank, state_rank, op_kind;
+    std::vector<int> k0, kq0;   // plain sample counts per task
     std::shared_ptr<BlockCache> blocks;
 };
 
@@ -570,6 +573,12 @@ std::shared_ptr<SymPlan> make_plan(const HMatrix& A, const HMatrix& B, const HMa
         crank[c] = rank;
     }
     plan->w = std::move(P.w);
+    plan->k0.resize(plan->w.size());
+    plan->kq0.resize(plan->w.size());
+    for (size_t i = 0; i < plan->w.size(); ++i) {
+        plan->k0[i] = plan->w[i].k;
+        plan->kq0[i] = plan->w[i].kq;
+    }
     plan->lops = std::move(P.lops);
     plan->dops = std::move(P.dops);
     return plan;
@@ -636,14 +645,22 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
     std::unique_ptr<HostScope> hs(new HostScope(ctx, "hh_symbolic"));
     const std::shared_ptr<SymPlan> plan = get_plan(ctx, A, B, C, alpha, beta, fresh, maxRankC);
     hs.reset(new HostScope(ctx, "hh_plan_copy"));
+    // The plan's task list is used in place: every per-product field
+    // (generator positions, arena offsets, pointers, sample counts) is
+    // rewritten below before it is read; sample counts start from the plan's.
     struct PlanView {
-        std::vector<WTask> w;
+        std::vector<WTask>& w;
         const PerBlock<LOp>& lops;
         const PerBlock<DOp>& dops;
     } P{plan->w, plan->lops, plan->dops};
-    // generator positions of the samples, from this call's starting state
-    for (WTask& t : P.w)
-        if (t.type == W_HH) t.omega = lcg_skip_host(ctx.serial_state, t.omega_steps);
+    for (size_t i = 0; i < P.w.size(); ++i) {
+        WTask& t = P.w[i];
+        if (t.type != W_HH) continue;
+        // generator positions of the samples, from this call's starting state
+        t.omega = lcg_skip_host(ctx.serial_state, t.omega_steps);
+        t.k = plan->k0[i];
+        t.kq = plan->kq0[i];
+    }
     const uint64_t serial_after = lcg_skip_host(ctx.serial_state, plan->serial_steps);
     const std::vector<int>& crank = plan->crank;
     const std::vector<int>& state_rank = plan->state_rank;
@@ -905,7 +922,20 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
 
     hs.reset(new HostScope(ctx, "hh_leaf_lists"));
     // ---------------- leaf products ----------------
-    {
+    // Cached with the plan's block lists (position-independent, reloc.h):
+    // they depend on the plan and on whether A and B are one matrix.
+    const bool a_is_b = A.data.get() == B.data.get();
+    std::shared_ptr<BlockCache> bc = plan->blocks;
+    if (bc && (bc->tol != ctx.compression_tol || bc->a_is_b != a_is_b)) bc.reset();
+    RelocBases leaf_bases{};
+    leaf_bases.d[0] = W0;
+    leaf_bases.d[1] = const_cast<double*>(A.data.get());
+    leaf_bases.d[2] = const_cast<double*>(B.data.get());
+    std::unique_ptr<GemmTileList> pending_leaf1, pending_leaf2;
+    if (bc && bc->leaves_cached) {
+        launch_gemm_tiles(ctx, bc->leaf1, leaf_bases, "leaf_products");
+        launch_gemm_tiles(ctx, bc->leaf2, leaf_bases, "leaf_products");
+    } else {
         std::vector<GemmOp> g1, g2;
         for (const WTask& t : P.w) {
             const Block& Ba = S.blocks[t.a];
@@ -946,8 +976,26 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
                     break;
             }
         }
-        launch_gemm_ops(ctx, g1, "leaf_products");
-        launch_gemm_ops(ctx, g2, "leaf_products");
+        // position-independent copies; kept once the block lists are cached
+        Relocator rel;
+        rel.add(0, W0, wa.used);
+        rel.add(1, A.data.get(), A.total);
+        rel.add(2, B.data.get(), B.total);
+        std::vector<GemmOp> t1 = g1, t2 = g2;
+        bool ok = true;
+        for (GemmOp& g : t1) ok = ok && rel.tag(g.A) && rel.tag(g.B) && rel.tag(g.C);
+        for (GemmOp& g : t2) ok = ok && rel.tag(g.A) && rel.tag(g.B) && rel.tag(g.C);
+        if (ok) {
+            pending_leaf1.reset(new GemmTileList);
+            pending_leaf2.reset(new GemmTileList);
+            upload_gemm_tiles(ctx, t1, *pending_leaf1);
+            upload_gemm_tiles(ctx, t2, *pending_leaf2);
+            launch_gemm_tiles(ctx, *pending_leaf1, leaf_bases, "leaf_products");
+            launch_gemm_tiles(ctx, *pending_leaf2, leaf_bases, "leaf_products");
+        } else {   // a pointer outside the registered buffers: run once, uncached
+            launch_gemm_ops(ctx, g1, "leaf_products");
+            launch_gemm_ops(ctx, g2, "leaf_products");
+        }
     }
 
     hs.reset(new HostScope(ctx, "hh_block_lists"));
@@ -958,9 +1006,6 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
     // last operation writes into C.  The lists depend only on the plan (and
     // the truncation tolerance): built once, cached with it, then replayed.
     const bool dyn = ctx.compression_tol > 0.0;
-    const bool a_is_b = A.data.get() == B.data.get();
-    std::shared_ptr<BlockCache> bc = plan->blocks;
-    if (bc && (bc->tol != ctx.compression_tol || bc->a_is_b != a_is_b)) bc.reset();
     double* parena = nullptr;   // state slots (scratch 2)
     double* wbuf = nullptr;     // rounding work (scratch 3)
     DeviceBuffer<int> rk;
@@ -1139,6 +1184,11 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
         bc->wk_used = wk.used;
         bc->tol = ctx.compression_tol;
         bc->a_is_b = a_is_b;
+        if (pending_leaf1) {
+            bc->leaf1 = std::move(*pending_leaf1);
+            bc->leaf2 = std::move(*pending_leaf2);
+            bc->leaves_cached = true;
+        }
         // lists that point outside the registered buffers run once, uncached
         if (ok) plan->blocks = bc;
         else HostScope uncached(ctx, "hh_block_lists_uncached");

@@ -58,6 +58,7 @@ SIGNATURES = {
     "hm_create_from_csr_complex": [_P, _I, _PI, _I, _I, _I, _PI64, _PI32, _PD, C.POINTER(_P)],
     "hm_is_complex": [_P, _PI],
     "hm_packed_size": [_P, C.POINTER(C.c_size_t)],
+    "hm_low_rank_product": [_P, _I, _D, _P, _I, _PD, _I, _PD, _I, _I, _PI],
     "hm_pack": [_P, _P, C.c_size_t, C.POINTER(C.c_size_t)],
     "hm_unpack": [_P, _I, _P, C.c_size_t, C.POINTER(_P)],
     "hm_multiply_dense_complex": [_P, _I, _D, _D, _P, _I, _D, _D, _P, _I, _I],

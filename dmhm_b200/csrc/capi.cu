@@ -419,6 +419,33 @@ int hm_create_from_csr_complex(hm_context ctx, int dim, const int* sizes, int nu
     });
 }
 
+int hm_low_rank_product(hm_matrix A, int op, double alpha, hm_matrix B, int sample_rank,
+                        double* U, int ldu, double* V, int ldv, int max_rank, int* rank) {
+    return guarded([&] {
+        HMB_REQUIRE(A && B && U && V && rank, HM_ERR_ARGUMENT, "NULL argument");
+        hm_context_s* ctx = owner_of(A);
+        HMB_REQUIRE(owner_of(B) == ctx, HM_ERR_ARGUMENT, "factors live in different contexts");
+        HMB_REQUIRE(A->h.S && B->h.S, HM_ERR_ARGUMENT, "empty H-matrix");
+        const int n = A->h.height();
+        HMB_REQUIRE(ldu >= std::max(1, n) && ldv >= std::max(1, n), HM_ERR_ARGUMENT,
+                    "leading dimension too small");
+        DeviceBuffer<double> dU, dV;
+        const int r = low_rank_product(ctx->c, A->h, op, alpha, B->h, sample_rank, dU, dV);
+        HMB_REQUIRE(r <= max_rank, HM_ERR_ARGUMENT, "max_rank is below the product's rank");
+        cudaStream_t st = ctx->c.stream;
+        if (r > 0) {
+            HMB_CUDA(cudaMemcpy2DAsync(U, (size_t)ldu * sizeof(double), dU.get(),
+                                       (size_t)n * sizeof(double), (size_t)n * sizeof(double), r,
+                                       cudaMemcpyDeviceToHost, st));
+            HMB_CUDA(cudaMemcpy2DAsync(V, (size_t)ldv * sizeof(double), dV.get(),
+                                       (size_t)n * sizeof(double), (size_t)n * sizeof(double), r,
+                                       cudaMemcpyDeviceToHost, st));
+        }
+        HMB_CUDA(cudaStreamSynchronize(st));
+        *rank = r;
+    });
+}
+
 int hm_packed_size(hm_matrix h, size_t* bytes) {
     return guarded([&] {
         HMB_REQUIRE(h && bytes, HM_ERR_ARGUMENT, "NULL argument");

@@ -216,6 +216,11 @@ void multiply_dense_tf32(HMatrix& H, double alpha, const double* B, int ldb, dou
 void multiply_dense_complex(HMatrix& H, int op, double ar, double ai, const double* B, int ldb,
                             double br, double bi, double* C, int ldc, int nrhs);
 
+// F := alpha op(A) B as one low-rank matrix U V^T (lrprod.cu; op 0 = A,
+// 1 = A^T, 2 = A^H); U, V: height x rank on the device; returns the rank.
+int low_rank_product(Context& ctx, const HMatrix& A, int op, double alpha, const HMatrix& B,
+                     int sample_rank, DeviceBuffer<double>& U, DeviceBuffer<double>& V);
+
 // The reference's Pack / Unpack wire format (pack.cpp).
 size_t packed_size(const HMatrix& H);
 size_t pack(const HMatrix& H, unsigned char* out, size_t cap);

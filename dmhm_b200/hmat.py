@@ -279,6 +279,25 @@ class _HMatBase:
         """SampleRank (hmat2d.hpp:32-33)."""
         return approxRank + self.ctx.oversample()
 
+    # -- one low-rank approximation of a product (hmat_tools) ---------------
+    def LowRankProduct(self, alpha: float, B: "_HMatBase", sampleRank: int = None,
+                       op: int = 0):
+        """F ~= alpha op(A) B as (U, V) with F = U V^T: hmat_tools::Multiply
+        (op 0), TransposeMultiply (op 1), AdjointMultiply (op 2)
+        (include/dmhm/hmat_tools.hpp:1657-2152).  sampleRank defaults to
+        SampleRank(min(A.MaxRank(), B.MaxRank()))."""
+        n = self.Height()
+        r = min(self.MaxRank(), B.MaxRank(), n)
+        if sampleRank is None:
+            sampleRank = self.SampleRank(r)
+        U = np.zeros((n, max(r, 1)), order="F")
+        V = np.zeros((n, max(r, 1)), order="F")
+        rk = C.c_int()
+        check(lib().hm_low_rank_product(self._h, int(op), float(alpha), B.handle, int(sampleRank),
+                                        U.ctypes.data_as(_lib._PD), n, V.ctypes.data_as(_lib._PD),
+                                        n, max(r, 1), C.byref(rk)))
+        return U[:, :rk.value].copy(), V[:, :rk.value].copy()
+
     # -- wire format (src/HMat2d/Pack-incl.hpp) -------------------------------
     def PackedSize(self) -> int:
         n = C.c_size_t()

@@ -121,6 +121,20 @@ HM_API int hm_is_complex(hm_matrix h, int* is_complex);
  * matrices (NODE_SYMMETRIC) and non-root sub-matrices.  Real matrices only.
  */
 HM_API int hm_packed_size(hm_matrix h, size_t* bytes);
+
+/*
+ * One low-rank approximation F = U V^T of a whole product (the randomized
+ * range finder hmat_tools::Multiply, include/dmhm/hmat_tools.hpp:1657-1746:
+ * F := alpha A B; TransposeMultiply, :1848-1937: F := alpha A^T B;
+ * AdjointMultiply, :2039-: F := alpha A^H B), sample_rank Gaussian samples
+ * from the context's serial generator (SampleRank(r) = r + Oversample() in
+ * the reference's callers), truncated to rank min(A.MaxRank, B.MaxRank,
+ * height) (or by the compression tolerance when one is set).  op 0, 1, 2.
+ * U, V: HOST, height x max_rank (leading dimensions ldu, ldv); *rank
+ * receives the number of columns written.  Real matrices only.
+ */
+HM_API int hm_low_rank_product(hm_matrix A, int op, double alpha, hm_matrix B, int sample_rank,
+                               double* U, int ldu, double* V, int ldv, int max_rank, int* rank);
 HM_API int hm_pack(hm_matrix h, void* buffer, size_t capacity, size_t* written);
 HM_API int hm_unpack(hm_context ctx, int dim, const void* buffer, size_t size, hm_matrix* out);
 /*

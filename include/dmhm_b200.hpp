@@ -13,6 +13,7 @@
 #ifndef DMHM_B200_HPP
 #define DMHM_B200_HPP
 
+#include <algorithm>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -306,6 +307,15 @@ class HMat3d : public HMatBase<Scalar, 3> {
     }
 };
 
+// LowRank<Scalar> (include/dmhm/core/low_rank.hpp:22-38): A = U V^T.
+template <typename Scalar>
+struct LowRank {
+    Dense<Scalar> U, V;
+    int Height() const { return U.Height(); }
+    int Width() const { return V.Height(); }
+    int Rank() const { return U.Width(); }
+};
+
 namespace hmat_tools {
 // EstimateTwoNorm (include/dmhm/hmat_tools.hpp:1504-1548)
 template <typename Scalar, int Dim>
@@ -313,6 +323,41 @@ Scalar EstimateTwoNorm(const HMatBase<Scalar, Dim>& A, Scalar theta, Scalar conf
     double est = 0;
     Check(hm_estimate_two_norm(A.Handle(), theta, confidence, &est));
     return est;
+}
+
+
+namespace detail {
+template <typename Scalar, int Dim>
+void LowRankProduct(int op, int sampleRank, Scalar alpha, const HMatBase<Scalar, Dim>& A,
+                    const HMatBase<Scalar, Dim>& B, LowRank<Scalar>& F) {
+    const int n = A.Height();
+    const int cap = std::max(1, std::min(std::min(A.MaxRank(), B.MaxRank()), n));
+    F.U.Resize(n, cap);
+    F.V.Resize(n, cap);
+    int r = 0;
+    Check(hm_low_rank_product(A.Handle(), op, alpha, B.Handle(), sampleRank, F.U.Buffer(),
+                              F.U.LDim(), F.V.Buffer(), F.V.LDim(), cap, &r));
+    F.U.Resize(n, r);
+    F.V.Resize(n, r);
+}
+}  // namespace detail
+
+// F := alpha A B, alpha A^T B, alpha A^H B as one low-rank matrix
+// (include/dmhm/hmat_tools.hpp:1657-1746, 1848-1937, 2039-)
+template <typename Scalar, int Dim>
+void Multiply(int sampleRank, Scalar alpha, const HMatBase<Scalar, Dim>& A,
+              const HMatBase<Scalar, Dim>& B, LowRank<Scalar>& F) {
+    detail::LowRankProduct(0, sampleRank, alpha, A, B, F);
+}
+template <typename Scalar, int Dim>
+void TransposeMultiply(int sampleRank, Scalar alpha, const HMatBase<Scalar, Dim>& A,
+                       const HMatBase<Scalar, Dim>& B, LowRank<Scalar>& F) {
+    detail::LowRankProduct(1, sampleRank, alpha, A, B, F);
+}
+template <typename Scalar, int Dim>
+void AdjointMultiply(int sampleRank, Scalar alpha, const HMatBase<Scalar, Dim>& A,
+                     const HMatBase<Scalar, Dim>& B, LowRank<Scalar>& F) {
+    detail::LowRankProduct(2, sampleRank, alpha, A, B, F);
 }
 }  // namespace hmat_tools
 

@@ -561,6 +561,25 @@ def randomized_product(sample_rank: int, alpha, A: HMat, B: HMat, rng: Rng) -> L
     return LR(U, V)
 
 
+def randomized_transpose_product(sample_rank: int, alpha, A: HMat, B: HMat, rng: Rng) -> LR:
+    """F := alpha A^T B by randomized sampling (TransposeMultiply,
+    include/dmhm/hmat_tools.hpp:1848-1937; AdjointMultiply, :2039-, is the
+    same for real scalars): Y = A^T (alpha B Omega), Q = orth(Y),
+    F.V = B^T (alpha A Q), truncated SVD, F.U = Q (Sigma V^T)^T."""
+    r = min(A.max_rank, B.max_rank, min(A.height, A.width), min(B.height, B.width))
+    Omega = rng.serial.gaussian_vectors(B.width, sample_rank)
+    X = multiply_dense(B, alpha, Omega)
+    Y = transpose_multiply_dense(A, 1.0, X)
+    Q, _, _ = sla.qr(Y, mode="economic", pivoting=True)     # geqp3 + orgqr
+    X = multiply_dense(A, alpha, Q)
+    FV = transpose_multiply_dense(B, 1.0, X)
+    Us, s, VT = sla.svd(FV, full_matrices=False, lapack_driver="gesvd")
+    r = _kept(s, min(r, s.size))
+    V = Us[:, :r].copy()
+    U = Q @ (VT[:r].T * s[:r])
+    return LR(U, V)
+
+
 def _low_rank_of(H: HMat) -> LR:
     return LR(H.U, H.V)
 

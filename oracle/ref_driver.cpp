@@ -334,6 +334,41 @@ int Run(const DriverArgs& a)
         std::vector<double> P = ReadDoubles(a.x, (size_t)N * a.nrhs);
         ApplyToProbes(U, P, N, a.nrhs, result);
     }
+    else if (a.cmd == "lrprod")
+    {
+        // F := alpha op(A) B as one low-rank matrix (hmat_tools::Multiply /
+        // TransposeMultiply, include/dmhm/hmat_tools.hpp:1657-1937), sample
+        // rank maxRank + Oversample(); B from --coefB (--useB 1) or A itself;
+        // F applied to the probes: F.U (F.V^T P)
+        HMat* B = A;
+        if (a.useB == 1)
+        {
+            std::vector<double> cB = ReadDoubles(a.coefB, N);
+            Sparse<double> SB;
+            BuildSparse(a, cB, map, SB);
+            B = Maker<HMat>::Make(a, SB);
+        }
+        std::vector<double> P = ReadDoubles(a.x, (size_t)N * a.nrhs);
+        LowRank<double> F;
+        const int sampleRank = a.rank + Oversample();
+        double t0 = Now();
+        if (a.iters == 1)
+            hmat_tools::TransposeMultiply(sampleRank, a.alpha, *A, *B, F);
+        else
+            hmat_tools::Multiply(sampleRank, a.alpha, *A, *B, F);
+        seconds = Now() - t0;
+        const int r = F.U.Width();
+        result.assign((size_t)N * a.nrhs, 0.0);
+        for (int j = 0; j < a.nrhs; ++j)
+            for (int l = 0; l < r; ++l)
+            {
+                double w = 0;
+                for (int i = 0; i < N; ++i) w += F.V.Get(i, l) * P[i + (size_t)j * N];
+                for (int i = 0; i < N; ++i) result[i + (size_t)j * N] += F.U.Get(i, l) * w;
+            }
+        extraInt = r;
+        if (B != A) delete B;
+    }
     else if (a.cmd == "norm")
     {
         double t0 = Now();

@@ -90,6 +90,13 @@ int main(int argc, char** argv) {
     X.Multiply(1.0, B, Cd);
     write_bin(dir + "/schulz3.bin", Cd.LockedBuffer(), (size_t)N * k);
     std::printf("norm estimate %.17g\n", hmat_tools::EstimateTwoNorm(A, 1.5, 6.0));
+    // one low-rank approximation of X^T X (hmat_tools::TransposeMultiply)
+    LowRank<double> F;
+    hmat_tools::TransposeMultiply(HMat2d<double>::SampleRank(X.MaxRank()), 1.0, X, X, F);
+    if (F.Height() != N || F.Rank() < 1 || F.Rank() > X.MaxRank()) {
+        std::fprintf(stderr, "low-rank product has the wrong shape\n");
+        return 1;
+    }
     // wire format round trip: X packed, unpacked into a fresh matrix, packed again
     std::vector<unsigned char> p1, p2;
     X.Pack(p1);

@@ -26,9 +26,9 @@ DRIVER = os.path.join(ROOT, "oracle", "_ref", "dmhm_ref_driver")
 # name: grid, levels, rank, oversample, strong, coefficient seed, probes
 CASES = {
     "c1": dict(sizes=(32, 32), levels=4, rank=8, oversample=4, strong=1, seed=1, probes=4,
-               ops=["matvec", "random", "hh_AA", "hh_AB", "schulz3", "schulz_stop"]),
+               ops=["matvec", "random", "hh_AA", "hh_AB", "schulz3", "schulz_stop", "lrprod"]),
     "ragged": dict(sizes=(24, 20), levels=3, rank=6, oversample=4, strong=1, seed=5, probes=3,
-                   ops=["matvec", "random", "hh_AA", "hh_AB", "schulz3"]),
+                   ops=["matvec", "random", "hh_AA", "hh_AB", "schulz3", "lrprod"]),
     "weak": dict(sizes=(16, 16), levels=3, rank=4, oversample=4, strong=0, seed=7, probes=3,
                  ops=["matvec", "random", "hh_AA", "schulz3"]),
     "c3d": dict(sizes=(16, 16, 16), levels=3, rank=8, oversample=8, strong=1, seed=9, probes=2,
@@ -86,6 +86,15 @@ def make_case(name, spec, tmp):
         elif op == "hh_AA":
             _, y = run(["hh"] + base + ["--x", ppath, "--nrhs", k], o)
             out["hh_AA"] = mat(y)
+        elif op == "lrprod":
+            # hmat_tools::Multiply / TransposeMultiply: F := alpha op(A) B with
+            # A SetToRandom and B from the second coefficient field
+            for opn, tag in ((0, "lr_AB"), (1, "lr_AtB")):
+                info, y = run(["lrprod"] + base + ["--x", ppath, "--nrhs", k, "--random", 1,
+                                                   "--useB", 1, "--coefB", cbpath,
+                                                   "--alpha", 0.75, "--iters", opn], o)
+                out[tag] = mat(y)
+                out[tag + "_rank"] = info["iterations"]
         elif op == "hh_AB":
             _, y = run(["hh"] + base + ["--x", ppath, "--nrhs", k, "--useB", 1,
                                         "--coefB", cbpath, "--alpha", -0.5], o)

@@ -86,6 +86,23 @@ def test_schulz_iterations(case, its):
     assert relerr(O.multiply_dense(X, 1.0, fx["probes"]), fx[key]) < 1e-8
 
 
+@pytest.mark.parametrize("case", ["c1", "ragged"])
+def test_low_rank_products(case):
+    """hmat_tools::Multiply / TransposeMultiply (F := alpha A B, alpha A^T B
+    as one low-rank matrix, sample rank maxRank + Oversample()): the
+    restatement reproduces the reference's F on probe vectors."""
+    fx = load(case)
+    for tag, fn in (("lr_AB", O.randomized_product), ("lr_AtB", O.randomized_transpose_product)):
+        rng = O.Rng(int(fx["oversample"]))
+        A = oracle_hmat(fx)
+        O.set_to_random(A, rng)
+        B = oracle_hmat(fx, "coefB")
+        F = fn(int(fx["rank"]) + int(fx["oversample"]), 0.75, A, B, rng)
+        assert F.U.shape[1] == int(fx[tag + "_rank"])
+        P = fx["probes"]
+        assert relerr(F.U @ (F.V.T @ P), fx[tag]) < 1e-10
+
+
 def test_complex_fixture_against_dense():
     """The reference's complex-double results (tests/golden/cplx.npz) against
     dense complex algebra of the same operator: products exact, the Schulz

@@ -628,7 +628,7 @@ std::shared_ptr<SymPlan> get_plan(Context& ctx, const HMatrix& A, const HMatrix&
 }  // namespace
 
 void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha, double beta,
-                 HMatrix& C, bool fresh) {
+                 HMatrix& C, bool fresh, bool compact) {
     HMB_REQUIRE(A.S && B.S && (A.S == B.S || same_structure(*A.S, *B.S)), HM_ERR_ARGUMENT,
                 "H*H multiply needs both factors on the same block structure");
     HMB_REQUIRE(&C != &A && &C != &B, HM_ERR_ARGUMENT,
@@ -1201,7 +1201,7 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
     // need nothing: their storage is empty.
     ctx.serial_state = serial_after;
     // tolerance truncation: store C at the ranks kept
-    if (ctx.compression_tol > 0.0) compact_ranks(ctx, C);
+    if (ctx.compression_tol > 0.0 && compact) compact_ranks(ctx, C);
 }
 
 }  // namespace hmb

@@ -6,9 +6,12 @@ namespace hmb {
 
 // C := alpha A B (fresh = true; C is rebuilt) or C := alpha A B + beta C
 // (fresh = false; C keeps its structure).  A, B, C share one block structure
-// and C must be a different object from A and B.
+// and C must be a different object from A and B.  With a compression
+// tolerance, compact = true drops C's unused trailing columns at the end
+// (compact_ranks, which waits for the product); callers that reach a
+// synchronisation point anyway pass false and compact there.
 void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
-                 double beta, HMatrix& C, bool fresh);
+                 double beta, HMatrix& C, bool fresh, bool compact = true);
 
 // Elementwise / structural operations used by Schulz inversion.
 void hmat_copy(Context& ctx, const HMatrix& src, HMatrix& dst);        // CopyFrom

@@ -176,9 +176,17 @@ void compact_ranks(Context& ctx, HMatrix& H) {
     HMB_CUDA(cudaMemcpyAsync(used.data(), dout.get(), used.size() * sizeof(int),
                              cudaMemcpyDeviceToHost, ctx.stream));
     HMB_CUDA(cudaStreamSynchronize(ctx.stream));
-    bool same = true;
-    for (size_t i = 0; i < blocks.size(); ++i) same &= used[i] == rs[i];
-    if (same) return;
+    // Re-lay out only when it saves at least 5 % of the low-rank storage: a
+    // re-layout changes the ranks, and with them the symbolic plans and cached
+    // operation lists of every later product; below that saving the trailing
+    // zero columns are kept (they add nothing to any product or rounding).
+    long long before = 0, after = 0;
+    for (size_t i = 0; i < blocks.size(); ++i) {
+        const Block& B = S.blocks[blocks[i]];
+        before += (long long)(B.m + B.n) * rs[i];
+        after += (long long)(B.m + B.n) * used[i];
+    }
+    if (after == before || after * 20 >= before * 19) return;
     // re-lay out with the used ranks and copy the kept columns over
     DeviceBuffer<double> old = std::move(H.data);
     const std::vector<long long> old_off = H.off;
@@ -370,29 +378,43 @@ SchulzResult schulz_invert(Context& ctx, HMatrix& A, int num_iterations, double 
                          (stop ? last > mixed_switch : k + 3 < num_iterations);
         ctx.low_precision = low || was_low;
         if (low) ++res.low_iterations;
+        // Tolerance truncation: the products leave their unused trailing
+        // columns in place and Z and X are compacted after the norm
+        // estimate, which waits for the device anyway (compacting right
+        // after each product would make the host wait for every product)
+        const bool tol = ctx.compression_tol > 0.0;
         HMatrix Z;
-        hh_multiply(ctx, *X, A, -1.0, 0.0, Z, true);
+        hh_multiply(ctx, *X, A, -1.0, 0.0, Z, true, false);
         if (stop) {
             hmat_add_diagonal(ctx, Z, 1.0);
             const double ez = estimate_two_norm(ctx, Z, theta, confidence);
             res.trace.push_back(ez);
             last = std::fabs(ez);
+            if (tol) {
+                compact_ranks(ctx, Z);
+                compact_ranks(ctx, *X);
+            }
             if (std::fabs(ez) < stop_tol && !low) {
                 hmat_add_diagonal(ctx, Z, 1.0);
                 auto Xn = std::make_unique<HMatrix>();
-                hh_multiply(ctx, Z, *X, 1.0, 0.0, *Xn, true);
+                hh_multiply(ctx, Z, *X, 1.0, 0.0, *Xn, true, false);
                 X = std::move(Xn);
                 ++k;
                 break;
             }
             hmat_add_diagonal(ctx, Z, 1.0);
         } else {
+            if (tol) {
+                compact_ranks(ctx, Z);
+                compact_ranks(ctx, *X);
+            }
             hmat_add_diagonal(ctx, Z, 2.0);
         }
         auto Xn = std::make_unique<HMatrix>();
-        hh_multiply(ctx, Z, *X, 1.0, 0.0, *Xn, true);
+        hh_multiply(ctx, Z, *X, 1.0, 0.0, *Xn, true, false);
         X = std::move(Xn);
     }
+    if (ctx.compression_tol > 0.0) compact_ranks(ctx, *X);
     res.iterations = k;
     // A := X (CopyFrom, Invert-incl.hpp:195): take over X's storage
     A.rank = X->rank;

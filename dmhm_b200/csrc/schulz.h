@@ -14,7 +14,8 @@ struct SchulzResult {
 
 double estimate_two_norm(Context& ctx, HMatrix& A, double theta, double confidence);
 // Drops the trailing zero columns that tolerance truncation leaves in the
-// low-rank blocks (synchronizes to read the ranks back).
+// low-rank blocks when that saves at least 5 % of the low-rank storage
+// (synchronizes to read the ranks back).
 void compact_ranks(Context& ctx, HMatrix& H);
 // mixed_switch > 0: mixed precision (iterations in the low-precision phase
 // while the last ||I - X A|| estimate is above mixed_switch).

@@ -194,6 +194,7 @@ __device__ void cta_jacobi(R* M, int rows, int cols, R* J, int* flag, R* red, R*
     // the start of every sweep, then updated by the rotations), so a pair
     // reduces only its inner product.
     const int hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
+    constexpr R jt2 = Prec<R>::jtol * Prec<R>::jtol;
     for (int sweep = 0; sweep < kJacobiSweeps; ++sweep) {
         for (int c = warp; c < cols; c += kW) {
             const R* g = M + (long long)c * rows;
@@ -204,6 +205,37 @@ __device__ void cta_jacobi(R* M, int rows, int cols, R* J, int* flag, R* red, R*
         }
         if (threadIdx.x == 0) *flag = 0;
         __syncthreads();
+        // Convergence test on all pairs at once (the off-diagonal of the
+        // Gram matrix, each pair's inner product by one thread): the sweep
+        // below runs only if some pair would rotate, so the sweep that finds
+        // nothing left to rotate is never run.  The inner products start at
+        // a row offset that differs per lane, so the lanes of a warp read
+        // different shared-memory banks.
+        {
+            bool rotate = false;
+            for (int idx = threadIdx.x; idx < cols * cols && !rotate; idx += kT) {
+                const int p = idx / cols, q = idx % cols;
+                if (q <= p) continue;
+                const R a = nrm[p], b = nrm[q];
+                if (!(a > tiny && b > tiny)) continue;
+                const R* gp = M + (long long)p * rows;
+                const R* gq = M + (long long)q * rows;
+                R c = 0;
+                int i = lane % rows;
+                for (int t = 0; t < rows; ++t) {
+                    c = r_fma(gp[i], gq[i], c);
+                    i = (i + 1 == rows) ? 0 : i + 1;
+                }
+                rotate = c != R(0) && c * c > jt2 * (a * b);
+            }
+            if (rotate) *flag = 1;
+            __syncthreads();
+            const int needed = *flag;
+            __syncthreads();
+            if (!needed) break;
+            if (threadIdx.x == 0) *flag = 0;
+            __syncthreads();
+        }
         for (int step = 0; step < n - 1; ++step) {
             // warp-uniform trip count: both half-warps of a warp iterate
             // together (their shuffles span the whole warp)
@@ -224,7 +256,6 @@ __device__ void cta_jacobi(R* M, int rows, int cols, R* J, int* flag, R* red, R*
 #pragma unroll
                 for (int o = 8; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
                 const R a = live ? nrm[p] : R(0), b = live ? nrm[q] : R(0);
-                constexpr R jt2 = Prec<R>::jtol * Prec<R>::jtol;
                 if (live && c != R(0) && a > tiny && b > tiny && c * c > jt2 * (a * b)) {
                     // t = tan of the rotation angle, the smaller root of
                     // t^2 + 2 zeta t - 1 = 0 with zeta = (b - a) / (2c),

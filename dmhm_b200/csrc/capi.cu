@@ -254,6 +254,11 @@ int hm_context_destroy(hm_context ctx) {
         ctx->c.layouts.clear();
         ctx->c.hh_cache.reset();
         for (auto& b : ctx->c.scratch_bufs) b.reset();
+        if (ctx->c.pinned) {
+            cudaStreamSynchronize(ctx->c.stream);
+            cudaFreeHost(ctx->c.pinned);
+            ctx->c.pinned = nullptr;
+        }
         ctx->c.counters.reset();
         ctx->c.errword.reset();
         cudaStreamSynchronize(ctx->c.stream);

@@ -87,6 +87,10 @@ struct Context {
     // a product's kernels finish before the next product's start.
     double* scratch(int slot, long long n);
     DeviceBuffer<double> scratch_bufs[4];
+    // One double of pinned host memory for results read back asynchronously
+    // (made on first use, freed with the context).
+    double* pinned_scalar();
+    double* pinned = nullptr;
     // Device word set by kernels whose bounded waits gave up (zero = fine).
     int* error_word();
     DeviceBuffer<int> errword;

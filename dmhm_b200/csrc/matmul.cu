@@ -1235,6 +1235,11 @@ int* Context::error_word() {
     return errword.get();
 }
 
+double* Context::pinned_scalar() {
+    if (!pinned) HMB_CUDA(cudaMallocHost((void**)&pinned, sizeof(double)));
+    return pinned;
+}
+
 double* Context::scratch(int slot, long long n) {
     DeviceBuffer<double>& b = scratch_bufs[slot];
     n = std::max<long long>(n, 2);

@@ -290,7 +290,10 @@ void hmat_add_diagonal(Context& ctx, HMatrix& H, double alpha) {
 // ---------------------------------------------------------------------------
 // EstimateTwoNorm
 // ---------------------------------------------------------------------------
-double estimate_two_norm(Context& ctx, HMatrix& A, double theta, double confidence) {
+// Issues the estimate: its result lands in *result (pinned host memory)
+// once `done` completes.
+void estimate_two_norm_issue(Context& ctx, HMatrix& A, double theta, double confidence,
+                             double* result, cudaEvent_t done) {
     HMB_REQUIRE(theta > 1.0, HM_ERR_ARGUMENT, "theta must be > 1");
     HMB_REQUIRE(confidence > 0.0, HM_ERR_ARGUMENT, "confidence must be positive");
     const int n = A.height();
@@ -335,10 +338,23 @@ double estimate_two_norm(Context& ctx, HMatrix& A, double theta, double confiden
         HMB_CHECK_LAUNCH();
         std::swap(cur, nxt);
     }
-    double est = 0.0;
-    HMB_CUDA(cudaMemcpyAsync(&est, scal.get() + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
-    HMB_CUDA(cudaStreamSynchronize(st));
-    return est;
+    HMB_CUDA(cudaMemcpyAsync(result, scal.get() + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+    HMB_CUDA(cudaEventRecord(done, st));
+}
+
+double estimate_two_norm(Context& ctx, HMatrix& A, double theta, double confidence) {
+    double* slot = ctx.pinned_scalar();
+    cudaEvent_t ev;
+    HMB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    try {
+        estimate_two_norm_issue(ctx, A, theta, confidence, slot, ev);
+        HMB_CUDA(cudaEventSynchronize(ev));
+    } catch (...) {
+        cudaEventDestroy(ev);
+        throw;
+    }
+    cudaEventDestroy(ev);
+    return *slot;
 }
 
 // ---------------------------------------------------------------------------
@@ -372,6 +388,12 @@ SchulzResult schulz_invert(Context& ctx, HMatrix& A, int num_iterations, double 
         ~Restore() { c.low_precision = v; }
     } restore{ctx, was_low};
     double last = std::numeric_limits<double>::infinity();
+    cudaEvent_t est_done;
+    HMB_CUDA(cudaEventCreateWithFlags(&est_done, cudaEventDisableTiming));
+    struct EventGuard {
+        cudaEvent_t e;
+        ~EventGuard() { cudaEventDestroy(e); }
+    } est_guard{est_done};
     int k = 0;
     for (; k < num_iterations; ++k) {
         const bool low = mixed_switch > 0.0 &&
@@ -385,6 +407,27 @@ SchulzResult schulz_invert(Context& ctx, HMatrix& A, int num_iterations, double 
         const bool tol = ctx.compression_tol > 0.0;
         HMatrix Z;
         hh_multiply(ctx, *X, A, -1.0, 0.0, Z, true, false);
+        if (stop && !tol) {
+            // X_{k+1} = (2I - X A) X is the same whether or not the stop
+            // test passes, so it is issued before the estimate is read: the
+            // host prepares it while the device runs the power iteration
+            hmat_add_diagonal(ctx, Z, 1.0);
+            double* slot = ctx.pinned_scalar();
+            estimate_two_norm_issue(ctx, Z, theta, confidence, slot, est_done);
+            hmat_add_diagonal(ctx, Z, 1.0);
+            auto Xn = std::make_unique<HMatrix>();
+            hh_multiply(ctx, Z, *X, 1.0, 0.0, *Xn, true, false);
+            HMB_CUDA(cudaEventSynchronize(est_done));
+            const double ez = *slot;
+            res.trace.push_back(ez);
+            last = std::fabs(ez);
+            X = std::move(Xn);
+            if (std::fabs(ez) < stop_tol && !low) {
+                ++k;
+                break;
+            }
+            continue;
+        }
         if (stop) {
             hmat_add_diagonal(ctx, Z, 1.0);
             const double ez = estimate_two_norm(ctx, Z, theta, confidence);

@@ -98,3 +98,18 @@ def test_complex_matches_reference():
     assert relerr(H.Multiply(1.0, H).Multiply(1.0, P), fx["hh_AA"]) < 1e-12
     its, trace = H.SchulzInvert(-1, 1.5, 6.0, 1e-8)
     assert relerr(H.Multiply(1.0, P), fx["schulz_stop"]) < 1e-7
+
+
+def test_complex_3d_products():
+    """HMat3d<std::complex<double>>: seven-point Helmholtz-like operator on an
+    8 x 8 x 8 grid, products and the H*H square against dense algebra."""
+    sizes = (8, 8, 8)
+    S = O.helmholtz(sizes, 4.0, 2)
+    ctx = D.Context(0)
+    H = D.HMat3d(S, 2, 8, True, *sizes, ctx=ctx)
+    assert H.is_complex and H.Height() == 512
+    A = O.dense_from_sparse(S)
+    X = cplx(np.random.default_rng(7), 512, 3)
+    assert relerr(H.Multiply(0.5 + 0.25j, X), (0.5 + 0.25j) * A @ X) < 1e-13
+    assert relerr(H.AdjointMultiply(1.0, X), A.conj().T @ X) < 1e-13
+    assert relerr(H.Multiply(1.0, H).Multiply(1.0, X), A @ (A @ X)) < 1e-12

@@ -256,9 +256,14 @@ def gpu_arm(args):
     prof = read_profile(ctx)
     _lib.check(lib.hm_profile_enable(ctx.handle, 0))
 
-    # roofline of the dominant kernel
+    # roofline of the dominant kernel: the two phases of the product take
+    # nearly equal time, so the choice is made by a 10 % margin with the
+    # output phase (hmm_row_tiles, the larger share of the bytes) preferred
+    # on a tie, which keeps the reported kernel the same from run to run
     hbm_peak, peak_kind = peaks()
     top = max(prof.items(), key=lambda kv: kv[1]["ms"])
+    if "hmm_row_tiles" in prof and prof["hmm_row_tiles"]["ms"] >= 0.9 * top[1]["ms"]:
+        top = ("hmm_row_tiles", prof["hmm_row_tiles"])
     kname, kv = top
     per_launch_ms = kv["ms"] / kv["launches"]
     kbytes = kernel_bytes(kname, census, N, NRHS, H)

@@ -57,6 +57,10 @@ SIGNATURES = {
     "hm_create_from_csr": [_P, _I, _PI, _I, _I, _I, _PI64, _PI32, _PD, C.POINTER(_P)],
     "hm_create_from_csr_complex": [_P, _I, _PI, _I, _I, _I, _PI64, _PI32, _PD, C.POINTER(_P)],
     "hm_is_complex": [_P, _PI],
+    "hm_scale_complex": [_P, _D, _D],
+    "hm_add_constant_to_diagonal_complex": [_P, _D, _D],
+    "hm_conjugate": [_P, C.POINTER(_P)],
+    "hm_transpose_complex": [_P, C.POINTER(_P)],
     "hm_packed_size": [_P, C.POINTER(C.c_size_t)],
     "hm_low_rank_product": [_P, _I, _D, _P, _I, _PD, _I, _PD, _I, _I, _PI],
     "hm_pack": [_P, _P, C.c_size_t, C.POINTER(C.c_size_t)],

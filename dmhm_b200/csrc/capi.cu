@@ -714,6 +714,47 @@ int hm_transpose(hm_matrix src, hm_matrix* dst) {
     });
 }
 
+int hm_scale_complex(hm_matrix h, double alpha_re, double alpha_im) {
+    return guarded([&] {
+        HMB_REQUIRE(h, HM_ERR_ARGUMENT, "h is NULL");
+        complex_scale(owner_of(h)->c, h->h, alpha_re, alpha_im);
+    });
+}
+
+int hm_add_constant_to_diagonal_complex(hm_matrix h, double alpha_re, double alpha_im) {
+    return guarded([&] {
+        HMB_REQUIRE(h, HM_ERR_ARGUMENT, "h is NULL");
+        complex_add_diagonal(owner_of(h)->c, h->h, alpha_re, alpha_im);
+    });
+}
+
+int hm_conjugate(hm_matrix src, hm_matrix* dst) {
+    return guarded([&] {
+        HMB_REQUIRE(src && dst, HM_ERR_ARGUMENT, "NULL argument");
+        HMB_REQUIRE(*dst != src, HM_ERR_ARGUMENT, "conjugate onto itself");
+        hm_context_s* ctx = owner_of(src);
+        HMB_REQUIRE(src->h.S && src->h.S->dof == 2, HM_ERR_ARGUMENT, "not a complex H-matrix");
+        if (*dst == nullptr) *dst = new_handle(ctx);
+        HMB_REQUIRE(owner_of(*dst) == ctx, HM_ERR_ARGUMENT, "dst lives in another context");
+        hmat_copy(ctx->c, src->h, (*dst)->h);
+        complex_conjugate(ctx->c, (*dst)->h);
+    });
+}
+
+int hm_transpose_complex(hm_matrix src, hm_matrix* dst) {
+    return guarded([&] {
+        HMB_REQUIRE(src && dst, HM_ERR_ARGUMENT, "NULL argument");
+        HMB_REQUIRE(*dst != src, HM_ERR_ARGUMENT, "transpose onto itself");
+        hm_context_s* ctx = owner_of(src);
+        HMB_REQUIRE(src->h.S && src->h.S->dof == 2, HM_ERR_ARGUMENT, "not a complex H-matrix");
+        if (*dst == nullptr) *dst = new_handle(ctx);
+        HMB_REQUIRE(owner_of(*dst) == ctx, HM_ERR_ARGUMENT, "dst lives in another context");
+        // A^T = conj(A^H); the real form's transpose is A^H
+        hmat_transpose(ctx->c, src->h, (*dst)->h);
+        complex_conjugate(ctx->c, (*dst)->h);
+    });
+}
+
 int hm_scale(hm_matrix h, double alpha) {
     return guarded([&] {
         HMB_REQUIRE(h, HM_ERR_ARGUMENT, "h is NULL");

@@ -64,7 +64,107 @@ int grid_for(const Context& ctx, long long total) {
     return (int)std::max<long long>(1, std::min<long long>((total + kT - 1) / kT, 4LL * ctx.num_sms));
 }
 
+// Elementwise work on the real form of one stored matrix piece (column-major
+// m x n, leading dimension m): kind 0 rows 2i, 2i+1 := [[a, -b], [b, a]] of
+// them (left multiplication by alpha = a + bi), kind 1 negate odd rows (the
+// conjugate of a factor: conj(U V^T) = (J U)(J V)^T with J = diag(1, -1)),
+// kind 2 negate the entries with row + column odd (the conjugate of a dense
+// block, J D J), kind 3 add [[a, -b], [b, a]] on the diagonal pairs (a dense
+// diagonal block plus alpha I).
+struct PieceTask {
+    double* p;
+    int m, n, kind, pad;
+};
+
+__global__ void complex_pieces_kernel(const PieceTask* __restrict__ tasks, double a, double b) {
+    const PieceTask t = tasks[blockIdx.x];
+    if (t.kind == 0) {
+        const long long pairs = (long long)(t.m / 2) * t.n;
+        for (long long e = threadIdx.x; e < pairs; e += blockDim.x) {
+            const int i = (int)(e % (t.m / 2)), j = (int)(e / (t.m / 2));
+            double* c = t.p + 2 * i + (long long)j * t.m;
+            const double x = c[0], y = c[1];
+            c[0] = a * x - b * y;
+            c[1] = b * x + a * y;
+        }
+    } else if (t.kind == 1) {
+        const long long total = (long long)(t.m / 2) * t.n;
+        for (long long e = threadIdx.x; e < total; e += blockDim.x) {
+            const int i = (int)(e % (t.m / 2)), j = (int)(e / (t.m / 2));
+            t.p[2 * i + 1 + (long long)j * t.m] *= -1.0;
+        }
+    } else if (t.kind == 2) {
+        const long long total = (long long)t.m * t.n;
+        for (long long e = threadIdx.x; e < total; e += blockDim.x) {
+            const int i = (int)(e % t.m), j = (int)(e / t.m);
+            if ((i + j) & 1) t.p[e] = -t.p[e];
+        }
+    } else {
+        for (int i = threadIdx.x; i < t.m / 2; i += blockDim.x) {
+            double* d = t.p + 2 * i + (long long)(2 * i) * t.m;   // (2i, 2i)
+            d[0] += a;
+            d[1] += b;                           // (2i+1, 2i)
+            d[t.m] -= b;                         // (2i, 2i+1)
+            d[t.m + 1] += a;                     // (2i+1, 2i+1)
+        }
+    }
+}
+
+void run_pieces(Context& ctx, HMatrix& H, const std::vector<PieceTask>& tasks, double a, double b,
+                const char* name) {
+    if (tasks.empty()) return;
+    DeviceBuffer<PieceTask> d;
+    d.upload(tasks, ctx.stream);
+    LaunchScope ls(ctx, name);
+    complex_pieces_kernel<<<(unsigned)tasks.size(), kT, 0, ctx.stream>>>(d.get(), a, b);
+    HMB_CHECK_LAUNCH();
+    H.shadow_valid = false;   // the FP32 copy no longer matches
+}
+
 }  // namespace
+
+// A := alpha A for complex alpha (Scale, HMat2d.cpp:616-647): every dense
+// block and every U factor multiplied from the left by alpha I.
+void complex_scale(Context& ctx, HMatrix& H, double a, double b) {
+    HMB_REQUIRE(H.S && H.S->dof == 2, HM_ERR_ARGUMENT, "not a complex H-matrix");
+    std::vector<PieceTask> t;
+    for (int blk : H.S->leaves) {
+        const Block& B = H.S->blocks[blk];
+        if (B.m == 0 || B.n == 0) continue;
+        if (B.kind == KIND_DENSE) t.push_back({H.D(blk), B.m, B.n, 0, 0});
+        else if (H.rank[blk] > 0) t.push_back({H.U(blk), B.m, H.rank[blk], 0, 0});
+    }
+    run_pieces(ctx, H, t, a, b, "complex_scale");
+}
+
+// A := A + alpha I for complex alpha (AddConstantToDiagonal, HMat2d.cpp:704-744).
+void complex_add_diagonal(Context& ctx, HMatrix& H, double a, double b) {
+    HMB_REQUIRE(H.S && H.S->dof == 2, HM_ERR_ARGUMENT, "not a complex H-matrix");
+    std::vector<PieceTask> t;
+    for (int blk : H.S->leaves) {
+        const Block& B = H.S->blocks[blk];
+        if (B.kind == KIND_DENSE && B.row_off == B.col_off && B.m == B.n && B.m > 0)
+            t.push_back({H.D(blk), B.m, B.n, 3, 0});
+    }
+    run_pieces(ctx, H, t, a, b, "complex_add_diagonal");
+}
+
+// A := conj(A) in place (the conjugation of ConjugateFrom, HMat2d.cpp:424-472).
+void complex_conjugate(Context& ctx, HMatrix& H) {
+    HMB_REQUIRE(H.S && H.S->dof == 2, HM_ERR_ARGUMENT, "not a complex H-matrix");
+    std::vector<PieceTask> t;
+    for (int blk : H.S->leaves) {
+        const Block& B = H.S->blocks[blk];
+        if (B.m == 0 || B.n == 0) continue;
+        if (B.kind == KIND_DENSE) {
+            t.push_back({H.D(blk), B.m, B.n, 2, 0});
+        } else if (H.rank[blk] > 0) {
+            t.push_back({H.U(blk), B.m, H.rank[blk], 1, 0});
+            t.push_back({H.V(blk), B.n, H.rank[blk], 1, 0});
+        }
+    }
+    run_pieces(ctx, H, t, 0.0, 0.0, "complex_conjugate");
+}
 
 void multiply_dense(HMatrix& H, int transpose, double alpha, const double* B, int ldb, double beta,
                     double* C, int ldc, int nrhs);

@@ -230,6 +230,12 @@ size_t packed_size(const HMatrix& H);
 size_t pack(const HMatrix& H, unsigned char* out, size_t cap);
 void unpack(Context& ctx, int dim, const unsigned char* buf, size_t size, HMatrix& H);
 
+// Complex helpers on the real form (complex.cu): Scale and
+// AddConstantToDiagonal with complex alpha, in-place conjugation.
+void complex_scale(Context& ctx, HMatrix& H, double a, double b);
+void complex_add_diagonal(Context& ctx, HMatrix& H, double a, double b);
+void complex_conjugate(Context& ctx, HMatrix& H);
+
 // Device kernels driven from the host side (launchers).
 void launch_fill_random(Context& ctx, HMatrix& H);
 

@@ -450,15 +450,38 @@ class _HMatBase:
         self._h = out
         return self
 
-    TransposeFrom = AdjointFrom
+    def TransposeFrom(self, B: "_HMatBase"):
+        """A := B^T (TransposeFrom, HMat2d.cpp:477-546; B^T = B^H for real
+        scalars, conj(B^H) for complex ones)."""
+        if B.is_complex:
+            out = _handle_of(self)
+            check(lib().hm_transpose_complex(B.handle, C.byref(out)))
+            self._h = out
+            return self
+        return self.AdjointFrom(B)
 
-    def Scale(self, alpha: float):
-        """A := alpha A (HMat2d.cpp:616-647)."""
-        check(lib().hm_scale(self._h, float(alpha)))
+    def ConjugateFrom(self, B: "_HMatBase"):
+        """A := conj(B) (ConjugateFrom, HMat2d.cpp:424-472); complex only."""
+        out = _handle_of(self)
+        check(lib().hm_conjugate(B.handle, C.byref(out)))
+        self._h = out
+        return self
 
-    def AddConstantToDiagonal(self, alpha: float):
-        """A := A + alpha I (HMat2d.cpp:704-744)."""
-        check(lib().hm_add_constant_to_diagonal(self._h, float(alpha)))
+    def Scale(self, alpha):
+        """A := alpha A (HMat2d.cpp:616-647); complex alpha on complex matrices."""
+        if isinstance(alpha, complex) or np.iscomplexobj(alpha):
+            a = complex(alpha)
+            check(lib().hm_scale_complex(self._h, a.real, a.imag))
+        else:
+            check(lib().hm_scale(self._h, float(alpha)))
+
+    def AddConstantToDiagonal(self, alpha):
+        """A := A + alpha I (HMat2d.cpp:704-744); complex alpha on complex matrices."""
+        if isinstance(alpha, complex) or np.iscomplexobj(alpha):
+            a = complex(alpha)
+            check(lib().hm_add_constant_to_diagonal_complex(self._h, a.real, a.imag))
+        else:
+            check(lib().hm_add_constant_to_diagonal(self._h, float(alpha)))
 
     def SchulzInvert(self, numIterations: int, theta: float = 1.5, confidence: float = 6.0,
                      stopTol: float = 1e-4):

@@ -151,6 +151,17 @@ HM_API int hm_multiply_dense_complex_host(hm_matrix h, int op, double alpha_re,
                                           double alpha_im, const double* B, int ldb,
                                           double beta_re, double beta_im, double* C, int ldc,
                                           int nrhs);
+/*
+ * Complex scalars on a complex H-matrix: Scale (src/HMat2d/HMat2d.cpp:616-647)
+ * and AddConstantToDiagonal (:704-744) with alpha = alpha_re + i alpha_im;
+ * ConjugateFrom (:424-472) into *dst; TransposeFrom without conjugation
+ * (:477-546; hm_transpose is AdjointFrom, :548-614, for a complex handle).
+ * *dst == NULL creates a new handle.
+ */
+HM_API int hm_scale_complex(hm_matrix h, double alpha_re, double alpha_im);
+HM_API int hm_add_constant_to_diagonal_complex(hm_matrix h, double alpha_re, double alpha_im);
+HM_API int hm_conjugate(hm_matrix src, hm_matrix* dst);
+HM_API int hm_transpose_complex(hm_matrix src, hm_matrix* dst);
 HM_API int hm_destroy(hm_matrix h);
 
 /* Height, width, number of levels, max rank, and the block census:

@@ -113,3 +113,30 @@ def test_complex_3d_products():
     assert relerr(H.Multiply(0.5 + 0.25j, X), (0.5 + 0.25j) * A @ X) < 1e-13
     assert relerr(H.AdjointMultiply(1.0, X), A.conj().T @ X) < 1e-13
     assert relerr(H.Multiply(1.0, H).Multiply(1.0, X), A @ (A @ X)) < 1e-12
+
+
+def test_complex_scalar_helpers():
+    """Scale and AddConstantToDiagonal with complex alpha, ConjugateFrom,
+    TransposeFrom (no conjugation) and AdjointFrom, against dense algebra, on
+    a weakly admissible matrix built from the operator (its low-rank blocks
+    hold the stencil entries between neighbouring boxes exactly)."""
+    sizes = (24, 20)
+    S = O.helmholtz(sizes, 3.0, 3)
+    ctx = D.Context(0)
+    H = D.HMat2d(S, 3, 12, False, *sizes, ctx=ctx)
+    assert H.BlockCensus()["rank_sum"] > 0
+    n = S.height
+    A = O.dense_from_sparse(S)
+    X = cplx(np.random.default_rng(8), n, 3)
+    assert relerr(H.Multiply(1.0, X), A @ X) < 1e-13
+    al, be = 0.6 - 1.3j, -0.2 + 0.7j
+    H.Scale(al)
+    H.AddConstantToDiagonal(be)
+    B = al * A + be * np.eye(n)
+    assert relerr(H.Multiply(1.0, X), B @ X) < 1e-13
+    Hc = D.HMat2d(ctx=ctx).ConjugateFrom(H)
+    assert relerr(Hc.Multiply(1.0, X), B.conj() @ X) < 1e-13
+    Ht = D.HMat2d(ctx=ctx).TransposeFrom(H)
+    assert relerr(Ht.Multiply(1.0, X), B.T @ X) < 1e-13
+    Ha = D.HMat2d(ctx=ctx).AdjointFrom(H)
+    assert relerr(Ha.Multiply(1.0, X), B.conj().T @ X) < 1e-13

@@ -455,7 +455,9 @@ __device__ void do_round(const RoundOp& op_in, R* dyn, long long smem_elems, Rou
         const double s0 = norms[order[0]];
         const double tol = op.tol > Prec<R>::tol_floor ? op.tol : Prec<R>::tol_floor;
         const double t2 = tol * tol;
-        int c = 0;
+        // SVDTrunc keeps at least sigma_0: one column when sigma_0 < tol^2
+        // (its cutoff index 0), else every sigma above tol * sigma_0
+        int c = 1;
         if (s0 >= t2 * t2)
             while (c < keep && (double)norms[order[c]] > t2 * s0) ++c;
         keep = c;

@@ -26,8 +26,8 @@ struct RoundOp {
     double alpha, beta;
     int kind, m, n, r1, r2, rout;
     int ldu1, ldv1, ldu2, ldv2;
-    // > 0: also drop the singular values at or below tol * sigma_0 (all of
-    // them when sigma_0 < tol^2), writing zero columns in their place
+    // > 0: also drop the singular values at or below tol * sigma_0 (all but
+    // sigma_0 when sigma_0 < tol^2), writing zero columns in their place
     // (GENERAL, DENSE, ORTHO).
     double tol;
     int* rank_out;      // if set: receives the rank of the output

@@ -63,9 +63,9 @@ HM_API int hm_get_oversample(hm_context ctx, int* oversample);
 /* SetCompressionTolerance / CompressionTolerance (src/core/global.cpp:
    160-181), applied as the single-rank DistHMat truncation does
    (SVDTrunc, src/DistHMat2d/Truncation-incl.hpp:37-63): every H*H
-   compression keeps the singular values above tol * sigma_0 (none when
-   sigma_0 < tol^2), at most maxRank, and the product is stored at the ranks
-   kept.  0 (the default) keeps HMat2d's fixed rank maxRank. */
+   compression keeps the singular values above tol * sigma_0 (at least
+   sigma_0; only sigma_0 when sigma_0 < tol^2), at most maxRank, and the
+   product is stored at the ranks kept.  0 (the default) keeps HMat2d's fixed rank maxRank. */
 HM_API int hm_set_compression_tolerance(hm_context ctx, double tol);
 HM_API int hm_get_compression_tolerance(hm_context ctx, double* tol);
 /* SeedSerialLcg (src/core/random.cpp:67-68) and the single-rank

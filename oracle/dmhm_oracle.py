@@ -500,7 +500,8 @@ def lr_times_lr(alpha, A: LR, B: LR) -> LR:
 # CompressionTolerance (src/core/global.cpp:160-181): 0 keeps the fixed rank
 # of HMat2d; > 0 truncates every SVD as the single-rank DistHMat does
 # (SVDTrunc, src/DistHMat2d/Truncation-incl.hpp:37-63): keep the singular
-# values above tol * sigma_0, none when sigma_0 < tol^2, at most the rank cap.
+# values above tol * sigma_0 (at least sigma_0; only sigma_0 when sigma_0 <
+# tol^2, the cutoff index 0 of Truncation-incl.hpp:52-55), at most the rank cap.
 _COMPRESSION_TOL = [0.0]
 
 
@@ -512,9 +513,11 @@ def _kept(s: np.ndarray, cap: int) -> int:
     tol = _COMPRESSION_TOL[0]
     if tol <= 0.0:
         return cap
-    if s.size == 0 or s[0] < tol * tol:
+    if s.size == 0 or cap == 0:
         return 0
-    return int(min(cap, np.count_nonzero(s > tol * s[0])))
+    if s[0] < tol * tol:
+        return 1
+    return int(min(cap, max(1, np.count_nonzero(s > tol * s[0]))))
 
 
 def rounded_update(max_rank: int, alpha, A: LR, beta, B: LR) -> LR:

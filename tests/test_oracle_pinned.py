@@ -157,3 +157,35 @@ def test_pack_fixture_layout(case):
     # the buffer (Pack-incl.hpp:32)
     end = _walk_pack(raw, header, oracle_hmat(fx))
     assert end + 4 == len(raw) and raw[end:] == bytes(4)
+
+
+def test_tolerance_rule_matches_svdtrunc():
+    """The oracle's kept-rank rule against the reference's SVDTrunc loop
+    (src/DistHMat2d/Truncation-incl.hpp:51-59) on spectra around the
+    thresholds: at least sigma_0 is kept, only sigma_0 below tol^2."""
+    def svdtrunc(s, rel_tol, max_rank):
+        k = len(s)
+        if k == 0:
+            return 0
+        tolerance = rel_tol * s[0]
+        if s[0] < rel_tol * rel_tol:
+            cutoff = 0
+        else:
+            cutoff = min(k, max_rank) - 1
+            while cutoff >= 0 and not s[cutoff] > tolerance:
+                cutoff -= 1
+        return cutoff + 1
+
+    rng = np.random.default_rng(4)
+    old = O._COMPRESSION_TOL[0]
+    try:
+        for tol in (1e-10, 1e-4, 0.3):
+            O.set_compression_tolerance(tol)
+            for _ in range(200):
+                k = int(rng.integers(1, 12))
+                s = np.sort(10.0 ** rng.uniform(-25, 2, k))[::-1]
+                cap = int(rng.integers(1, 14))
+                assert O._kept(s, cap) == svdtrunc(list(s), tol, cap)
+            assert O._kept(np.array([1e-30, 1e-31]), 4) == 1
+    finally:
+        O.set_compression_tolerance(old)

@@ -8,12 +8,14 @@ runs in hand-written CUDA kernels behind the C ABI of
 Python mirror of the reference's C++ API.
 """
 from ._lib import HMError, LIB_PATH, lib
-from .hmat import (Context, EstimateTwoNorm, Finalize, HMat2d, HMat3d, Initialize,
+from .hmat import (Context, DistHMat2d, DistHMat3d, EstimateTwoNorm, Finalize, HMat2d, HMat3d,
+                   Initialize, Teams,
                    Oversample, SetOversample, SetCompressionTolerance, CompressionTolerance,
                    RankModel, Sparse, natural_to_hierarchical_map)
 from . import operators
 
-__all__ = ["Context", "EstimateTwoNorm", "Finalize", "HMError", "HMat2d", "HMat3d", "Initialize",
+__all__ = ["Context", "DistHMat2d", "DistHMat3d", "EstimateTwoNorm", "Finalize", "HMError",
+           "HMat2d", "HMat3d", "Initialize", "Teams",
            "LIB_PATH", "Oversample", "SetOversample", "SetCompressionTolerance",
            "CompressionTolerance", "RankModel", "Sparse", "lib",
            "natural_to_hierarchical_map", "operators"]

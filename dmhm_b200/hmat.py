@@ -157,14 +157,33 @@ def Oversample(ctx: Optional[Context] = None) -> int:
     return _ctx(ctx).oversample()
 
 
-def SetCompressionTolerance(tol: float, ctx: Optional[Context] = None):
-    """SetCompressionTolerance (global.cpp:160-181): relative truncation of
-    the H*H compressions (0 = the fixed rank maxRank)."""
-    _ctx(ctx).set_compression_tolerance(tol)
+_DIST_TOL = [1e-16]   # compressionTolDouble (src/core/global.cpp:34)
 
 
-def CompressionTolerance(ctx: Optional[Context] = None) -> float:
-    return _ctx(ctx).compression_tolerance()
+def SetCompressionTolerance(tol: float):
+    """SetCompressionTolerance (global.cpp:160-181): the relative tolerance
+    of the DistHMat2d / DistHMat3d products.  As in the reference it leaves
+    HMat2d / HMat3d at their fixed rank; ``Context.set_compression_tolerance``
+    applies a tolerance to every product of one context."""
+    if not 0.0 <= tol < 1.0:
+        raise _lib.HMError(1, "compression tolerance must be in [0, 1)")
+    _DIST_TOL[0] = float(tol)
+
+
+def CompressionTolerance() -> float:
+    return _DIST_TOL[0]
+
+
+class _ScopedTolerance:
+    def __init__(self, ctx: "Context", tol: float):
+        self.ctx, self.tol = ctx, tol
+
+    def __enter__(self):
+        self.old = self.ctx.compression_tolerance()
+        self.ctx.set_compression_tolerance(self.tol)
+
+    def __exit__(self, *exc):
+        self.ctx.set_compression_tolerance(self.old)
 
 
 def _as_i32(a):
@@ -559,6 +578,78 @@ class HMat3d(_HMatBase):
     def BuildNaturalToHierarchicalMap(xSize: int, ySize: int, zSize: int,
                                       numLevels: int) -> np.ndarray:
         return natural_to_hierarchical_map((xSize, ySize, zSize), numLevels)
+
+
+class _DistOps:
+    """Single-rank DistHMat2d / DistHMat3d (include/dmhm/dist_hmat2d.hpp): the
+    whole matrix is local, products truncate by the global
+    CompressionTolerance (SVDTrunc, src/DistHMat2d/Truncation-incl.hpp:37-63),
+    and multType has no effect on the result.  The reference compresses with
+    two-sided sketches and Gram eigendecompositions; this engine rounds with
+    QR and a Jacobi SVD under the same truncation rule, so results agree to
+    the tolerance's scale."""
+
+    def LocalHeight(self) -> int:
+        return self.Height()
+
+    def LocalWidth(self) -> int:
+        return self.Width()
+
+    def FirstLocalRow(self) -> int:
+        return 0
+
+    def FirstLocalCol(self) -> int:
+        return 0
+
+    def ParallelEstimateTwoNorm(self, theta: float, confidence: float) -> float:
+        """ParallelEstimateTwoNorm (src/DistHMat2d/Norm-incl.hpp:12-77)."""
+        return EstimateTwoNorm(self, theta, confidence)
+
+    def Multiply(self, alpha, B, beta=None, C=None, multType: int = 2):
+        """Vectors and dense blocks as HMat2d; H*H C := alpha A B under the
+        global compression tolerance (MultiplyHMat-incl.hpp:28-52)."""
+        if isinstance(B, _HMatBase):
+            with _ScopedTolerance(self.ctx, CompressionTolerance()):
+                return super().Multiply(alpha, B, beta, C)
+        return super().Multiply(alpha, B, beta, C)
+
+    def SchulzInvert(self, numIterations: int, multType: int = 2, theta: float = 1.5,
+                     confidence: float = 6.0, stopTol: float = 1e-4, printRank: bool = False):
+        """SchulzInvert (src/DistHMat2d/Invert-incl.hpp:14-105) under the global
+        compression tolerance."""
+        with _ScopedTolerance(self.ctx, CompressionTolerance()):
+            return super().SchulzInvert(numIterations, theta, confidence, stopTol)
+
+
+class Teams:
+    """Teams(mpi::Comm) of the distributed classes: one team of one process."""
+
+    def __init__(self, comm=None):
+        self.comm = comm
+
+    def NumLevels(self) -> int:
+        return 1
+
+
+class DistHMat2d(_DistOps, HMat2d):
+    """Single-rank DistHMat2d<double> (include/dmhm/dist_hmat2d.hpp)."""
+
+    def __init__(self, S: Optional[Sparse] = None, numLevels: int = 1, maxRank: int = 0,
+                 stronglyAdmissible: bool = True, xSize: int = 0, ySize: int = 0,
+                 teams: Optional[Teams] = None, ctx: Optional[Context] = None, _handle=None):
+        HMat2d.__init__(self, S, numLevels, maxRank, stronglyAdmissible, xSize, ySize,
+                        ctx=ctx, _handle=_handle)
+
+
+class DistHMat3d(_DistOps, HMat3d):
+    """Single-rank DistHMat3d<double> (include/dmhm/dist_hmat3d.hpp)."""
+
+    def __init__(self, S: Optional[Sparse] = None, numLevels: int = 1, maxRank: int = 0,
+                 stronglyAdmissible: bool = True, xSize: int = 0, ySize: int = 0,
+                 zSize: int = 0, teams: Optional[Teams] = None, ctx: Optional[Context] = None,
+                 _handle=None):
+        HMat3d.__init__(self, S, numLevels, maxRank, stronglyAdmissible, xSize, ySize, zSize,
+                        ctx=ctx, _handle=_handle)
 
 
 class RankModel:

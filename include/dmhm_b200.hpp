@@ -55,13 +55,38 @@ inline int Oversample() {
     return p;
 }
 inline void SetOversample(int oversample) { Check(hm_set_oversample(Context(), oversample)); }
-// SetCompressionTolerance / CompressionTolerance (src/core/global.cpp:160-181).
-inline void SetCompressionTolerance(double tol) { Check(hm_set_compression_tolerance(Context(), tol)); }
-inline double CompressionTolerance() {
-    double t = 0.0;
-    Check(hm_get_compression_tolerance(Context(), &t));
+// SetCompressionTolerance / CompressionTolerance (src/core/global.cpp:
+// 160-181): the global relative tolerance of the DistHMat products (default
+// 1e-16, global.cpp:34).  As in the reference it does not change HMat2d /
+// HMat3d, whose H*H products truncate to the fixed rank maxRank; the
+// engine's per-context tolerance (hm_set_compression_tolerance) is set to it
+// for the duration of each DistHMat product or inversion.
+namespace detail {
+inline double& DistTol() {
+    static double t = 1e-16;
     return t;
 }
+// sets the context's tolerance for one scope and restores it
+class ScopedTolerance {
+  public:
+    explicit ScopedTolerance(double tol) {
+        Check(hm_get_compression_tolerance(Context(), &old_));
+        Check(hm_set_compression_tolerance(Context(), tol));
+    }
+    ~ScopedTolerance() { hm_set_compression_tolerance(Context(), old_); }
+    ScopedTolerance(const ScopedTolerance&) = delete;
+    ScopedTolerance& operator=(const ScopedTolerance&) = delete;
+
+  private:
+    double old_ = 0.0;
+};
+}  // namespace detail
+inline void SetCompressionTolerance(double tol) {
+    if (!(tol >= 0.0 && tol < 1.0))
+        throw std::runtime_error("dmhm_b200: compression tolerance must be in [0, 1)");
+    detail::DistTol() = tol;
+}
+inline double CompressionTolerance() { return detail::DistTol(); }
 
 // SeedSerialLcg (src/core/random.cpp:67-68): restart the serial generator
 // (the one the randomized H*H sampling and EstimateTwoNorm draw from).
@@ -304,6 +329,85 @@ class HMat3d : public HMatBase<Scalar, 3> {
     void SchulzInvert(int numIterations, Scalar theta = 1.5, Scalar confidence = 6) {
         Check(hm_schulz_invert(this->Need(), numIterations, theta, confidence, 1e-4, nullptr,
                                nullptr, 0, nullptr));
+    }
+};
+
+// ----- single-rank DistHMat2d / DistHMat3d ----------------------------------
+// include/dmhm/dist_hmat2d.hpp (and dist_hmat3d.hpp) on one process: the
+// whole matrix is local (LocalHeight() = Height(), FirstLocalRow() = 0), the
+// products truncate by the global CompressionTolerance (SVDTrunc,
+// src/DistHMat2d/Truncation-incl.hpp:37-63) instead of to the fixed rank,
+// and multType (the reference's accumulation schedules, MultiplyHMat-incl.hpp:
+// 28-52) has no effect on the result here.  The reference compresses with
+// two-sided sketches and Gram eigendecompositions; this engine rounds with
+// QR and a Jacobi SVD under the same truncation rule, so results agree to
+// the tolerance's scale, not bit for bit.
+// Teams(mpi::Comm) of the distributed classes: one team of one process.
+class DistTeams {
+  public:
+    explicit DistTeams(int comm = 0) { (void)comm; }
+    int NumLevels() const { return 1; }
+    int TeamLevel(int) const { return 0; }
+};
+
+namespace detail {
+template <typename Base>
+class DistOps : public Base {
+  public:
+    typedef typename Base::Real Real;
+    typedef DistTeams Teams;
+
+    int LocalHeight() const { return this->Height(); }
+    int LocalWidth() const { return this->Width(); }
+    int FirstLocalRow() const { return 0; }
+    int FirstLocalCol() const { return 0; }
+
+    // ParallelEstimateTwoNorm (src/DistHMat2d/Norm-incl.hpp:12-77)
+    Real ParallelEstimateTwoNorm(Real theta, Real confidence) {
+        double est = 0;
+        Check(hm_estimate_two_norm(this->Handle(), theta, confidence, &est));
+        return est;
+    }
+    using Base::Multiply;
+    // C := alpha A B (MultiplyHMat-incl.hpp:28-52)
+    void Multiply(double alpha, DistOps& B, DistOps& C, int multType = 2) {
+        (void)multType;
+        ScopedTolerance tol(CompressionTolerance());
+        Base::Multiply(alpha, B, C);
+    }
+    // SchulzInvert (src/DistHMat2d/Invert-incl.hpp:14-105)
+    void SchulzInvert(int numIterations, int multType = 2, Real theta = 1.5,
+                      Real confidence = 6, Real stopTol = 1e-4, bool printRank = false) {
+        (void)multType;
+        (void)printRank;
+        ScopedTolerance tol(CompressionTolerance());
+        Check(hm_schulz_invert(this->Handle(), numIterations, theta, confidence, stopTol,
+                               nullptr, nullptr, 0, nullptr));
+    }
+};
+}  // namespace detail
+
+template <typename Scalar>
+class DistHMat2d : public detail::DistOps<HMat2d<Scalar>> {
+  public:
+    DistHMat2d() {}
+    DistHMat2d(const Sparse<Scalar>& S, int numLevels, int maxRank, bool stronglyAdmissible,
+               int xSize, int ySize, const DistTeams& teams) {
+        (void)teams;
+        int sizes[2] = {xSize, ySize};
+        this->FromSparse(S, numLevels, maxRank, stronglyAdmissible, sizes);
+    }
+};
+
+template <typename Scalar>
+class DistHMat3d : public detail::DistOps<HMat3d<Scalar>> {
+  public:
+    DistHMat3d() {}
+    DistHMat3d(const Sparse<Scalar>& S, int numLevels, int maxRank, bool stronglyAdmissible,
+               int xSize, int ySize, int zSize, const DistTeams& teams) {
+        (void)teams;
+        int sizes[3] = {xSize, ySize, zSize};
+        this->FromSparse(S, numLevels, maxRank, stronglyAdmissible, sizes);
     }
 };
 

@@ -90,6 +90,35 @@ int main(int argc, char** argv) {
     X.Multiply(1.0, B, Cd);
     write_bin(dir + "/schulz3.bin", Cd.LockedBuffer(), (size_t)N * k);
     std::printf("norm estimate %.17g\n", hmat_tools::EstimateTwoNorm(A, 1.5, 6.0));
+    // single-rank DistHMat2d: the same operator, A*A under the global
+    // compression tolerance (exact for sparse-built factors), against the
+    // HMat2d product C computed above
+    {
+        SetCompressionTolerance(1e-10);
+        DistHMat2d<double>::Teams teams(0);
+        DistHMat2d<double> DA(S, levels, rank, true, nx, ny, teams), DC;
+        if (DA.LocalHeight() != N || DA.FirstLocalRow() != 0) {
+            std::fprintf(stderr, "DistHMat2d local sizes\n");
+            return 1;
+        }
+        DA.Multiply(1.0, DA, DC, 2);
+        Dense<double> R1, R2;
+        DC.Multiply(1.0, B, R1);
+        C.Multiply(1.0, B, R2);
+        double num = 0, den = 0;
+        for (int j = 0; j < k; ++j)
+            for (int i = 0; i < N; ++i) {
+                const double d = R1.Get(i, j) - R2.Get(i, j);
+                num += d * d;
+                den += R2.Get(i, j) * R2.Get(i, j);
+            }
+        if (!(num <= 1e-20 * den)) {
+            std::fprintf(stderr, "DistHMat2d A*A differs from HMat2d's\n");
+            return 1;
+        }
+        if (!(DA.ParallelEstimateTwoNorm(1.5, 6.0) > 0)) return 1;
+        SetCompressionTolerance(1e-16);
+    }
     // one low-rank approximation of X^T X (hmat_tools::TransposeMultiply)
     LowRank<double> F;
     hmat_tools::TransposeMultiply(HMat2d<double>::SampleRank(X.MaxRank()), 1.0, X, X, F);

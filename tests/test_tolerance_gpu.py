@@ -86,3 +86,34 @@ def test_schulz_with_tolerance_converges():
     P = np.random.default_rng(3).standard_normal((A.Width(), 4))
     res = relerr(X.Multiply(1.0, A.Multiply(1.0, P)), P)
     assert res < 1e-4
+
+
+def test_dist_hmat_single_rank():
+    """Single-rank DistHMat2d: products and SchulzInvert under the global
+    CompressionTolerance (DistHMat semantics) equal the HMat2d ones run with
+    the same tolerance on a context; HMat2d itself stays at fixed rank."""
+    fx = load("c1")
+    sizes = [int(s) for s in fx["sizes"]]
+    L, r = int(fx["levels"]), int(fx["rank"])
+    S = D.operators.stencil(sizes, fx["coef"], L)
+    P = fx["probes"]
+    old = D.CompressionTolerance()
+    try:
+        D.SetCompressionTolerance(1e-10)
+        c1 = D.Context(0)
+        c1.set_oversample(int(fx["oversample"]))
+        A = D.DistHMat2d(S, L, r, True, *sizes, D.Teams(), ctx=c1)
+        assert A.LocalHeight() == A.Height() and A.FirstLocalRow() == 0
+        C = A.Multiply(1.0, A, multType=2)
+        assert c1.compression_tolerance() == 0.0          # restored after the product
+        assert relerr(C.Multiply(1.0, P), fx["hh_AA"]) < 1e-11
+        A.SchulzInvert(6, 2, 1.5, 6.0, 1e-4)
+        c2 = D.Context(0)
+        c2.set_oversample(int(fx["oversample"]))
+        c2.set_compression_tolerance(1e-10)
+        B = D.HMat2d(S, L, r, True, *sizes, ctx=c2)
+        B.Multiply(1.0, B)                                # same generator use as above
+        B.SchulzInvert(6)
+        assert relerr(A.Multiply(1.0, P), B.Multiply(1.0, P)) < 1e-12
+    finally:
+        D.SetCompressionTolerance(old)

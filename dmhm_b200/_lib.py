@@ -58,6 +58,9 @@ SIGNATURES = {
     "hm_create_from_csr_complex": [_P, _I, _PI, _I, _I, _I, _PI64, _PI32, _PD, C.POINTER(_P)],
     "hm_is_complex": [_P, _PI],
     "hm_scale_complex": [_P, _D, _D],
+    "hm_update_with": [_P, _D, _P],
+    "hm_set_to_identity": [_P],
+    "hm_conjugate_in_place": [_P],
     "hm_add_constant_to_diagonal_complex": [_P, _D, _D],
     "hm_conjugate": [_P, C.POINTER(_P)],
     "hm_transpose_complex": [_P, C.POINTER(_P)],

@@ -755,6 +755,31 @@ int hm_transpose_complex(hm_matrix src, hm_matrix* dst) {
     });
 }
 
+int hm_update_with(hm_matrix A, double alpha, hm_matrix B) {
+    return guarded([&] {
+        HMB_REQUIRE(A && B, HM_ERR_ARGUMENT, "NULL argument");
+        hm_context_s* ctx = owner_of(A);
+        HMB_REQUIRE(owner_of(B) == ctx, HM_ERR_ARGUMENT, "matrices live in different contexts");
+        hmat_update_with(ctx->c, A->h, alpha, B->h);
+    });
+}
+
+int hm_set_to_identity(hm_matrix h) {
+    return guarded([&] {
+        HMB_REQUIRE(h, HM_ERR_ARGUMENT, "h is NULL");
+        hmat_set_identity(owner_of(h)->c, h->h);
+    });
+}
+
+int hm_conjugate_in_place(hm_matrix h) {
+    return guarded([&] {
+        HMB_REQUIRE(h, HM_ERR_ARGUMENT, "h is NULL");
+        owner_of(h);
+        HMB_REQUIRE(h->h.S != nullptr, HM_ERR_ARGUMENT, "empty H-matrix");
+        if (h->h.S->dof == 2) complex_conjugate(owner_of(h)->c, h->h);
+    });
+}
+
 int hm_scale(hm_matrix h, double alpha) {
     return guarded([&] {
         HMB_REQUIRE(h, HM_ERR_ARGUMENT, "h is NULL");

@@ -18,5 +18,7 @@ void hmat_copy(Context& ctx, const HMatrix& src, HMatrix& dst);        // CopyFr
 void hmat_transpose(Context& ctx, const HMatrix& src, HMatrix& dst);   // TransposeFrom / AdjointFrom
 void hmat_scale(Context& ctx, HMatrix& H, double alpha);               // Scale
 void hmat_add_diagonal(Context& ctx, HMatrix& H, double alpha);        // AddConstantToDiagonal
+void hmat_update_with(Context& ctx, HMatrix& A, double alpha, const HMatrix& B);  // UpdateWith
+void hmat_set_identity(Context& ctx, HMatrix& H);                     // SetToIdentity
 
 }  // namespace hmb

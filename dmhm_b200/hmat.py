@@ -479,6 +479,20 @@ class _HMatBase:
             return self
         return self.AdjointFrom(B)
 
+    def UpdateWith(self, alpha: float, B: "_HMatBase"):
+        """A := alpha B + A (UpdateWith, HMat2d.cpp:749-781): low-rank blocks
+        by RoundedUpdate to maxRank, dense blocks added."""
+        check(lib().hm_update_with(self._h, float(alpha), B.handle))
+
+    def SetToIdentity(self):
+        """A := I (SetToIdentity, HMat2d.cpp:652-702): low-rank blocks emptied,
+        dense diagonal I."""
+        check(lib().hm_set_to_identity(self._h))
+
+    def Conjugate(self):
+        """A := conj(A) (Conjugate, HMat2d.cpp:396-422); nothing for real."""
+        check(lib().hm_conjugate_in_place(self._h))
+
     def ConjugateFrom(self, B: "_HMatBase"):
         """A := conj(B) (ConjugateFrom, HMat2d.cpp:424-472); complex only."""
         out = _handle_of(self)

@@ -159,6 +159,15 @@ HM_API int hm_multiply_dense_complex_host(hm_matrix h, int op, double alpha_re,
  * *dst == NULL creates a new handle.
  */
 HM_API int hm_scale_complex(hm_matrix h, double alpha_re, double alpha_im);
+/* UpdateWith(alpha, B) (src/HMat2d/HMat2d.cpp:749-781): A := alpha B + A,
+   low-rank blocks by RoundedUpdate to maxRank (src/hmat_tools/
+   RoundedUpdate.cpp:14-162), dense blocks by Update; A and B on one block
+   structure.  SetToIdentity (HMat2d.cpp:652-702): empty low-rank blocks,
+   identity dense diagonal.  Conjugate (HMat2d.cpp:396-422): A := conj(A) in
+   place (nothing to do for a real matrix). */
+HM_API int hm_update_with(hm_matrix A, double alpha, hm_matrix B);
+HM_API int hm_set_to_identity(hm_matrix h);
+HM_API int hm_conjugate_in_place(hm_matrix h);
 HM_API int hm_add_constant_to_diagonal_complex(hm_matrix h, double alpha_re, double alpha_im);
 HM_API int hm_conjugate(hm_matrix src, hm_matrix* dst);
 HM_API int hm_transpose_complex(hm_matrix src, hm_matrix* dst);

@@ -250,6 +250,13 @@ class HMatBase {
     void AdjointFrom(const HMatBase& B) { Check(hm_transpose(B.Need(), &h_)); }
     void TransposeFrom(const HMatBase& B) { Check(hm_transpose(B.Need(), &h_)); }
     void Scale(Scalar alpha) { Check(hm_scale(Need(), alpha)); }
+    // UpdateWith (HMat2d.cpp:749-781): A := alpha B + A
+    void UpdateWith(Scalar alpha, const HMatBase& B) { Check(hm_update_with(Need(), alpha, B.Need())); }
+    // SetToIdentity (HMat2d.cpp:652-702)
+    void SetToIdentity() { Check(hm_set_to_identity(Need())); }
+    // Conjugate / ConjugateFrom (HMat2d.cpp:396-472): nothing to do for real scalars
+    void Conjugate() { Check(hm_conjugate_in_place(Need())); }
+    void ConjugateFrom(const HMatBase& B) { CopyFrom(B); }
     void AddConstantToDiagonal(Scalar alpha) { Check(hm_add_constant_to_diagonal(Need(), alpha)); }
 
   protected:

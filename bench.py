@@ -37,6 +37,14 @@ SIZES, LEVELS, RANK, NRHS, SEED = (128, 128), 5, 16, 64, 2
 REF_DRIVER = os.path.join(ROOT, "oracle", "_ref", "dmhm_ref_driver")
 
 
+# DRAM read + write bytes per launch of the dominant kernels on the bench
+# workload, from one ncu capture each (the profiles/ summaries name the
+# commands): FP64 64-column product phases and the one-vector product
+KERNEL_TRAFFIC = {"hmm_row_tiles": (257.7 + 12.2) * 1e6,
+                  "hmm_lowrank_inner": (127.5 + 46.4) * 1e6,
+                  "hmv_blocks": (276.4 + 3.3) * 1e6}
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -286,13 +294,18 @@ def gpu_arm(args):
     e2e_s = (time.perf_counter() - t0) / e2e_steps
     e2e_val = world * nbytes / e2e_s / 1e9
 
+    # DRAM bytes per launch from the committed ncu captures of this workload
+    # (profiles/wide_kernel_128x128_r16_64rhs.md,
+    # profiles/hmv_blocks_128x128_r16_1rhs.md): read + write
+    traffic = KERNEL_TRAFFIC.get(kname)
     line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic", "config": workload_config(),
             "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved,
                          "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-                         "peak_source": peak_kind, "traffic": None,
+                         "peak_source": peak_kind, "traffic": traffic,
+                         "traffic_source": "ncu capture in profiles/" if traffic else None,
                          "algorithmic_bytes_per_launch": kbytes},
             "e2e": {"value": e2e_val, "unit": "GB/s", "h2d_bytes_per_step": N * NRHS * 8,
                     "d2h_bytes_per_step": N * NRHS * 8},
@@ -373,7 +386,8 @@ def matvec_leg(ctx, H, stream, census, hbm_peak, peak_kind, args):
             "roofline": {"bound": "hbm", "kernel": kname,
                          "achieved": kbytes / (kms * 1e-3) / 1e9, "peak": hbm_peak,
                          "unit": "GB/s", "frac": kbytes / (kms * 1e-3) / 1e9 / hbm_peak,
-                         "peak_source": peak_kind, "algorithmic_bytes_per_launch": kbytes},
+                         "peak_source": peak_kind, "algorithmic_bytes_per_launch": kbytes,
+                         "traffic": KERNEL_TRAFFIC.get(kname)},
             "adjoint_identity_rel_diff": abs(lhs - rhs) / max(abs(lhs), 1e-300),
             "kernels": {k: {"ms_per_launch": v["ms"] / v["launches"], "launches": v["launches"]}
                         for k, v in prof.items()}}

@@ -7,7 +7,7 @@ blocks (1e-12); SchulzInvert (stopTol 1e-8, maxRank 12) is compared with the
 dense inverse on probe vectors to 1e-7, above the truncation floor that
 fixed-rank compression leaves (the reference's own complex run of the first
 case lands 3e-9 from the dense inverse), as the reference's Invert test
-judges its result (tests/HMat2d/Invert.cpp:71-104).
+evaluates its result (tests/HMat2d/Invert.cpp:71-104).
 """
 import numpy as np
 import pytest

@@ -13,6 +13,10 @@
  *           include/dmhm/core/random.hpp:238-445)
  *   cmatvec / chh / cschulz   the same on HMat2d<std::complex<double>> over a
  *           shifted Helmholtz-like operator (RunComplex below)
+ *   dhh / dschulz / dnorm   single-rank DistHMat2d / DistHMat3d (built with
+ *           -DORACLE_WITH_DIST, RunDist below): the H.H product with its
+ *           multType, SchulzInvert and ParallelEstimateTwoNorm under the global
+ *           CompressionTolerance
  *
  * The operator is the grid stencil the workloads use: a 5-point (2-D) or
  * 7-point (3-D) operator in natural x-fastest order, diagonal 2*d*c_i + shift,
@@ -47,14 +51,14 @@ struct DriverArgs
 {
     std::string cmd;
     int dim, nx, ny, nz, levels, rank, oversample, strong, random;
-    int nrhs, repeat, iters, count, useB;
-    double shift, alpha, theta, conf, stopTol, kwave, absorption;
+    int nrhs, repeat, iters, count, useB, mult;
+    double shift, alpha, theta, conf, stopTol, kwave, absorption, tol;
     std::string coef, coefB, x, out;
     DriverArgs()
     : dim(2), nx(32), ny(32), nz(1), levels(4), rank(8), oversample(4),
       strong(1), random(0), nrhs(1), repeat(1), iters(-1), count(16), useB(0),
-      shift(0.1), alpha(1.0), theta(1.5), conf(6.0), stopTol(1e-4), kwave(5.0),
-      absorption(0.2) { }
+      mult(2), shift(0.1), alpha(1.0), theta(1.5), conf(6.0), stopTol(1e-4), kwave(5.0),
+      absorption(0.2), tol(1e-16) { }
 };
 
 std::vector<double> ReadDoubles(const std::string& path, size_t n)
@@ -387,6 +391,97 @@ int Run(const DriverArgs& a)
     return 0;
 }
 
+#ifdef ORACLE_WITH_DIST
+// Single-rank distributed classes over the serial MPI stand-in: one process
+// owns the whole matrix (LocalHeight() == Height(), FirstLocalRow() == 0), so
+// vectors and probes are the same hierarchical-order arrays as above.
+template<typename HMat> struct DistMaker;
+
+template<> struct DistMaker<HMat2d<double> >
+{
+    typedef DistHMat2d<double> D;
+    static D* Make(const DriverArgs& a, const Sparse<double>& S, const D::Teams& t)
+    { return new D(S, a.levels, a.rank, a.strong != 0, a.nx, a.ny, t); }
+    // src/DistHMat2d/Invert-incl.hpp:14-105
+    static void Schulz(D& H, const DriverArgs& a)
+    { H.SchulzInvert(a.iters, a.mult, a.theta, a.conf, a.stopTol); }
+};
+
+template<> struct DistMaker<HMat3d<double> >
+{
+    typedef DistHMat3d<double> D;
+    static D* Make(const DriverArgs& a, const Sparse<double>& S, const D::Teams& t)
+    { return new D(S, a.levels, a.rank, a.strong != 0, a.nx, a.ny, a.nz, t); }
+    // src/DistHMat3d/Invert-incl.hpp (stop test fixed at 1e-4)
+    static void Schulz(D& H, const DriverArgs& a)
+    { H.SchulzInvert(a.iters, a.mult, a.theta, a.conf); }
+};
+
+template<typename HMat>
+int RunDist(const DriverArgs& a)
+{
+    typedef typename DistMaker<HMat>::D DHMat;
+    const int N = a.nx * a.ny * a.nz;
+    Vector<int> map;
+    Maker<HMat>::Map(a, map);
+    std::vector<double> c = ReadDoubles(a.coef, N);
+    Sparse<double> S;
+    BuildSparse(a, c, map, S);
+    SetOversample(a.oversample);
+    SetCompressionTolerance<double>(a.tol);
+    typename DHMat::Teams teams(mpi::COMM_WORLD);
+    DHMat* A = DistMaker<HMat>::Make(a, S, teams);
+    if (A->LocalHeight() != N || A->FirstLocalRow() != 0)
+    { fprintf(stderr, "single-rank DistHMat is not whole\n"); return 3; }
+    std::vector<double> result;
+    double seconds = 0, extra = 0;
+    double t0 = Now();
+    if (a.cmd == "dhh")
+    {
+        // C := alpha A B, B = A or built from --coefB (--useB 1)
+        // (src/DistHMat2d/MultiplyHMat-incl.hpp:28-53)
+        DHMat* B = A;
+        if (a.useB == 1)
+        {
+            std::vector<double> cB = ReadDoubles(a.coefB, N);
+            Sparse<double> SB;
+            BuildSparse(a, cB, map, SB);
+            B = DistMaker<HMat>::Make(a, SB, teams);
+        }
+        std::vector<double> P = ReadDoubles(a.x, (size_t)N * a.nrhs);
+        DHMat C(teams);
+        t0 = Now();
+        A->Multiply(a.alpha, *B, C, a.mult);
+        seconds = Now() - t0;
+        ApplyToProbes(C, P, N, a.nrhs, result);
+        if (B != A) delete B;
+    }
+    else if (a.cmd == "dschulz")
+    {
+        std::vector<double> P = ReadDoubles(a.x, (size_t)N * a.nrhs);
+        t0 = Now();
+        DistMaker<HMat>::Schulz(*A, a);
+        seconds = Now() - t0;
+        ApplyToProbes(*A, P, N, a.nrhs, result);
+    }
+    else if (a.cmd == "dnorm")
+    {
+        extra = A->ParallelEstimateTwoNorm(a.theta, a.conf);
+        seconds = Now() - t0;
+    }
+    else
+    {
+        fprintf(stderr, "unknown command %s\n", a.cmd.c_str());
+        return 2;
+    }
+    if (!a.out.empty()) WriteDoubles(a.out + ".bin", result);
+    printf("{\"cmd\": \"%s\", \"N\": %d, \"seconds\": %.9g, \"iterations\": 0,"
+           " \"value\": %.17g}\n", a.cmd.c_str(), N, seconds, extra);
+    delete A;
+    return 0;
+}
+#endif
+
 // Complex-double path (HMat2d<std::complex<double>>, explicitly instantiated
 // at src/HMat2d/HMat2d.cpp:1321-1324) on the shifted five-point
 // Helmholtz-like operator: diagonal 4 + absorption i - (k h)^2 with
@@ -512,6 +607,8 @@ int main(int argc, char* argv[])
         else if (k == "--iters") a.iters = atoi(v);
         else if (k == "--count") a.count = atoi(v);
         else if (k == "--useB") a.useB = atoi(v);
+        else if (k == "--mult") a.mult = atoi(v);
+        else if (k == "--tol") a.tol = atof(v);
         else if (k == "--shift") a.shift = atof(v);
         else if (k == "--alpha") a.alpha = atof(v);
         else if (k == "--theta") a.theta = atof(v);
@@ -533,6 +630,10 @@ int main(int argc, char* argv[])
     {
         if (a.cmd == "lcg") rc = RunLcg(a);
         else if (a.cmd[0] == 'c') rc = RunComplex(a);
+#ifdef ORACLE_WITH_DIST
+        else if (a.cmd[0] == 'd') rc = a.dim == 2 ? RunDist<HMat2d<double> >(a)
+                                                  : RunDist<HMat3d<double> >(a);
+#endif
         else if (a.dim == 2) rc = Run<HMat2d<double> >(a);
         else rc = Run<HMat3d<double> >(a);
     }

@@ -8,6 +8,7 @@ touch the reference; the fixtures let the GPU tests check parity without it.
     python tests/golden/make_golden.py            # all cases
     python tests/golden/make_golden.py c1 ragged  # some cases
     python tests/golden/make_golden.py cplx       # the complex-double case
+    python tests/golden/make_golden.py d2s d2w d3s  # single-rank DistHMat cases
 """
 from __future__ import annotations
 
@@ -22,6 +23,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 DRIVER = os.path.join(ROOT, "oracle", "_ref", "dmhm_ref_driver")
+DIST_DRIVER = os.path.join(ROOT, "oracle", "_ref", "dmhm_ref_dist_driver")
 
 # name: grid, levels, rank, oversample, strong, coefficient seed, probes
 CASES = {
@@ -36,8 +38,8 @@ CASES = {
 }
 
 
-def run(args, out_prefix):
-    r = subprocess.run([DRIVER] + [str(a) for a in args] + ["--out", out_prefix],
+def run(args, out_prefix, driver=DRIVER):
+    r = subprocess.run([driver] + [str(a) for a in args] + ["--out", out_prefix],
                        capture_output=True, text=True, env={**os.environ, "OPENBLAS_NUM_THREADS": "1"})
     if r.returncode != 0:
         raise RuntimeError(f"reference driver failed: {args}\n{r.stderr}")
@@ -198,10 +200,76 @@ def make_lcg(tmp):
     print("lcg ok")
 
 
+# single-rank DistHMat2d / DistHMat3d (the reference's distributed classes
+# run as one process over the serial MPI stand-in), beside the serial HMat2d /
+# HMat3d on the same operator: products with multType 0 and 2, a fixed-count
+# SchulzInvert and the stop-test SchulzInvert, all under the global
+# CompressionTolerance `tol`
+DIST_CASES = {
+    "d2s": dict(sizes=(32, 32), levels=3, rank=8, oversample=4, strong=1, seed=13, probes=3,
+                tol=1e-8, iters=16),
+    "d2w": dict(sizes=(32, 32), levels=4, rank=8, oversample=4, strong=0, seed=17, probes=3,
+                tol=1e-8, iters=16),
+    "d3s": dict(sizes=(16, 16, 16), levels=3, rank=8, oversample=8, strong=1, seed=19, probes=2,
+                tol=1e-8, iters=14),
+}
+
+
+def make_dist_case(name, spec, tmp):
+    sizes = spec["sizes"]
+    dim = len(sizes)
+    N = int(np.prod(sizes))
+    rng = np.random.default_rng(spec["seed"])
+    coef = 1.0 + rng.random(N)
+    coefB = 1.0 + rng.random(N)
+    P = rng.standard_normal((N, spec["probes"]))
+    cpath, cbpath, ppath = (os.path.join(tmp, f) for f in ("dc.bin", "dcb.bin", "dp.bin"))
+    coef.tofile(cpath)
+    coefB.tofile(cbpath)
+    np.asfortranarray(P).T.copy().tofile(ppath)
+    k = spec["probes"]
+    base = ["--dim", dim, "--nx", sizes[0], "--ny", sizes[1],
+            "--nz", sizes[2] if dim == 3 else 1, "--levels", spec["levels"],
+            "--rank", spec["rank"], "--oversample", spec["oversample"],
+            "--strong", spec["strong"], "--coef", cpath, "--x", ppath, "--nrhs", k]
+    dist = base + ["--tol", spec["tol"]]
+    out = dict(sizes=np.array(sizes), levels=spec["levels"], rank=spec["rank"],
+               oversample=spec["oversample"], strong=spec["strong"], coef=coef, coefB=coefB,
+               probes=P, tol=spec["tol"], iters=spec["iters"])
+    o = os.path.join(tmp, "d")
+
+    def mat(v):
+        return v.reshape(k, N).T.copy()
+
+    def drun(args):
+        info, y = run(args, o, DIST_DRIVER)
+        print(f"  {name} {args[0]} {args[-4:]} {info['seconds']:.2f} s", flush=True)
+        return mat(y)
+
+    for m in (0, 2):
+        out[f"dist_hh_AA_m{m}"] = drun(["dhh"] + dist + ["--mult", m])
+    out["dist_hh_AB_m2"] = drun(["dhh"] + dist + ["--mult", 2, "--useB", 1, "--coefB", cbpath,
+                                                  "--alpha", -0.5])
+    out["dist_schulz"] = drun(["dschulz"] + dist + ["--mult", 2, "--iters", spec["iters"]])
+    out["dist_schulz_stop"] = drun(["dschulz"] + dist + ["--mult", 2, "--iters", -1,
+                                                         "--stopTol", 1e-4])
+    _, y = run(["hh"] + base, o)
+    out["serial_hh_AA"] = mat(y)
+    _, y = run(["schulz"] + base + ["--iters", spec["iters"]], o)
+    out["serial_schulz"] = mat(y)
+    _, y = run(["schulz"] + base + ["--iters", -1, "--stopTol", 1e-4], o)
+    out["serial_schulz_stop"] = mat(y)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name, "ok", sorted(out))
+
+
 def main(argv):
     subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-j8"], check=True,
                    capture_output=True)
-    names = argv or list(CASES) + list(COMPLEX_CASES) + ["lcg", "pack"]
+    names = argv or list(CASES) + list(COMPLEX_CASES) + ["lcg", "pack"] + list(DIST_CASES)
+    if any(n in DIST_CASES for n in names):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-j8", "dist"], check=True,
+                       capture_output=True)
     with tempfile.TemporaryDirectory() as tmp:
         for n in names:
             if n == "lcg":
@@ -210,6 +278,8 @@ def main(argv):
                 make_pack(tmp)
             elif n in COMPLEX_CASES:
                 make_complex_case(n, COMPLEX_CASES[n], tmp)
+            elif n in DIST_CASES:
+                make_dist_case(n, DIST_CASES[n], tmp)
             else:
                 make_case(n, CASES[n], tmp)
 

@@ -14,7 +14,9 @@ It restates, function by function, the reference's serial ``HMat2d`` /
 * ``Multiply`` / ``TransposeMultiply`` against vectors and dense matrices,
 * the H*H ``Multiply`` with randomized low-rank compression, ``RoundedUpdate``,
   ``Compress`` and the dense/low-rank leaf products,
-* ``EstimateTwoNorm`` and ``SchulzInvert``.
+* ``EstimateTwoNorm`` and ``SchulzInvert``,
+* ``SetToIdentity`` and ``DirectInvert`` (recursive Schur complements with
+  LU-inverted dense leaves).
 
 Each function cites the reference file:line it follows.  The oracle is pinned
 against the reference itself: ``oracle/Makefile`` compiles the unmodified
@@ -779,6 +781,84 @@ def add_constant_to_diagonal(H: HMat, alpha):
     elif H.kind == DENSE:
         k = min(H.D.shape)
         H.D[np.arange(k), np.arange(k)] += alpha
+
+
+def set_to_identity(H: HMat):
+    """SetToIdentity (src/HMat2d/HMat2d.cpp:650-702): diagonal children
+    recursively, Scale(0) elsewhere (low-rank blocks drop to rank 0); a dense
+    block becomes the leading identity.  A low-rank block is left alone, as
+    the RELEASE build does."""
+    if H.kind == NODE:
+        q = H.nchild_side
+        for t in range(q):
+            for s in range(q):
+                if s == t:
+                    set_to_identity(H.child(t, s))
+                else:
+                    scale(H.child(t, s), 0.0)
+    elif H.kind == DENSE:
+        H.D = np.zeros_like(H.D)
+        k = min(H.D.shape)
+        H.D[np.arange(k), np.arange(k)] = 1.0
+
+
+def invert_dense(D: np.ndarray) -> np.ndarray:
+    """hmat_tools::Invert, non-symmetric branch (src/hmat_tools/Invert.cpp
+    :14-42): LU with partial pivoting (?getrf) and the inverse from the
+    factors (?getri, workspace n * 32 as lapack.hpp:1500-1504)."""
+    from scipy.linalg import lapack
+    n = D.shape[0]
+    lu, piv, info = lapack.dgetrf(np.asfortranarray(D))
+    if info < 0:
+        raise ValueError("dgetrf: bad argument %d" % -info)
+    inv, info = lapack.dgetri(lu, piv, lwork=max(1, 32 * n))
+    if info < 0:
+        raise ValueError("dgetri: bad argument %d" % -info)
+    return np.array(inv)
+
+
+def direct_invert(H: HMat, rng: Rng):
+    """A := inv(A) in place by recursive Schur complements (DirectInvert,
+    src/HMat2d/Invert-incl.hpp:17-125; 3-D src/HMat3d/Invert-incl.hpp:14-122).
+
+    Block Gauss-Jordan over the 2^d x 2^d children: B keeps a copy of A, A
+    starts as the identity; for each pivot l the diagonal child is inverted
+    recursively, row l of A and of B is multiplied by it, and the rows below
+    are eliminated; a backward sweep then clears the rows above.  Every
+    product is the H*H product above (fresh for the row scalings, the
+    update form for the eliminations), in the reference's order, so the
+    generator is drawn in the same sequence."""
+    if H.kind == DENSE:
+        H.D = invert_dense(H.D)
+        return
+    if H.kind != NODE:
+        return
+    q = H.nchild_side
+    B = copy(H)
+    set_to_identity(H)
+    A = H
+
+    def put(M: HMat, t: int, s: int, X: HMat):
+        M.children[s + q * t] = X
+
+    for l in range(q):
+        put(A, l, l, copy(B.child(l, l)))
+        direct_invert(A.child(l, l), rng)
+        for j in range(l):
+            C = copy(A.child(l, j))
+            put(A, l, j, hh_multiply(A.child(l, l), 1.0, C, rng))
+        for j in range(l + 1, q):
+            C = copy(B.child(l, j))
+            put(B, l, j, hh_multiply(A.child(l, l), 1.0, C, rng))
+        for i in range(l + 1, q):
+            for j in range(l + 1):
+                hh_multiply_update(B.child(i, l), -1.0, A.child(l, j), 1.0, A.child(i, j), rng)
+            for j in range(l + 1, q):
+                hh_multiply_update(B.child(i, l), -1.0, B.child(l, j), 1.0, B.child(i, j), rng)
+    for l in range(q - 1, -1, -1):
+        for i in range(l - 1, -1, -1):
+            for j in range(q):
+                hh_multiply_update(B.child(i, l), -1.0, A.child(l, j), 1.0, A.child(i, j), rng)
 
 
 def estimate_two_norm(H: HMat, theta: float, confidence: float, rng: Rng) -> float:

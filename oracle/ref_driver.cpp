@@ -9,6 +9,8 @@
  *                               dense form src/HMat2d/MultiplyDense-incl.hpp:56-68)
  *   hh      C = alpha A B      (HMat2d::Multiply H.H, src/HMat2d/MultiplyHMat-incl.hpp:12-187)
  *   schulz  SchulzInvert       (src/HMat2d/Invert-incl.hpp:127-196; 3-D :127-186)
+ *   direct  DirectInvert       (src/HMat2d/Invert-incl.hpp:17-125; 3-D src/HMat3d/
+ *                               Invert-incl.hpp:14-122), X applied to the probes
  *   lcg     first draws of the serial generator (src/core/random.cpp:13-119,
  *           include/dmhm/core/random.hpp:238-445)
  *   cmatvec / chh / cschulz   the same on HMat2d<std::complex<double>> over a
@@ -251,6 +253,16 @@ int Run(const DriverArgs& a)
         X.CopyFrom(*A);
         double t0 = Now();
         Maker<HMat>::Schulz(X, a);
+        seconds = Now() - t0;
+        ApplyToProbes(X, P, N, a.nrhs, result);
+    }
+    else if (a.cmd == "direct")
+    {
+        std::vector<double> P = ReadDoubles(a.x, (size_t)N * a.nrhs);
+        HMat X;
+        X.CopyFrom(*A);
+        double t0 = Now();
+        X.DirectInvert();
         seconds = Now() - t0;
         ApplyToProbes(X, P, N, a.nrhs, result);
     }

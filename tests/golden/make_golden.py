@@ -28,13 +28,14 @@ DIST_DRIVER = os.path.join(ROOT, "oracle", "_ref", "dmhm_ref_dist_driver")
 # name: grid, levels, rank, oversample, strong, coefficient seed, probes
 CASES = {
     "c1": dict(sizes=(32, 32), levels=4, rank=8, oversample=4, strong=1, seed=1, probes=4,
-               ops=["matvec", "random", "hh_AA", "hh_AB", "schulz3", "schulz_stop", "lrprod"]),
+               ops=["matvec", "random", "hh_AA", "hh_AB", "schulz3", "schulz_stop", "lrprod",
+                    "direct"]),
     "ragged": dict(sizes=(24, 20), levels=3, rank=6, oversample=4, strong=1, seed=5, probes=3,
-                   ops=["matvec", "random", "hh_AA", "hh_AB", "schulz3", "lrprod"]),
+                   ops=["matvec", "random", "hh_AA", "hh_AB", "schulz3", "lrprod", "direct"]),
     "weak": dict(sizes=(16, 16), levels=3, rank=4, oversample=4, strong=0, seed=7, probes=3,
-                 ops=["matvec", "random", "hh_AA", "schulz3"]),
+                 ops=["matvec", "random", "hh_AA", "schulz3", "direct"]),
     "c3d": dict(sizes=(16, 16, 16), levels=3, rank=8, oversample=8, strong=1, seed=9, probes=2,
-                ops=["matvec", "random", "hh_AA", "schulz2"]),
+                ops=["matvec", "random", "hh_AA", "schulz2", "direct"]),
 }
 
 
@@ -107,6 +108,11 @@ def make_case(name, spec, tmp):
             out[op] = mat(y)
             out[op + "_trace"] = np.fromfile(o + ".trace.bin")
             out[op + "_seconds"] = info["seconds"]
+        elif op == "direct":
+            # DirectInvert (recursive Schur complements) applied to the probes
+            info, y = run(["direct"] + base + ["--x", ppath, "--nrhs", k], o)
+            out["direct"] = mat(y)
+            out["direct_seconds"] = info["seconds"]
         elif op == "schulz_stop":
             info, y = run(["schulz_trace"] + base + ["--x", ppath, "--nrhs", k, "--iters", -1,
                                                      "--stopTol", 1e-4], o)

@@ -86,6 +86,22 @@ def test_schulz_iterations(case, its):
     assert relerr(O.multiply_dense(X, 1.0, fx["probes"]), fx[key]) < 1e-8
 
 
+@pytest.mark.parametrize("case,bound", [("c1", 1e-5), ("ragged", 1e-5), ("weak", 0.1),
+                                        ("c3d", 1e-4)])
+def test_direct_invert(case, bound):
+    """DirectInvert (recursive Schur complements) equals the reference's to
+    rounding: the oracle draws the generator in the reference's order, and
+    the result is the inverse to the accuracy of its fixed-rank products."""
+    fx = load(case)
+    A = oracle_hmat(fx)
+    O.direct_invert(A, O.Rng(int(fx["oversample"])))
+    Y = O.multiply_dense(A, 1.0, fx["probes"])
+    assert relerr(Y, fx["direct"]) < 1e-12
+    # against the exact inverse: weak admissibility at rank 4 is lossy
+    Ad = O.to_dense(oracle_hmat(fx))              # A itself is exact (dense leaves)
+    assert relerr(fx["direct"], np.linalg.solve(Ad, fx["probes"])) < bound
+
+
 @pytest.mark.parametrize("case", ["c1", "ragged"])
 def test_low_rank_products(case):
     """hmat_tools::Multiply / TransposeMultiply (F := alpha A B, alpha A^T B

@@ -45,6 +45,48 @@ KERNEL_TRAFFIC = {"hmm_row_tiles": (257.7 + 12.2) * 1e6,
                   "hmv_blocks": (276.4 + 3.3) * 1e6}
 
 
+class Replicas:
+    """N independent replicas of the workload, one process per GPU (the path
+    does not shard: no data crosses between ranks).  Ranks meet only to
+    line up the timed region and to take the slowest rank's time, so the
+    whole-job rate is the units all ranks processed over the max over ranks.
+    Every rank takes the same collective steps in the same order."""
+
+    def __init__(self, backend: str = "nccl", device=None, timeout_s: float = 120.0):
+        import datetime
+
+        import torch.distributed as dist
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.device = device
+        self._dist = dist
+        if self.world > 1:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+
+    def barrier(self):
+        if self.world > 1:
+            self._dist.barrier()
+
+    def max(self, x: float) -> float:
+        """The largest value of x over all ranks (x itself with one rank)."""
+        if self.world == 1:
+            return float(x)
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64, device=self.device)
+        self._dist.all_reduce(t, op=self._dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def rate(self, units_per_rank: float, seconds_per_rank: float) -> float:
+        """Whole-job rate: all ranks' units over the slowest rank's time
+        (seconds_per_rank is this rank's own time; the max is taken here)."""
+        return self.world * units_per_rank / self.max(seconds_per_rank)
+
+    def close(self):
+        if self.world > 1:
+            self._dist.barrier()
+            self._dist.destroy_process_group()
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -202,18 +244,14 @@ def workload_config():
 
 def gpu_arm(args):
     import torch
-    import torch.distributed as dist
 
     import dmhm_b200 as D
     from dmhm_b200 import _lib
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    group = Replicas("nccl", device=f"cuda:{local}")
+    world, rank = group.world, group.rank
 
     stream = torch.cuda.Stream()
     ctx = D.Context(local, stream=stream.cuda_stream)
@@ -236,8 +274,7 @@ def gpu_arm(args):
     for _ in range(args.warmup):
         step()
     ctx.synchronize()
-    if world > 1:
-        dist.barrier()
+    group.barrier()
     ctx.synchronize()
     # timed region: CUDA events on the context's stream around the K steps
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -251,11 +288,7 @@ def gpu_arm(args):
         ctx.synchronize()
         wall = time.perf_counter() - t0
     launches = lib.hm_kernel_launches() - launches0
-    step_ms = ev0.elapsed_time(ev1) / args.steps
-    if world > 1:
-        t = torch.tensor([step_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        step_ms = float(t.item())
+    step_ms = group.max(ev0.elapsed_time(ev1) / args.steps)
     value = world * nbytes / (step_ms * 1e-3) / 1e9
     # per-kernel event timing (separate pass, events bracket each launch)
     _lib.check(lib.hm_profile_enable(ctx.handle, 1))
@@ -291,8 +324,7 @@ def gpu_arm(args):
     for _ in range(e2e_steps):
         _lib.check(lib.hm_multiply_dense_host(H.handle, 0, 1.0, Xp.ctypes.data_as(_lib._PD), N,
                                               0.0, Yp.ctypes.data_as(_lib._PD), N, NRHS))
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    e2e_val = world * nbytes / e2e_s / 1e9
+    e2e_val = group.rate(nbytes, (time.perf_counter() - t0) / e2e_steps) / 1e9
 
     # DRAM bytes per launch from the committed ncu captures of this workload
     # (profiles/wide_kernel_128x128_r16_64rhs.md,
@@ -325,9 +357,7 @@ def gpu_arm(args):
                                                       args.helmholtz_max_side or None)
     if rank == 0:
         print(json.dumps(line))
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    group.close()
 
 
 def _time_steps(stream, fn, steps):

@@ -121,17 +121,28 @@ def kept(sq_norms_sorted: np.ndarray, rout: int, tol: float) -> int:
 
 
 def round_factors(U: np.ndarray, V: np.ndarray, rout: int, tol: float = 0.0,
-                  dtype=np.float64):
+                  dtype=np.float64, precondition: bool = False):
     """The general rounding: U V^T (m x n, k terms) to at most rout terms.
 
     QR of U and of V, core M = R_u R_v^T (min(m, k) x min(n, k)), its Jacobi
     SVD, columns by decreasing norm, the kept count, then
     U_out = Q_u M_out[:, kept], V_out = Q_v J[:, kept] (so U_out has the
     singular values in its column norms and V_out orthonormal columns).
-    Returns (U_out, V_out, sweeps)."""
+
+    With `precondition` the Jacobi runs on R_4^T, where M^T = Q_4 R_4 (one
+    more QR of the core; Drmac and Veselic, SIAM J. Matrix Anal. Appl. 29,
+    2008): R_4^T J = W gives M = W (Q_4 J)^T, so U_out = Q_u W[:, kept] and
+    V_out = Q_v Q_4 J[:, kept] keep the same convention, in fewer sweeps on
+    graded cores.  Returns (U_out, V_out, sweeps)."""
     Qu, Ru = sla.qr(np.asarray(U, dtype=dtype), mode="economic")
     Qv, Rv = sla.qr(np.asarray(V, dtype=dtype), mode="economic")
-    M, J, sweeps = jacobi(Ru @ Rv.T, dtype)
+    core = Ru @ Rv.T
+    if precondition:
+        Q4, R4 = sla.qr(core.T, mode="economic")
+        M, J, sweeps = jacobi(R4.T, dtype)
+        J = Q4 @ J
+    else:
+        M, J, sweeps = jacobi(core, dtype)
     order = column_order(M)
     sq = np.sum(M * M, axis=0)[order]
     keep = kept(sq, rout, tol)

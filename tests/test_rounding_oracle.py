@@ -104,3 +104,22 @@ def test_rounding_tolerance_rule_against_lapack(tol):
     Uo, Vo, _ = R.round_factors(U, V, 64, tol)
     want = R.kept(sla.svdvals(U @ V.T) ** 2, 64, tol)
     assert Uo.shape[1] == want == max(1, int(np.sum(sig > tol * sig[0])))
+
+
+@pytest.mark.parametrize("k,rout", [(24, 16), (40, 32), (12, 8)])
+def test_preconditioned_rounding_same_result_fewer_sweeps(k, rout):
+    """Jacobi on R_4^T (M^T = Q_4 R_4) returns the same rounding, in the
+    same convention (singular values in U, V orthonormal), with fewer
+    sweeps on a graded core."""
+    rng = np.random.default_rng(k + rout)
+    m, n = 64, 64
+    U = spectrum_matrix(rng, m, k, np.logspace(0, -12, k))
+    V = rng.standard_normal((n, k))
+    U1, V1, s1 = R.round_factors(U, V, rout)
+    U2, V2, s2 = R.round_factors(U, V, rout, precondition=True)
+    A = U @ V.T
+    assert np.linalg.norm(U1 @ V1.T - U2 @ V2.T) <= 1e-12 * np.linalg.norm(A)
+    assert np.allclose(np.linalg.norm(U1, axis=0), np.linalg.norm(U2, axis=0),
+                       rtol=1e-10, atol=1e-13 * np.linalg.norm(A))
+    assert np.linalg.norm(V2.T @ V2 - np.eye(V2.shape[1])) < 1e-13
+    assert s2 < s1

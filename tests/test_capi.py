@@ -55,3 +55,23 @@ def test_stencil_operator_matches_oracle():
         r, cc, v, _ = O.stencil_csr(sizes, c, L)
         assert (S.rowOffsets == r).all() and (S.columnIndices == cc).all()
         assert np.array_equal(S.nonzeros, v)
+
+
+def test_cpp_facade_builds_against_the_library(tmp_path):
+    """The header-only C++ facade (include/dmhm_b200.hpp) and the C header
+    compile in a C++17 program that uses the whole facade (the GPU test's
+    driver, tests/cpp/facade_check.cpp) and link against the built library:
+    every entry point the facade calls resolves."""
+    import shutil
+    import subprocess
+    import pytest
+    if shutil.which("g++") is None:
+        pytest.skip("no host C++ compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    libdir = os.path.dirname(_lib.LIB_PATH)
+    exe = tmp_path / "facade_check"
+    r = subprocess.run(["g++", "-O0", "-std=c++17", "-Wall", "-I", os.path.join(root, "include"),
+                        os.path.join(root, "tests", "cpp", "facade_check.cpp"), "-o", str(exe),
+                        "-L", libdir, "-ldmhm_b200", f"-Wl,-rpath,{libdir}"],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]

@@ -12,11 +12,10 @@ of the reference's (1.5x for one product, 3x for a fixed-count Schulz
 inverse, 10x for the stop-test one, whose error depends on where the stop
 test fell), and the two results agree to within that error.  Products of
 the sparse-built strongly admissible matrices are exact in both (1e-11)."""
-import numpy as np
 import pytest
 
 import dmhm_b200 as D
-from helpers import load, relerr
+from helpers import load, relerr, stencil_exact as exact
 
 pytestmark = pytest.mark.gpu
 
@@ -29,15 +28,6 @@ def dist_of(fx, coef_key, ctx):
     S = D.operators.stencil(sizes, fx[coef_key], L)
     cls = D.DistHMat2d if len(sizes) == 2 else D.DistHMat3d
     return cls(S, L, int(fx["rank"]), bool(fx["strong"]), *sizes, D.Teams(), ctx=ctx)
-
-
-def exact(fx):
-    sizes = [int(s) for s in fx["sizes"]]
-    L = int(fx["levels"])
-    A = D.operators.dense_from_sparse(D.operators.stencil(sizes, fx["coef"], L))
-    B = D.operators.dense_from_sparse(D.operators.stencil(sizes, fx["coefB"], L))
-    P = fx["probes"]
-    return dict(AA=A @ (A @ P), AB=-0.5 * (A @ (B @ P)), inv=np.linalg.solve(A, P))
 
 
 def close_at_scale(mine, ref, truth, factor):

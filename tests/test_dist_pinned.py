@@ -15,24 +15,12 @@ GPU engine that follow them, round after each contribution.  Both are
 approximations of the same product, so these tests compare them at the
 approximation's own scale: each against exact dense algebra, and with each
 other within that error."""
-import numpy as np
 import pytest
 
-from helpers import load, relerr
-from dmhm_b200 import operators as ops
+from helpers import load, relerr, stencil_exact as exact
 from oracle import dmhm_oracle as O
 
 CASES = ["d2s", "d2w", "d3s"]
-
-
-def exact(fx):
-    """Exact A*A P, -0.5 A*B P and inv(A) P of a fixture (dense algebra)."""
-    sizes = [int(s) for s in fx["sizes"]]
-    L = int(fx["levels"])
-    A = ops.dense_from_sparse(ops.stencil(sizes, fx["coef"], L))
-    B = ops.dense_from_sparse(ops.stencil(sizes, fx["coefB"], L))
-    P = fx["probes"]
-    return dict(AA=A @ (A @ P), AB=-0.5 * (A @ (B @ P)), inv=np.linalg.solve(A, P))
 
 
 @pytest.mark.parametrize("case", CASES)

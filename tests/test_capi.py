@@ -75,3 +75,12 @@ def test_cpp_facade_builds_against_the_library(tmp_path):
                         "-L", libdir, "-ldmhm_b200", f"-Wl,-rpath,{libdir}"],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-3000:]
+
+
+def test_workloads_module_imports_and_rejects_unknown_cases():
+    """The profiling workloads (dmhm_b200/workloads.py, named by the
+    commands in profiles/) import without a GPU and refuse unknown names."""
+    import pytest
+    from dmhm_b200 import workloads
+    with pytest.raises(SystemExit):
+        workloads.main(["no_such_workload"])

@@ -38,8 +38,9 @@ REF_DRIVER = os.path.join(ROOT, "oracle", "_ref", "dmhm_ref_driver")
 
 
 # DRAM read + write bytes per launch of the dominant kernels on the bench
-# workload, from one ncu capture each (the profiles/ summaries name the
-# commands): FP64 64-column product phases and the one-vector product
+# workload, each from one ncu capture (dram__bytes_read.sum +
+# dram__bytes_write.sum) of `python -m dmhm_b200.workloads`: FP64 64-column
+# product phases and the one-vector product
 KERNEL_TRAFFIC = {"hmm_row_tiles": (257.7 + 12.2) * 1e6,
                   "hmm_lowrank_inner": (127.5 + 46.4) * 1e6,
                   "hmv_blocks": (276.4 + 3.3) * 1e6}
@@ -203,13 +204,20 @@ def run_reference_driver(coef, X, repeat, threads):
 
 
 def ref_bytes(N, nrhs):
-    return census_bytes(SIZES, LEVELS, RANK) + 2 * N * 8 * nrhs
+    return 8 * sum(census_entries(SIZES, LEVELS, RANK)) + 2 * N * 8 * nrhs
 
 
 def census_bytes(sizes, levels, rank, strong=True):
     """Bytes of the SetToRandom operator's blocks (dense leaves m*n, low-rank
-    (m+n)*rank), from the block structure alone (include/dmhm/hmat2d.hpp:
-    288-341, admissibility src/HMat2d/HMat2d.cpp:797-809)."""
+    (m+n)*rank), from the block structure alone."""
+    return 8 * sum(census_entries(sizes, levels, rank, strong))
+
+
+def census_entries(sizes, levels, rank, strong=True):
+    """(dense-leaf entries, U entries, V entries) of an operator whose every
+    admissible block has rank `rank` (SetToRandom), from the block structure
+    alone (include/dmhm/hmat2d.hpp:288-341, admissibility
+    src/HMat2d/HMat2d.cpp:797-809): dense leaves m*n, U m*rank, V n*rank."""
     d = len(sizes)
 
     def kids(box):
@@ -226,13 +234,50 @@ def census_bytes(sizes, levels, rank, strong=True):
         dif = [abs(a - b) for a, b in zip(t[0], s[0])]
         m, n = int(np.prod(t[1])), int(np.prod(s[1]))
         if (max(dif) > 1) if strong else any(dif):
-            return (m + n) * rank
+            return np.array([0, m * rank, n * rank])
         if levels - level > 1:
             return sum(rec(tc, sc, level + 1) for tc in kids(t) for sc in kids(s))
-        return m * n
+        return np.array([m * n, 0, 0])
 
     root = (tuple([0] * d), tuple(sizes))
-    return 8 * rec(root, root, 0)
+    return tuple(int(v) for v in rec(root, root, 0))
+
+
+def phase_work(entries, N, nrhs, rank_sum):
+    """Algorithmic bytes and flops of one launch of each phase of the FP64
+    H x dense product with nrhs columns (s = 8 bytes):
+      hmm_lowrank_inner  T = V^T X for every low-rank block: reads every V
+                         entry and the input rows once, writes T
+                         (rank_sum x nrhs); 2 V nrhs flop;
+      hmm_row_tiles      Y = sum U T + sum D X: reads every U and dense entry,
+                         T and the input rows once, writes Y; 2 (U + D) nrhs
+                         flop."""
+    dense, u, v = entries
+    s = 8
+    io = N * nrhs * s
+    t = rank_sum * nrhs * s
+    return {"hmm_lowrank_inner": {"bytes": v * s + io + t, "flops": 2.0 * v * nrhs},
+            "hmm_row_tiles": {"bytes": (u + dense) * s + t + 2 * io,
+                              "flops": 2.0 * (u + dense) * nrhs}}
+
+
+def fp64_peaks(device):
+    """FP64 throughput (TFLOP/s) of each instruction form on this GPU, from
+    the library's register-only calibration kernels (hm_measure_fp64_peak);
+    the largest is the FP64 roofline of the product kernels."""
+    import ctypes as C
+    from dmhm_b200 import _lib
+    names = {0: "mma_m8n8k4", 1: "mma_m16n8k4", 2: "mma_m16n8k8", 3: "mma_m16n8k16", 4: "fma"}
+    out = {}
+    for form, nm in names.items():
+        tf, ms = C.c_double(), C.c_double()
+        best = 0.0
+        for _ in range(3):
+            _lib.check(_lib.lib().hm_measure_fp64_peak(device, form, 20000, C.byref(tf),
+                                                       C.byref(ms)))
+            best = max(best, tf.value)
+        out[nm] = best
+    return out
 
 
 def workload_config():
@@ -297,18 +342,30 @@ def gpu_arm(args):
     prof = read_profile(ctx)
     _lib.check(lib.hm_profile_enable(ctx.handle, 0))
 
-    # roofline of the dominant kernel: the two phases of the product take
-    # nearly equal time, so the choice is made by a 10 % margin with the
-    # output phase (hmm_row_tiles, the larger share of the bytes) preferred
-    # on a tie, which keeps the reported kernel the same from run to run
+    # roofline: every phase's algorithmic bytes and flops (structural census
+    # of the SetToRandom operator) over its per-launch CUDA-event time; both
+    # phases do 16 flop per byte at 64 columns, above the FP64 ridge point
+    # (measured FP64 peak / measured copy bandwidth), so the bound is the FP64
+    # tensor pipe, and the peak is the best FP64 form measured on this GPU in
+    # this run; the dominant kernel is the one with the larger time
     hbm_peak, peak_kind = peaks()
-    top = max(prof.items(), key=lambda kv: kv[1]["ms"])
-    if "hmm_row_tiles" in prof and prof["hmm_row_tiles"]["ms"] >= 0.9 * top[1]["ms"]:
-        top = ("hmm_row_tiles", prof["hmm_row_tiles"])
-    kname, kv = top
-    per_launch_ms = kv["ms"] / kv["launches"]
-    kbytes = kernel_bytes(kname, census, N, NRHS, H)
-    achieved = kbytes / (per_launch_ms * 1e-3) / 1e9
+    fp64 = fp64_peaks(local)
+    fp64_peak = max(fp64.values())
+    work = phase_work(census_entries(SIZES, LEVELS, RANK), N, NRHS, census["rank_sum"])
+    phases = {}
+    for k, w in work.items():
+        if k not in prof:
+            continue
+        kms = prof[k]["ms"] / prof[k]["launches"]
+        tf = w["flops"] / (kms * 1e-3) / 1e12
+        gbs = w["bytes"] / (kms * 1e-3) / 1e9
+        phases[k] = {"ms_per_launch": kms, "algorithmic_flops_per_launch": w["flops"],
+                     "algorithmic_bytes_per_launch": w["bytes"], "tflops": tf,
+                     "frac_of_fp64_peak": tf / fp64_peak, "gbs": gbs,
+                     "frac_of_hbm": gbs / hbm_peak, "traffic": KERNEL_TRAFFIC.get(k)}
+    kname = max(phases, key=lambda k: phases[k]["ms_per_launch"])
+    kp = phases[kname]
+    step_flops = sum(w["flops"] for w in work.values())
 
     # end to end through the C ABI with host buffers (pinned host memory,
     # column-major N x k: the transposed view of a pinned k x N tensor)
@@ -326,19 +383,26 @@ def gpu_arm(args):
                                               0.0, Yp.ctypes.data_as(_lib._PD), N, NRHS))
     e2e_val = group.rate(nbytes, (time.perf_counter() - t0) / e2e_steps) / 1e9
 
-    # DRAM bytes per launch from the committed ncu captures of this workload
-    # (profiles/wide_kernel_128x128_r16_64rhs.md,
-    # profiles/hmv_blocks_128x128_r16_1rhs.md): read + write
-    traffic = KERNEL_TRAFFIC.get(kname)
     line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic", "config": workload_config(),
-            "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved,
-                         "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-                         "peak_source": peak_kind, "traffic": traffic,
-                         "traffic_source": "ncu capture in profiles/" if traffic else None,
-                         "algorithmic_bytes_per_launch": kbytes},
+            "roofline": {"bound": "tensor", "kernel": kname, "achieved": kp["tflops"],
+                         "peak": fp64_peak, "unit": "TFLOP/s",
+                         "frac": kp["tflops"] / fp64_peak,
+                         "peak_source": "measured in this run: FP64 tensor-core throughput "
+                                        "(best mma.sync .f64 form, hm_measure_fp64_peak)",
+                         "traffic": kp["traffic"],
+                         "traffic_source": ("DRAM read + write bytes per launch from an ncu "
+                                            "capture of this workload (constant in bench.py)"),
+                         "ms_per_launch": kp["ms_per_launch"],
+                         "algorithmic_flops_per_launch": kp["algorithmic_flops_per_launch"],
+                         "algorithmic_bytes_per_launch": kp["algorithmic_bytes_per_launch"],
+                         "hbm_achieved_gbs": kp["gbs"], "hbm_peak_gbs": hbm_peak,
+                         "hbm_frac": kp["frac_of_hbm"], "hbm_peak_source": peak_kind},
+            "fp64_peaks_tflops": fp64, "phases": phases,
+            "step_tflops": step_flops / (step_ms * 1e-3) / 1e12,
+            "step_frac_of_fp64_peak": step_flops / (step_ms * 1e-3) / 1e12 / fp64_peak,
             "e2e": {"value": e2e_val, "unit": "GB/s", "h2d_bytes_per_step": N * NRHS * 8,
                     "d2h_bytes_per_step": N * NRHS * 8},
             "gpu_launches": int(launches), "clocks": clk.summary(),
@@ -457,17 +521,6 @@ def tf32_leg(ctx, H, stream, X, Y, nrhs, nbytes, args):
             "rel_err_vs_fp64": forms["autotuned"]["rel_err_vs_fp64"],
             "autotuned_choice": {1: "tcgen05", 2: "mma_sync"}[w.value], "forms": forms,
             "dtype": "tf32 inputs, f32 accumulation"}
-
-
-def kernel_bytes(name, census, N, nrhs, H):
-    """Algorithmic bytes one launch of `name` must move: phase 1 reads every
-    V (n x r) and its input rows; phase 2 reads every U row slice and dense
-    leaf once and writes the output."""
-    from dmhm_b200 import _lib  # noqa: F401
-    tot = census["bytes"]
-    if name == "hmm_lowrank_inner":
-        return tot // 2 + N * 8 * nrhs            # roughly the V half of the low-rank data
-    return tot + 2 * N * 8 * nrhs
 
 
 def read_profile(ctx):

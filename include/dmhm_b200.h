@@ -348,6 +348,16 @@ HM_API int hm_profile_enable(hm_context ctx, int on);
 HM_API int hm_profile_read(hm_context ctx, int index, char* name, int name_cap,
                            double* ms, int64_t* launches);
 
+/* Measurement aid (no reference counterpart): FP64 throughput of one
+   instruction form on `device`, from a register-only kernel of the library
+   (4 CTAs of 256 threads per SM, 8 independent accumulators per thread,
+   `iterations` rounds), timed with CUDA events on a private stream.
+   form: 0 mma.sync m8n8k4 .f64, 1 m16n8k4 .f64, 2 m16n8k8 .f64,
+   3 m16n8k16 .f64, 4 scalar fma.rn.f64.  *tflops receives 1e-12 flop/s;
+   *ms (may be NULL) the launch time. */
+HM_API int hm_measure_fp64_peak(int device, int form, int iterations, double* tflops,
+                                double* ms);
+
 #ifdef __cplusplus
 }
 #endif

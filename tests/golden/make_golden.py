@@ -9,6 +9,9 @@ touch the reference; the fixtures let the GPU tests check parity without it.
     python tests/golden/make_golden.py c1 ragged  # some cases
     python tests/golden/make_golden.py cplx       # the complex-double case
     python tests/golden/make_golden.py d2s d2w d3s  # single-rank DistHMat cases
+    python tests/golden/make_golden.py cfg2 cfg1s cfg3 cfg4   # benchmark sizes
+                                                   # (not in the default set: cfg4
+                                                   # runs for many minutes)
 """
 from __future__ import annotations
 
@@ -19,6 +22,9 @@ import sys
 import tempfile
 
 import numpy as np
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+from helpers import big_case_inputs  # noqa: E402
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
@@ -269,6 +275,74 @@ def make_dist_case(name, spec, tmp):
     print(name, "ok", sorted(out))
 
 
+# Cases at the benchmark workloads' own sizes.  Their inputs (coefficient
+# fields and right-hand sides) come from a counter-based hash
+# (``hashed_uniform``), so the tests regenerate them exactly and the fixtures
+# hold only the reference's outputs, reduced to a few full columns plus a
+# sketch G^T Y of every column (G hashed too).
+#   kind "matmat": y = H X and y = H^T X for a SetToRandom H (64 columns)
+#   kind "schulz": SchulzInvert (iters, stopTol), X applied to the probes
+#   kind "hh":     C = A A of the sparse-built operator, applied to the probes
+BIG_CASES = {
+    # 128^2 five-point grid, 64-point leaves, maxRank 16, 64 right-hand sides
+    "cfg2": dict(sizes=(128, 128), levels=5, rank=16, oversample=4, kind="matmat", nrhs=64,
+                 keep=2, coef="uniform", seed=202),
+    # 32^2 five-point grid, 16-point leaves, maxRank 8: Schulz down to 1e-8
+    "cfg1s": dict(sizes=(32, 32), levels=4, rank=8, oversample=4, kind="schulz", nrhs=4,
+                  keep=4, coef="uniform", seed=101, iters=-1, stopTol=1e-8),
+    # 32^3 seven-point grid, 64-point leaves, maxRank 24, oversample 8: A A
+    "cfg3": dict(sizes=(32, 32, 32), levels=4, rank=24, oversample=8, kind="hh", nrhs=4,
+                 keep=1, coef="uniform", seed=303),
+    # 256^2 five-point grid, log-uniform c, 64-point leaves, maxRank 32:
+    # two fixed Schulz iterations
+    "cfg4": dict(sizes=(256, 256), levels=6, rank=32, oversample=4, kind="schulz", nrhs=4,
+                 keep=1, coef="log_uniform", seed=404, iters=2, stopTol=1e-4),
+}
+def make_big_case(name, spec, tmp):
+    sizes = spec["sizes"]
+    dim = len(sizes)
+    N = int(np.prod(sizes))
+    k = spec["nrhs"]
+    coef, X, G = big_case_inputs(spec)
+    cpath, xpath = os.path.join(tmp, "bc.bin"), os.path.join(tmp, "bx.bin")
+    coef.tofile(cpath)
+    np.asfortranarray(X).T.copy().tofile(xpath)
+    base = ["--dim", dim, "--nx", sizes[0], "--ny", sizes[1],
+            "--nz", sizes[2] if dim == 3 else 1, "--levels", spec["levels"],
+            "--rank", spec["rank"], "--oversample", spec["oversample"], "--strong", 1,
+            "--coef", cpath, "--x", xpath, "--nrhs", k]
+    o = os.path.join(tmp, "b")
+    out = dict(sizes=np.array(sizes), levels=spec["levels"], rank=spec["rank"],
+               oversample=spec["oversample"], nrhs=k, seed=spec["seed"], coef_kind=spec["coef"])
+
+    def reduce(tag, y):
+        Y = y.reshape(k, N).T
+        out[tag] = Y[:, :spec["keep"]].copy()
+        out[tag + "_sketch"] = G.T @ Y
+
+    if spec["kind"] == "matmat":
+        info, y = run(["matvec"] + base + ["--random", 1], o)
+        reduce("Y", y)
+        out["seconds"] = info["seconds"]
+        info, y = run(["transpose"] + base + ["--random", 1], o)
+        reduce("YT", y)
+    elif spec["kind"] == "schulz":
+        info, y = run(["schulz_trace"] + base + ["--iters", spec["iters"],
+                                                 "--stopTol", spec["stopTol"]], o)
+        reduce("XP", y)
+        out["trace"] = np.fromfile(o + ".trace.bin")
+        out["iterations"] = info["iterations"]
+        out["seconds"] = info["seconds"]
+        out["iters"] = spec["iters"]
+        out["stopTol"] = spec["stopTol"]
+    elif spec["kind"] == "hh":
+        info, y = run(["hh"] + base, o)
+        reduce("CP", y)
+        out["seconds"] = info["seconds"]
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name, "ok", f"{out['seconds']:.1f} s", sorted(out), flush=True)
+
+
 def main(argv):
     subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-j8"], check=True,
                    capture_output=True)
@@ -286,6 +360,8 @@ def main(argv):
                 make_complex_case(n, COMPLEX_CASES[n], tmp)
             elif n in DIST_CASES:
                 make_dist_case(n, DIST_CASES[n], tmp)
+            elif n in BIG_CASES:
+                make_big_case(n, BIG_CASES[n], tmp)
             else:
                 make_case(n, CASES[n], tmp)
 

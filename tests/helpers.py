@@ -36,3 +36,36 @@ def stencil_exact(fx):
     B = ops.dense_from_sparse(ops.stencil(sizes, fx["coefB"], L))
     P = fx["probes"]
     return dict(AA=A @ (A @ P), AB=-0.5 * (A @ (B @ P)), inv=np.linalg.solve(A, P))
+
+
+SKETCH = 8
+
+
+def hashed_uniform(n, k, seed):
+    """n x k matrix (column-major element order i + j n) of uniforms in
+    [-1, 1) from the splitmix64 hash of (seed, element index); exact on every
+    machine and numpy version."""
+    with np.errstate(over="ignore"):
+        z = (np.arange(n * k, dtype=np.uint64)
+             + np.uint64(seed) * np.uint64(0xD1B54A32D192ED03)
+             + np.uint64(0x9E3779B97F4A7C15))
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    u = (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+    return (2.0 * u - 1.0).reshape(k, n).T.copy()
+
+
+def big_case_inputs(spec):
+    """Coefficient field (natural order), right-hand sides and sketch matrix
+    of a benchmark-size case (a make_golden.BIG_CASES entry, or the fixture
+    it wrote: keys sizes, seed, nrhs and coef / coef_kind = "uniform" for c in
+    [1, 2) or "log_uniform" for c in [1, 100))."""
+    N = int(np.prod(spec["sizes"]))
+    s = int(spec["seed"])
+    kind = str(spec["coef_kind"] if "coef_kind" in spec else spec["coef"])
+    u = 0.5 * (hashed_uniform(N, 1, s)[:, 0] + 1.0)               # [0, 1)
+    coef = 1.0 + u if kind == "uniform" else 100.0 ** u
+    X = hashed_uniform(N, int(spec["nrhs"]), s + 1)
+    G = hashed_uniform(N, SKETCH, s + 2)
+    return coef, X, G

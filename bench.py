@@ -409,14 +409,25 @@ def gpu_arm(args):
             "wall_ms_per_step": wall * 1e3 / args.steps,
             "kernels": {k: {"ms_per_launch": v["ms"] / v["launches"], "launches": v["launches"]}
                         for k, v in prof.items()}}
-    line["matvec"] = matvec_leg(ctx, H, stream, census, hbm_peak, peak_kind, args)
-    line["tf32"] = tf32_leg(ctx, H, stream, X, Y, NRHS, nbytes, args)
+    legs = set(LEGS if args.legs == "all" else [x for x in args.legs.split(",") if x])
+    if "matvec" in legs:
+        line["matvec"] = matvec_leg(ctx, H, stream, census, hbm_peak, peak_kind, args)
+    if "tf32" in legs:
+        line["tf32"] = tf32_leg(ctx, H, stream, X, Y, NRHS, nbytes, args)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(coef, Xh, nbytes)
-    if not args.no_schulz:
+    legs = set(LEGS if args.legs == "all" else [x for x in args.legs.split(",") if x])
+    if args.no_schulz:
+        legs -= {"schulz", "schulz_modes", "schulz256"}
+    if "schulz" in legs:
         line["schulz"] = schulz_leg(local, rank == 0 and not args.no_cpu_baseline)
+    if "schulz_modes" in legs:
         line["schulz_modes"] = schulz_modes_leg(local)
-    if args.helmholtz_count > 0:
+    if "hh3d" in legs:
+        line["hh3d"] = hh3d_leg(local)
+    if "schulz256" in legs:
+        line["schulz256"] = schulz256_leg(local, rank == 0 and not args.no_cpu_baseline)
+    if args.helmholtz_count > 0 and "helmholtz" in legs:
         line["helmholtz_batch"] = helmholtz_batch_leg(local, args.helmholtz_count,
                                                       args.helmholtz_max_side or None)
     if rank == 0:
@@ -702,6 +713,192 @@ def schulz_modes_leg(device):
     return out
 
 
+# legs run after the headline product (all of them by default)
+LEGS = ("matvec", "tf32", "schulz", "schulz_modes", "hh3d", "schulz256", "helmholtz")
+
+HH3D = dict(sizes=(32, 32, 32), levels=4, rank=24, oversample=8, tol=1e-10, seed=3,
+            train=(((16, 16, 16), 3, (31, 32, 33)), ((32, 32, 32), 4, (34,))),
+            margin=2, probes=4)
+
+
+def hh3d_leg(device):
+    """The 3-D H*H product A A: HMat3d<double> from the seven-point operator
+    on a 32 x 32 x 32 grid (N = 32768, c ~ U[1, 2)), numLevels 4 (64-point
+    leaves), maxRank 24, oversample 8, compression tolerance 1e-10 (the
+    single-rank DistHMat truncation), side by side:
+      plain    every randomized compression draws maxRank + 8 samples;
+      learned  the rank predictor sets each compression's sample count
+               (predicted rank + 2 + 8), every block so sized checked by 4
+               Gaussian probes and redone with the plain count when its
+               estimated error exceeds the tolerance.
+    The predictor is trained on the GPU on the kept ranks that the plain
+    method logs for A A on other coefficient fields (16^3 with numLevels 3,
+    and 32^3).  Each mode times its second product (the first builds the
+    symbolic plan) with the device synchronized on both sides; accuracy is
+    the relative difference of C P from the plain product and from the exact
+    A (A P) on 4 probe vectors."""
+    import dmhm_b200 as D
+    cfg = HH3D
+    sz, L, r = cfg["sizes"], cfg["levels"], cfg["rank"]
+
+    def make(sizes, levels, seed, log=False):
+        coef = D.operators.uniform_coefficients(sizes, seed)
+        S = D.operators.stencil(sizes, coef, levels)
+        ctx = D.Context(device)
+        ctx.set_oversample(cfg["oversample"])
+        ctx.set_compression_tolerance(cfg["tol"])
+        if log:
+            ctx.rank_log_enable(True)
+        return ctx, S
+
+    t0 = time.perf_counter()
+    xs, ts = [], []
+    for tsz, tl, seeds in cfg["train"]:
+        for sd in seeds:
+            ctx, S = make(tsz, tl, sd, log=True)
+            A = D.HMat3d(S, tl, r, True, *tsz, ctx=ctx)
+            A.Multiply(1.0, A)
+            ctx.synchronize()
+            x, t = ctx.rank_log(clear=True)
+            xs.append(x)
+            ts.append(t)
+            del A, ctx
+    x, t = np.concatenate(xs), np.concatenate(ts)
+    ctx, _ = make(sz, L, cfg["seed"])
+    model = D.RankModel(ctx, seed=7)
+    loss0, _ = model.loss_grad(x, t)
+    loss = model.train(x, t, epochs=800, lr=1e-2)
+    params = model.params()
+    del model, ctx
+    out = {"workload": "HMat3d<double> 32x32x32 seven-point operator (N=32768), numLevels 4 "
+                       "(64-point leaves), maxRank 24, oversample 8, tolerance 1e-10: C = A A",
+           "training": {"rows": int(x.shape[0]), "loss_initial": loss0, "loss_final": loss,
+                        "epochs": 800, "seconds": time.perf_counter() - t0,
+                        "kept_rank_fraction_mean": float(t.mean()) if len(t) else None}}
+    P = np.random.default_rng(9).standard_normal((int(np.prod(sz)), 4))
+    ref = None
+    exact = None
+    for mode in ("plain", "learned"):
+        ctx, S = make(sz, L, cfg["seed"])
+        if mode == "learned":
+            m = D.RankModel(ctx, seed=7)
+            m.set_params(params)
+            ctx.use_rank_model(m, cfg["margin"], cfg["probes"])
+        A = D.HMat3d(S, L, r, True, *sz, ctx=ctx)
+        Cw = A.Multiply(1.0, A)               # plan, lists, memory pool
+        ctx.synchronize()
+        del Cw
+        stats0 = ctx.rank_stats()
+        t1 = time.perf_counter()
+        Cm = A.Multiply(1.0, A)
+        ctx.synchronize()
+        secs = time.perf_counter() - t1
+        stats1 = ctx.rank_stats()
+        cp = Cm.Multiply(1.0, P)
+        if exact is None:
+            exact = A.Multiply(1.0, A.Multiply(1.0, P))
+        if ref is None:
+            ref = cp
+        out[mode] = {"seconds": secs,
+                     "rel_diff_vs_plain": float(np.linalg.norm(cp - ref) / np.linalg.norm(ref)),
+                     "rel_err_vs_exact": float(np.linalg.norm(cp - exact) /
+                                               np.linalg.norm(exact)),
+                     "rank_sum": Cm.BlockCensus()["rank_sum"],
+                     "sampling": {k: stats1[k] - stats0[k] for k in stats1}}
+        del Cm, A, ctx
+    out["learned_speedup_vs_plain"] = out["plain"]["seconds"] / out["learned"]["seconds"]
+    return out
+
+
+SCHULZ256 = dict(sizes=(256, 256), levels=6, rank=32, oversample=4, seed=4, stop_tol=1e-8,
+                 tol=1e-10, mixed_switch=0.1,
+                 train=(((64, 64), 4, 6), ((128, 128), 5, 3)), margin=2, probes=4)
+
+
+def schulz256_leg(device, with_reference):
+    """SchulzInvert on the 256 x 256 five-point operator with c log-uniform
+    in [1, 100) (N = 65536, numLevels 6: 64-point leaves, maxRank 32,
+    oversample 4) down to ||I - X A|| < 1e-8:
+      plain_fp64           the reference's method (fixed rank, FP64);
+      mixed_learned_1e-10  the early iterations in the low-precision phase
+                           (TF32 range samples, FP32 roundings) while the
+                           last estimate is above 0.1, compression tolerance
+                           1e-10, learned sample counts (predictor trained on
+                           kept ranks logged by short runs at 64^2 and 128^2
+                           on another log-uniform field), probe check and
+                           plain fallback.
+    Wall seconds of each call, iterations, final estimate, residual
+    ||X A p - p|| / ||p|| and the relative difference of X p from the plain
+    inverse on 4 probes."""
+    import dmhm_b200 as D
+    cfg = SCHULZ256
+    sz, L, r = cfg["sizes"], cfg["levels"], cfg["rank"]
+
+    def make(sizes, levels, seed, tol, log=False):
+        coef = D.operators.log_uniform_coefficients(sizes, seed)
+        S = D.operators.stencil(sizes, coef, levels)
+        ctx = D.Context(device)
+        ctx.set_oversample(cfg["oversample"])
+        ctx.set_compression_tolerance(tol)
+        if log:
+            ctx.rank_log_enable(True)
+        return ctx, S
+
+    t0 = time.perf_counter()
+    xs, ts = [], []
+    for tsz, tl, tits in cfg["train"]:
+        ctx, S = make(tsz, tl, cfg["seed"] + 100, cfg["tol"], log=True)
+        H = D.HMat2d(S, tl, r, True, *tsz, ctx=ctx)
+        H.SchulzInvert(tits, 1.5, 6.0, 1e-30)
+        x, t = ctx.rank_log(clear=True)
+        xs.append(x)
+        ts.append(t)
+        del H, ctx
+    x, t = np.concatenate(xs), np.concatenate(ts)
+    ctx, _ = make(sz, L, cfg["seed"], cfg["tol"])
+    model = D.RankModel(ctx, seed=7)
+    loss0, _ = model.loss_grad(x, t)
+    loss = model.train(x, t, epochs=800, lr=1e-2)
+    params = model.params()
+    del model, ctx
+    out = {"workload": "SchulzInvert(-1, theta 1.5, confidence 6, stopTol 1e-8), HMat2d<double> "
+                       "256x256 five-point operator, c log-uniform in [1, 100), numLevels 6 "
+                       "(64-point leaves), maxRank 32, oversample 4",
+           "training": {"rows": int(x.shape[0]), "loss_initial": loss0, "loss_final": loss,
+                        "epochs": 800, "seconds": time.perf_counter() - t0}}
+    P = np.random.default_rng(6).standard_normal((sz[0] * sz[1], 4))
+    ref = None
+    for mode, tol, learned, switch in (("plain_fp64", 0.0, False, 0.0),
+                                       ("mixed_learned_1e-10", cfg["tol"], True,
+                                        cfg["mixed_switch"])):
+        ctx, S = make(sz, L, cfg["seed"], tol)
+        if learned:
+            m = D.RankModel(ctx, seed=7)
+            m.set_params(params)
+            ctx.use_rank_model(m, cfg["margin"], cfg["probes"])
+        H = D.HMat2d(S, L, r, True, *sz, ctx=ctx)
+        ctx.synchronize()
+        t1 = time.perf_counter()
+        its, low, trace = H.SchulzInvertMixed(-1, 1.5, 6.0, cfg["stop_tol"], switch)
+        ctx.synchronize()
+        secs = time.perf_counter() - t1
+        A = D.HMat2d(S, L, r, True, *sz, ctx=ctx)
+        xp = H.Multiply(1.0, P)
+        res = np.linalg.norm(H.Multiply(1.0, A.Multiply(1.0, P)) - P) / np.linalg.norm(P)
+        if ref is None:
+            ref = xp
+        out[mode] = {"seconds": secs, "iterations": its, "low_precision_iterations": low,
+                     "final_norm_estimate": trace[-1],
+                     "relative_residual_XAp_minus_p": float(res),
+                     "rel_diff_vs_plain_fp64": float(np.linalg.norm(xp - ref) /
+                                                     np.linalg.norm(ref)),
+                     "rank_sum": H.BlockCensus()["rank_sum"], "sampling": ctx.rank_stats()}
+        del H, A, ctx
+    out["speedup_vs_plain_fp64"] = (out["plain_fp64"]["seconds"] /
+                                    out["mixed_learned_1e-10"]["seconds"])
+    return out
+
+
 HELMHOLTZ = dict(count=48, sides=(32, 48, 64, 96, 128), k_range=(2.0, 10.0), rank=24,
                  oversample=4, rhs=8, stop_tol=1e-8, mixed_switch=0.1, seed=21, leaf_target=32,
                  streams=8, dense_check_max_n=2304)
@@ -814,6 +1011,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-schulz", action="store_true")
+    ap.add_argument("--legs", default="all",
+                    help="comma-separated legs after the headline product: " + ",".join(LEGS))
     # complex Helmholtz batch: a bounded sample by default (the full 48
     # instances take tens of minutes: --helmholtz-count 48 --helmholtz-max-side 0)
     ap.add_argument("--helmholtz-count", type=int, default=8)

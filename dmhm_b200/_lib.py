@@ -72,12 +72,14 @@ SIGNATURES = {
     "hm_multiply_dense_complex_host": [_P, _I, _D, _D, _PD, _I, _D, _D, _PD, _I, _I],
     "hm_destroy": [_P],
     "hm_info": [_P, _PI, _PI, _PI, _PI, _PI64, _PI64],
+    "hm_structure": [_P, _PI, _PI, _PI, _PI],
     "hm_set_to_random": [_P],
     "hm_multiply_dense": [_P, _I, _D, _P, _I, _D, _P, _I, _I],
     "hm_multiply_dense_host": [_P, _I, _D, _PD, _I, _D, _PD, _I, _I],
     "hm_multiply_hmat": [_P, _D, _P, C.POINTER(_P)],
     "hm_multiply_hmat_update": [_P, _D, _P, _D, _P],
     "hm_estimate_two_norm": [_P, _D, _D, _PD],
+    "hm_direct_invert": [_P],
     "hm_schulz_invert": [_P, _I, _D, _D, _D, _PI, _PD, _I, _PI],
     "hm_schulz_invert_mixed": [_P, _I, _D, _D, _D, _D, _PI, _PI, _PD, _I, _PI],
     "hm_set_low_precision": [_P, _I],
@@ -103,6 +105,8 @@ SIGNATURES = {
     "hm_rank_log_read": [_P, _PF, _PF, _I, _PI, _I],
     "hm_rank_stats": [_P, _PI64, _PI64, _PI64, _PI64],
     "hm_kernel_launches": [],
+    "hm_measure_fp64_peak": [_I, _I, _I, _PD, _PD],
+    "hm_check_bounded_wait": [_I, C.c_longlong, _PI],
     "hm_profile_enable": [_P, _I],
     "hm_profile_read": [_P, _I, C.c_char_p, _I, _PD, _PI64],
 }

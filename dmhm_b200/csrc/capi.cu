@@ -261,6 +261,7 @@ int hm_context_destroy(hm_context ctx) {
         }
         ctx->c.counters.reset();
         ctx->c.errword.reset();
+        ctx->c.numword.reset();
         cudaStreamSynchronize(ctx->c.stream);
         hmb::release_staging(ctx->c.stream);
         if (ctx->c.own_stream) cudaStreamDestroy(ctx->c.stream);
@@ -272,6 +273,7 @@ int hm_context_synchronize(hm_context ctx) {
     return guarded([&] {
         HMB_REQUIRE(ctx, HM_ERR_ARGUMENT, "ctx is NULL");
         HMB_CUDA(cudaStreamSynchronize(ctx->c.stream));
+        ctx->c.check_numerical();
     });
 }
 
@@ -535,6 +537,21 @@ int hm_destroy(hm_matrix h) {
     return guarded([&] {
         if (!h) return;
         delete_handle(h);
+    });
+}
+
+int hm_structure(hm_matrix h, int* dim, int* sizes, int* strongly_admissible,
+                 int* unknowns_per_point) {
+    return guarded([&] {
+        HMB_REQUIRE(h, HM_ERR_ARGUMENT, "h is NULL");
+        owner_of(h);
+        HMB_REQUIRE(h->h.S != nullptr, HM_ERR_ARGUMENT, "empty H-matrix");
+        const Structure& S = *h->h.S;
+        if (dim) *dim = S.dim;
+        if (sizes)
+            for (int d = 0; d < S.dim; ++d) sizes[d] = S.sizes[d];
+        if (strongly_admissible) *strongly_admissible = S.strong ? 1 : 0;
+        if (unknowns_per_point) *unknowns_per_point = S.dof;
     });
 }
 
@@ -811,6 +828,24 @@ int hm_multiply_vector_noalloc(hm_matrix h, int transpose, double alpha, const d
         owner_of(h);
         HMB_REQUIRE(h->h.S != nullptr, HM_ERR_ARGUMENT, "empty H-matrix");
         multiply_vector_noalloc(h->h, transpose != 0, alpha, x, beta, y);
+    });
+}
+
+int hm_direct_invert(hm_matrix h) {
+    return guarded([&] {
+        HMB_REQUIRE(h, HM_ERR_ARGUMENT, "h is NULL");
+        hm_context ctx = owner_of(h);
+        HMB_REQUIRE(h->h.S != nullptr, HM_ERR_ARGUMENT, "empty H-matrix");
+        hmat_direct_invert(ctx->c, h->h);
+    });
+}
+
+int hm_check_bounded_wait(int device, long long polls, int* timed_out) {
+    return guarded([&] {
+        HMB_REQUIRE(timed_out, HM_ERR_ARGUMENT, "timed_out is NULL");
+        HMB_REQUIRE(polls > 0 && polls <= (1LL << 26), HM_ERR_ARGUMENT,
+                    "polls must be in 1..2^26");
+        *timed_out = bounded_wait_times_out(device, polls) ? 1 : 0;
     });
 }
 

@@ -94,6 +94,13 @@ struct Context {
     // Device word set by kernels whose bounded waits gave up (zero = fine).
     int* error_word();
     DeviceBuffer<int> errword;
+    // Device word set by a low-rank rounding whose core held NaN or Inf
+    // (zero = fine); read and cleared by check_numerical().
+    int* numerical_word();
+    DeviceBuffer<int> numword;
+    // Synchronizes the stream and throws HM_ERR_NUMERICAL (clearing the
+    // word) when a rounding since the last check met a non-finite value.
+    void check_numerical();
 };
 
 // Host-side wall time of a phase, recorded under `name` when profiling.
@@ -211,6 +218,10 @@ int tf32_kernel_choice(Context& ctx, HMatrix& H, const double* B, int ldb, int n
 // FP32 copy of the block data rounded to TF32 (data32), made on first use
 // and kept until the data change.
 void ensure_tf32_copy(Context& ctx, HMatrix& H);
+// Runs the tensor-core kernels' bounded mbarrier wait on a barrier nothing
+// arrives at, with `limit` polls; true when the wait gave up as it must.
+bool bounded_wait_times_out(int device, long long limit);
+
 void multiply_dense_tf32(HMatrix& H, double alpha, const double* B, int ldb, double beta,
                          double* C, int ldc, int nrhs);
 

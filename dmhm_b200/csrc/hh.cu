@@ -491,11 +491,13 @@ struct SymKey {
     int fresh = 1, maxRankC = 0, oversample = 0, maxA = 0, maxB = 0;
     double alpha = 0, beta = 0;
     std::vector<int> ra, rb, rc;
+    std::vector<int> roots;   // flattened (a, b, c) sub-tree roots; empty: the whole matrix
     uint64_t hash = 0;
     bool operator==(const SymKey& o) const {
         return hash == o.hash && S == o.S && fresh == o.fresh && maxRankC == o.maxRankC &&
                oversample == o.oversample && maxA == o.maxA && maxB == o.maxB &&
-               alpha == o.alpha && beta == o.beta && ra == o.ra && rb == o.rb && rc == o.rc;
+               alpha == o.alpha && beta == o.beta && ra == o.ra && rb == o.rb && rc == o.rc &&
+               roots == o.roots;
     }
 };
 
@@ -515,15 +517,28 @@ struct HHPlanCache {
 
 namespace {
 
+// roots empty: the product of the whole matrices (C rebuilt when fresh).
+// Otherwise one product per listed sub-tree triple, in order (fresh: C_c :=
+// alpha A_a B_b; else C_c := alpha A_a B_b + beta C_c), into an existing C
+// whose other leaves keep their content.
 std::shared_ptr<SymPlan> make_plan(const HMatrix& A, const HMatrix& B, const HMatrix& C,
                                    double alpha, double beta, bool fresh, int maxRankC,
-                                   int oversample) {
+                                   int oversample, const std::vector<HHRoot>& roots) {
     const Structure& S = *A.S;
     Planner P(A, B, maxRankC, oversample, 0);
-    if (fresh)
-        P.fresh(0, 0, 0, alpha);
-    else
-        P.update(0, 0, 0, alpha, beta);
+    const bool exec_fresh = fresh && roots.empty();
+    if (roots.empty()) {
+        if (fresh)
+            P.fresh(0, 0, 0, alpha);
+        else
+            P.update(0, 0, 0, alpha, beta);
+    }
+    for (const HHRoot& r : roots) {
+        if (fresh)
+            P.fresh(r.a, r.b, r.c, alpha);
+        else
+            P.update(r.a, r.b, r.c, alpha, beta);
+    }
     P.lops.finalize(S.blocks.size());
     P.dops.finalize(S.blocks.size());
     auto plan = std::make_shared<SymPlan>();
@@ -539,7 +554,7 @@ std::shared_ptr<SymPlan> make_plan(const HMatrix& A, const HMatrix& B, const HMa
     for (int c : S.leaves) {
         const Block& Cb = S.blocks[c];
         if (Cb.kind != KIND_LOWRANK) continue;
-        int rank = fresh ? 0 : C.rank[c];
+        int rank = exec_fresh ? 0 : C.rank[c];
         const int minDim = std::min(Cb.m, Cb.n);
         const int nops = P.lops.size(c);
         const LOp* ops = P.lops.of(c);
@@ -586,7 +601,7 @@ std::shared_ptr<SymPlan> make_plan(const HMatrix& A, const HMatrix& B, const HMa
 
 std::shared_ptr<SymPlan> get_plan(Context& ctx, const HMatrix& A, const HMatrix& B,
                                   const HMatrix& C, double alpha, double beta, bool fresh,
-                                  int maxRankC) {
+                                  int maxRankC, const std::vector<HHRoot>& roots) {
     SymKey key;
     key.S = A.S.get();
     key.fresh = fresh ? 1 : 0;
@@ -598,7 +613,12 @@ std::shared_ptr<SymPlan> get_plan(Context& ctx, const HMatrix& A, const HMatrix&
     key.beta = beta;
     key.ra = A.rank;
     key.rb = B.rank;
-    if (!fresh) key.rc = C.rank;
+    if (!fresh || !roots.empty()) key.rc = C.rank;
+    for (const HHRoot& r : roots) {
+        key.roots.push_back(r.a);
+        key.roots.push_back(r.b);
+        key.roots.push_back(r.c);
+    }
     uint64_t h = 1469598103934665603ULL;
     h = fnv(h, &key.S, sizeof(key.S));
     h = fnv(h, &key.fresh, sizeof(int) * 5);
@@ -606,6 +626,7 @@ std::shared_ptr<SymPlan> get_plan(Context& ctx, const HMatrix& A, const HMatrix&
     h = fnv(h, key.ra.data(), key.ra.size() * sizeof(int));
     h = fnv(h, key.rb.data(), key.rb.size() * sizeof(int));
     h = fnv(h, key.rc.data(), key.rc.size() * sizeof(int));
+    h = fnv(h, key.roots.data(), key.roots.size() * sizeof(int));
     key.hash = h;
     if (!ctx.hh_cache) ctx.hh_cache = std::make_shared<HHPlanCache>();
     auto& E = ctx.hh_cache->entries;
@@ -619,7 +640,7 @@ std::shared_ptr<SymPlan> get_plan(Context& ctx, const HMatrix& A, const HMatrix&
     }
     // complex matrices (real form, 2 rows per point): oversample complex
     // directions = 2 x oversample real ones
-    auto plan = make_plan(A, B, C, alpha, beta, fresh, maxRankC, ctx.oversample * A.S->dof);
+    auto plan = make_plan(A, B, C, alpha, beta, fresh, maxRankC, ctx.oversample * A.S->dof, roots);
     E.emplace_back(std::move(key), plan);
     if (E.size() > kHHPlans) E.erase(E.begin());
     return plan;
@@ -629,12 +650,40 @@ std::shared_ptr<SymPlan> get_plan(Context& ctx, const HMatrix& A, const HMatrix&
 
 void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha, double beta,
                  HMatrix& C, bool fresh, bool compact) {
+    hh_multiply_roots(ctx, A, B, alpha, beta, C, fresh, {}, compact);
+}
+
+void hh_multiply_sub(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha, double beta,
+                     HMatrix& C, bool fresh, const std::vector<HHRoot>& roots) {
+    HMB_REQUIRE(!roots.empty(), HM_ERR_ARGUMENT, "no sub-tree product listed");
+    HMB_REQUIRE(C.S != nullptr, HM_ERR_ARGUMENT, "sub-tree products need an existing C");
+    const Structure& S = *C.S;
+    for (const HHRoot& r : roots) {
+        HMB_REQUIRE(r.a >= 0 && r.b >= 0 && r.c >= 0 && r.a < (int)S.blocks.size() &&
+                        r.b < (int)S.blocks.size() && r.c < (int)S.blocks.size(),
+                    HM_ERR_ARGUMENT, "sub-tree root out of range");
+        const Block& Ba = S.blocks[r.a];
+        const Block& Bb = S.blocks[r.b];
+        const Block& Bc = S.blocks[r.c];
+        HMB_REQUIRE(Ba.m == Bc.m && Bb.n == Bc.n && Ba.n == Bb.m && Ba.row_off == Bc.row_off &&
+                        Bb.col_off == Bc.col_off && Ba.col_off == Bb.row_off,
+                    HM_ERR_ARGUMENT, "sub-tree product roots are not conformal");
+    }
+    hh_multiply_roots(ctx, A, B, alpha, beta, C, fresh, roots, false);
+}
+
+void hh_multiply_roots(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
+                       double beta, HMatrix& C, bool fresh_plan,
+                       const std::vector<HHRoot>& roots, bool compact) {
     HMB_REQUIRE(A.S && B.S && (A.S == B.S || same_structure(*A.S, *B.S)), HM_ERR_ARGUMENT,
                 "H*H multiply needs both factors on the same block structure");
     HMB_REQUIRE(&C != &A && &C != &B, HM_ERR_ARGUMENT,
                 "the product must not overwrite a factor");
     const Structure& S = *A.S;
     cudaStream_t st = ctx.stream;
+    // sub-tree products update C in place (every other leaf is kept), so
+    // they execute like the update form whatever their planner form
+    const bool fresh = fresh_plan && roots.empty();
     if (!fresh) {
         HMB_REQUIRE(C.S && (C.S == A.S || same_structure(*C.S, *A.S)), HM_ERR_ARGUMENT,
                     "C must share the factors' block structure");
@@ -643,7 +692,8 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
 
     // ---------------- symbolic phase ----------------
     std::unique_ptr<HostScope> hs(new HostScope(ctx, "hh_symbolic"));
-    const std::shared_ptr<SymPlan> plan = get_plan(ctx, A, B, C, alpha, beta, fresh, maxRankC);
+    const std::shared_ptr<SymPlan> plan =
+        get_plan(ctx, A, B, C, alpha, beta, fresh_plan, maxRankC, roots);
     hs.reset(new HostScope(ctx, "hh_plan_copy"));
     // The plan's task list is used in place: every per-product field
     // (generator positions, arena offsets, pointers, sample counts) is
@@ -1057,7 +1107,30 @@ void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha,
                 const int nops = P.lops.size(c);
                 const LOp* ops = P.lops.of(c);
                 const int obase = P.lops.begin[c];
-                if (nops == 0) continue;
+                if (nops == 0) {
+                    // outside every sub-tree of a sub-tree product: keep the
+                    // block (an exact copy, the concatenation with nothing)
+                    if (!fresh && c_old_rank[c] > 0 && Cb.m > 0 && Cb.n > 0) {
+                        RoundOp r{};
+                        r.kind = ROUND_CONCAT;
+                        r.m = Cb.m;
+                        r.n = Cb.n;
+                        r.alpha = 1.0;
+                        r.beta = 1.0;
+                        r.r2 = c_old_rank[c];
+                        r.rout = c_old_rank[c];
+                        r.u2 = c_old_data.get() + c_old_off[c];
+                        r.v2 = r.u2 + (long long)Cb.m * c_old_rank[c];
+                        r.ldu2 = Cb.m;
+                        r.ldv2 = Cb.n;
+                        r.uo = C.U(c);
+                        r.vo = C.V(c);
+                        rops.push_back(r);
+                        rwork.push_back(0);
+                        rbegin.push_back((int)rops.size());
+                    }
+                    continue;
+                }
                 const double* cu = nullptr;
                 const double* cv = nullptr;
                 int cr = 0;

@@ -59,6 +59,15 @@ __device__ __forceinline__ float r_abs(float x) { return fabsf(x); }
 __device__ __forceinline__ double r_copysign(double a, double b) { return copysign(a, b); }
 __device__ __forceinline__ float r_copysign(float a, float b) { return copysignf(a, b); }
 
+// f(i, c) for every entry of an m x cols column-major array: column c by
+// warp c % kW, rows by lane (no integer division in the index arithmetic)
+template <typename F>
+__device__ __forceinline__ void for_each_entry(int m, int cols, F f) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int c = warp; c < cols; c += kW)
+        for (int i = lane; i < m; i += 32) f(i, c);
+}
+
 template <typename R>
 __device__ __forceinline__ R warp_sum(R v) {
 #pragma unroll
@@ -177,14 +186,18 @@ __device__ __forceinline__ int rr_pos(int i, int step, int n) {
 // the squared Frobenius norm of M) are left alone: rotating noise against
 // noise never settles, and such columns carry no singular value above
 // rounding level.
+//
+// A core holding NaN or Inf (non-finite block data) sets *numflag; the
+// sweeps still end within their bound.
 template <typename R>
-__device__ void cta_jacobi(R* M, int rows, int cols, R* J, int* flag, R* red, R* nrm) {
+__device__ void cta_jacobi(R* M, int rows, int cols, R* J, int* flag, R* red, R* nrm,
+                           int* numflag) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int e = threadIdx.x; e < cols * cols; e += kT)
-        J[e] = (e % cols == e / cols) ? R(1) : R(0);
+    for_each_entry(cols, cols, [&](int i, int c) { J[i + c * cols] = i == c ? R(1) : R(0); });
     R fro = 0;
     for (long long e = threadIdx.x; e < (long long)rows * cols; e += kT) fro = r_fma(M[e], M[e], fro);
     fro = block_sum(fro, red);
+    if (threadIdx.x == 0 && numflag && !isfinite((double)fro)) atomicOr(numflag, 1);
     const R tiny = R(Prec<R>::tiny) * fro;
     __syncthreads();
     if (cols < 2) return;
@@ -327,7 +340,8 @@ struct RoundShared {
 // One rounding operation, executed by the whole CTA.  `dyn` holds the core
 // and the rotations in shared memory when they fit in `smem_elems` elements.
 template <typename R>
-__device__ void do_round(const RoundOp& op_in, R* dyn, long long smem_elems, RoundShared<R>& sh) {
+__device__ void do_round(const RoundOp& op_in, R* dyn, long long smem_elems, RoundShared<R>& sh,
+                         int* numflag) {
     R* red = sh.red;
     R* norms = sh.norms;
     int* order = sh.order;
@@ -341,18 +355,17 @@ __device__ void do_round(const RoundOp& op_in, R* dyn, long long smem_elems, Rou
         // exact: [beta U2, alpha U1], [V2, V1] (SET: r2 = 0), zero beyond
         const int r2 = op.kind == ROUND_SET ? 0 : op.r2, r = op.r1 + r2;
         const int cap = max(r, op.rout);
-        for (long long e = tid; e < (long long)m * cap; e += kT) {
-            int i = (int)(e % m), c = (int)(e / m);
-            op.uo[e] = c >= r    ? 0.0
-                       : c < r2 ? op.beta * op.u2[i + (long long)c * op.ldu2]
-                                : op.alpha * op.u1[i + (long long)(c - r2) * op.ldu1];
-        }
-        for (long long e = tid; e < (long long)n * cap; e += kT) {
-            int i = (int)(e % n), c = (int)(e / n);
-            op.vo[e] = c >= r    ? 0.0
-                       : c < r2 ? op.v2[i + (long long)c * op.ldv2]
-                                : op.v1[i + (long long)(c - r2) * op.ldv1];
-        }
+        for_each_entry(m, cap, [&](int i, int c) {
+            op.uo[i + (long long)c * m] =
+                c >= r    ? 0.0
+                : c < r2 ? op.beta * op.u2[i + (long long)c * op.ldu2]
+                         : op.alpha * op.u1[i + (long long)(c - r2) * op.ldu1];
+        });
+        for_each_entry(n, cap, [&](int i, int c) {
+            op.vo[i + (long long)c * n] = c >= r    ? 0.0
+                                          : c < r2 ? op.v2[i + (long long)c * op.ldv2]
+                                                   : op.v1[i + (long long)(c - r2) * op.ldv1];
+        });
         if (tid == 0 && op.rank_out) *op.rank_out = r;
         return;
     }
@@ -394,31 +407,28 @@ __device__ void do_round(const RoundOp& op_in, R* dyn, long long smem_elems, Rou
         // orthonormal ones, so the leading part of the core is already
         // diagonal and the Jacobi sweeps mostly rotate the new columns in
         const int r2 = op.r2;
-        for (long long e = tid; e < (long long)m * k; e += kT) {
-            int i = (int)(e % m), c = (int)(e / m);
-            Ucat[e] = (R)(c < r2 ? op.beta * op.u2[i + (long long)c * op.ldu2]
-                                 : op.alpha * op.u1[i + (long long)(c - r2) * op.ldu1]);
-        }
-        for (long long e = tid; e < (long long)n * k; e += kT) {
-            int i = (int)(e % n), c = (int)(e / n);
-            Vcat[e] = (R)(c < r2 ? op.v2[i + (long long)c * op.ldv2]
-                                 : op.v1[i + (long long)(c - r2) * op.ldv1]);
-        }
+        for_each_entry(m, k, [&](int i, int c) {
+            Ucat[i + (long long)c * m] =
+                (R)(c < r2 ? op.beta * op.u2[i + (long long)c * op.ldu2]
+                           : op.alpha * op.u1[i + (long long)(c - r2) * op.ldu1]);
+        });
+        for_each_entry(n, k, [&](int i, int c) {
+            Vcat[i + (long long)c * n] = (R)(c < r2 ? op.v2[i + (long long)c * op.ldv2]
+                                                    : op.v1[i + (long long)(c - r2) * op.ldv1]);
+        });
     } else if (dense) {
-        for (long long e = tid; e < (long long)m * n; e += kT) {
-            int i = (int)(e % m), c = (int)(e / m);
+        for_each_entry(m, n, [&](int i, int c) {
             double v = op.alpha * op.u1[i + (long long)c * op.ldu1];
             if (op.beta != 0.0)
                 for (int l = 0; l < op.r2; ++l)
                     v = fma(op.beta * op.u2[i + (long long)l * op.ldu2],
                             op.v2[c + (long long)l * op.ldv2], v);
-            Ucat[e] = (R)v;
-        }
+            Ucat[i + (long long)c * m] = (R)v;
+        });
     } else {  // ortho: Q1 is used in place; Z is copied
-        for (long long e = tid; e < (long long)n * k; e += kT) {
-            int i = (int)(e % n), c = (int)(e / n);
-            Vcat[e] = (R)op.v1[i + (long long)c * op.ldv1];
-        }
+        for_each_entry(n, k, [&](int i, int c) {
+            Vcat[i + (long long)c * n] = (R)op.v1[i + (long long)c * op.ldv1];
+        });
     }
     __syncthreads();
 
@@ -427,8 +437,7 @@ __device__ void do_round(const RoundOp& op_in, R* dyn, long long smem_elems, Rou
     if (!dense) cta_qr(Vcat, n, k, n, tauV, red);
 
     // ---- core M = R_u R_v^T (ku x kv) -------------------------------------
-    for (int e = tid; e < ku * kv; e += kT) {
-        const int i = e % ku, l = e / ku;
+    for_each_entry(ku, kv, [&](int i, int l) {
         R v = 0;
         if (ortho) {
             v = (i >= l) ? Vcat[l + (long long)i * n] : R(0);     // R_v^T
@@ -439,11 +448,11 @@ __device__ void do_round(const RoundOp& op_in, R* dyn, long long smem_elems, Rou
                 v = r_fma(Ucat[i + (long long)p * m], Vcat[l + (long long)p * n], v);
         }
         M[i + (long long)l * ku] = v;
-    }
+    });
     __syncthreads();
 
     // ---- SVD of the core ---------------------------------------------------
-    cta_jacobi(M, ku, kv, J, &sh.flag, red, sh.nrm);
+    cta_jacobi(M, ku, kv, J, &sh.flag, red, sh.nrm, numflag);
     cta_order_columns(M, ku, kv, norms, order);
 
     // ---- outputs -------------------------------------------------------------
@@ -464,25 +473,24 @@ __device__ void do_round(const RoundOp& op_in, R* dyn, long long smem_elems, Rou
     }
     if (tid == 0 && op.rank_out) *op.rank_out = keep;
     if (ortho) {
-        for (long long e = tid; e < (long long)m * rout; e += kT) {
-            int i = (int)(e % m), c = (int)(e / m);
+        for_each_entry(m, rout, [&](int i, int c) {
             double v = 0.0;
             if (c < keep) {
                 const R* g = M + (long long)order[c] * ku;
                 for (int p = 0; p < ku; ++p) v = fma(op.u1[i + (long long)p * op.ldu1], (double)g[p], v);
             }
-            op.uo[e] = v;
-        }
+            op.uo[i + (long long)c * m] = v;
+        });
     } else {
-        for (long long e = tid; e < (long long)m * rout; e += kT) {
-            int i = (int)(e % m), c = (int)(e / m);
-            op.uo[e] = (i < ku && c < keep) ? (double)M[i + (long long)order[c] * ku] : 0.0;
-        }
+        for_each_entry(m, rout, [&](int i, int c) {
+            op.uo[i + (long long)c * m] =
+                (i < ku && c < keep) ? (double)M[i + (long long)order[c] * ku] : 0.0;
+        });
     }
-    for (long long e = tid; e < (long long)n * rout; e += kT) {
-        int i = (int)(e % n), c = (int)(e / n);
-        op.vo[e] = (i < kv && c < keep) ? (double)J[i + (long long)order[c] * kv] : 0.0;
-    }
+    for_each_entry(n, rout, [&](int i, int c) {
+        op.vo[i + (long long)c * n] =
+            (i < kv && c < keep) ? (double)J[i + (long long)order[c] * kv] : 0.0;
+    });
     __syncthreads();
     if (!ortho) cta_apply_q(Ucat, m, min(m, k), m, tauU, op.uo, rout, m);
     if (!dense) cta_apply_q(Vcat, n, min(n, k), n, tauV, op.vo, rout, n);
@@ -494,7 +502,7 @@ template <typename R>
 __global__ void __launch_bounds__(kT, 4)
 round_worker_kernel(const RoundOp* __restrict__ ops, const int* __restrict__ begin,
                     const int* __restrict__ workers, long long smem_elems,
-                    const RelocBases bases) {
+                    const RelocBases bases, int* numflag) {
     extern __shared__ __align__(16) unsigned char round_dyn[];
     R* dyn = reinterpret_cast<R*>(round_dyn);
     __shared__ RoundShared<R> sh;
@@ -512,7 +520,7 @@ round_worker_kernel(const RoundOp* __restrict__ ops, const int* __restrict__ beg
         op.rank_out = reloc(op.rank_out, bases);
         op.r1_dev = reloc(op.r1_dev, bases);
         op.r2_dev = reloc(op.r2_dev, bases);
-        do_round(op, dyn, smem_elems, sh);
+        do_round(op, dyn, smem_elems, sh, numflag);
         __syncthreads();
     }
 }
@@ -523,10 +531,7 @@ __global__ void __launch_bounds__(kT) qr_formq_kernel(const QrOp* __restrict__ o
     const int kq = min(op.m, op.k);
     if (op.m == 0 || kq == 0) return;
     cta_qr(op.Y, op.m, op.k, op.ldy, op.tau, red);
-    for (long long e = threadIdx.x; e < (long long)op.m * kq; e += kT) {
-        int i = (int)(e % op.m), c = (int)(e / op.m);
-        op.Q[e] = (i == c) ? 1.0 : 0.0;
-    }
+    for_each_entry(op.m, kq, [&](int i, int c) { op.Q[i + (long long)c * op.m] = (i == c) ? 1.0 : 0.0; });
     __syncthreads();
     cta_apply_q(op.Y, op.m, kq, op.ldy, op.tau, op.Q, kq, op.m);
 }
@@ -574,7 +579,7 @@ void launch_round_typed(Context& ctx, const RoundList& L, const RelocBases& base
     }
     LaunchScope ls(ctx, name);
     round_worker_kernel<R><<<(unsigned)L.nw, kT, smem * sizeof(R), ctx.stream>>>(
-        L.ops.get(), L.begin.get(), L.workers.get(), smem, bases);
+        L.ops.get(), L.begin.get(), L.workers.get(), smem, bases, ctx.numerical_word());
     HMB_CHECK_LAUNCH();
 }
 

@@ -1235,6 +1235,27 @@ int* Context::error_word() {
     return errword.get();
 }
 
+int* Context::numerical_word() {
+    if (!numword.get()) {
+        numword.allocate(1, stream);
+        HMB_CUDA(cudaMemsetAsync(numword.get(), 0, sizeof(int), stream));
+    }
+    return numword.get();
+}
+
+void Context::check_numerical() {
+    HMB_CUDA(cudaStreamSynchronize(stream));
+    if (!numword.get()) return;
+    int h = 0;
+    HMB_CUDA(cudaMemcpy(&h, numword.get(), sizeof(int), cudaMemcpyDeviceToHost));
+    if (h) {
+        HMB_CUDA(cudaMemset(numword.get(), 0, sizeof(int)));
+        throw Error(HM_ERR_NUMERICAL,
+                    "a low-rank rounding met NaN or Inf (non-finite block data entered an "
+                    "H*H product)");
+    }
+}
+
 double* Context::pinned_scalar() {
     if (!pinned) HMB_CUDA(cudaMallocHost((void**)&pinned, sizeof(double)));
     return pinned;

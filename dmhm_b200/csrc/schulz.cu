@@ -24,13 +24,6 @@ namespace {
 
 constexpr int kT = 256;
 
-struct CopyTask {
-    const double* src;
-    double* dst;
-    double alpha;
-    int m, n, lds, transpose;   // dst (m x n, ld m) = alpha * (transpose ? src^T : src)
-};
-
 __global__ void copy_tasks_kernel(const CopyTask* __restrict__ tasks) {
     const CopyTask t = tasks[blockIdx.x];
     const long long total = (long long)t.m * t.n;
@@ -39,18 +32,6 @@ __global__ void copy_tasks_kernel(const CopyTask* __restrict__ tasks) {
         double v = t.transpose ? t.src[j + (long long)i * t.lds] : t.src[i + (long long)j * t.lds];
         t.dst[e] = t.alpha * v;
     }
-}
-
-void launch_copy_tasks(Context& ctx, const std::vector<CopyTask>& tasks, const char* name) {
-    std::vector<CopyTask> live;
-    for (const CopyTask& t : tasks)
-        if (t.m > 0 && t.n > 0) live.push_back(t);
-    if (live.empty()) return;
-    DeviceBuffer<CopyTask> d;
-    d.upload(live, ctx.stream);
-    LaunchScope ls(ctx, name);
-    copy_tasks_kernel<<<(unsigned)live.size(), kT, 0, ctx.stream>>>(d.get());
-    HMB_CHECK_LAUNCH();
 }
 
 struct DiagTask {
@@ -123,6 +104,18 @@ __global__ void scale_vector_kernel(double* x, int n, const double* inv) {
 __global__ void set_scalar_kernel(double* p, double v) { *p = v; }
 
 }  // namespace
+
+void launch_copy_tasks(Context& ctx, const std::vector<CopyTask>& tasks, const char* name) {
+    std::vector<CopyTask> live;
+    for (const CopyTask& t : tasks)
+        if (t.m > 0 && t.n > 0) live.push_back(t);
+    if (live.empty()) return;
+    DeviceBuffer<CopyTask> d;
+    d.upload(live, ctx.stream);
+    LaunchScope ls(ctx, name);
+    copy_tasks_kernel<<<(unsigned)live.size(), kT, 0, ctx.stream>>>(d.get());
+    HMB_CHECK_LAUNCH();
+}
 
 // ---------------------------------------------------------------------------
 // Elementwise H-matrix operations
@@ -354,7 +347,10 @@ double estimate_two_norm(Context& ctx, HMatrix& A, double theta, double confiden
         throw;
     }
     cudaEventDestroy(ev);
-    return *slot;
+    const double est = *slot;
+    HMB_REQUIRE(std::isfinite(est), HM_ERR_NUMERICAL,
+                "EstimateTwoNorm met NaN or Inf (non-finite block data)");
+    return est;
 }
 
 // ---------------------------------------------------------------------------
@@ -419,6 +415,8 @@ SchulzResult schulz_invert(Context& ctx, HMatrix& A, int num_iterations, double 
             hh_multiply(ctx, Z, *X, 1.0, 0.0, *Xn, true, false);
             HMB_CUDA(cudaEventSynchronize(est_done));
             const double ez = *slot;
+            HMB_REQUIRE(std::isfinite(ez), HM_ERR_NUMERICAL,
+                        "SchulzInvert: the estimate of ||I - X A|| is NaN or Inf");
             res.trace.push_back(ez);
             last = std::fabs(ez);
             X = std::move(Xn);

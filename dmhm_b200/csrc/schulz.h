@@ -12,6 +12,16 @@ struct SchulzResult {
     std::vector<double> trace;   // [est ||A||, est ||I - X_k A|| per stop check]
 };
 
+// Block copies: dst (m x n, ld m) = alpha * (transpose ? src^T : src), src
+// with leading dimension lds; one CTA per task, all tasks in one launch.
+struct CopyTask {
+    const double* src;
+    double* dst;
+    double alpha;
+    int m, n, lds, transpose;
+};
+void launch_copy_tasks(Context& ctx, const std::vector<CopyTask>& tasks, const char* name);
+
 double estimate_two_norm(Context& ctx, HMatrix& A, double theta, double confidence);
 // Drops the trailing zero columns that tolerance truncation leaves in the
 // low-rank blocks when that saves at least 5 % of the low-rank storage

@@ -49,8 +49,9 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar) {
 }
 
 // Bounded wait for the given phase parity; false (and err set) on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
-    for (long long it = 0; it < kWaitLimit; ++it) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err,
+                                          long long limit = kWaitLimit) {
+    for (long long it = 0; it < limit; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -351,7 +352,44 @@ __global__ void input_tf32_kernel(const double* __restrict__ X, int ldx, float* 
     }
 }
 
+// Check of the bounded wait itself: one warp initialises an mbarrier that
+// expects one arrival, never arrives, and waits for it with a short limit.
+// The wait gives up, records the timeout in *err and the kernel returns.
+__global__ void bounded_wait_probe_kernel(long long limit, int* err) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    mbar_wait(&bar, 0, err, limit);
+}
+
 }  // namespace
+
+// Runs the bounded-wait check on `device` (its own stream and flag); returns
+// whether the wait ran out, as it must.
+bool bounded_wait_times_out(int device, long long limit) {
+    HMB_CUDA(cudaSetDevice(device));
+    cudaStream_t s;
+    HMB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    int* d_err = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&d_err, sizeof(int), s);
+    int h_err = 0;
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_err, 0, sizeof(int), s);
+    if (e == cudaSuccess) {
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+        bounded_wait_probe_kernel<<<1, 32, 0, s>>>(limit, d_err);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (d_err) cudaFreeAsync(d_err, s);
+    const cudaError_t e2 = cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    HMB_CUDA(e);
+    HMB_CUDA(e2);
+    return h_err != 0;
+}
 
 // FP32 (TF32-rounded) copy of the block data, made on first use.
 void ensure_tf32_copy(Context& ctx, HMatrix& H) {

@@ -516,6 +516,11 @@ class _HMatBase:
         else:
             check(lib().hm_add_constant_to_diagonal(self._h, float(alpha)))
 
+    def DirectInvert(self):
+        """A := inv(A) by recursive Schur complements
+        (src/HMat2d/Invert-incl.hpp:17-125, src/HMat3d/Invert-incl.hpp:14-122)."""
+        check(lib().hm_direct_invert(self._h))
+
     def SchulzInvert(self, numIterations: int, theta: float = 1.5, confidence: float = 6.0,
                      stopTol: float = 1e-4):
         """A :~= inv(A) by Schulz iteration (src/HMat2d/Invert-incl.hpp:127-196).

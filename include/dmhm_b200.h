@@ -56,6 +56,8 @@ HM_API int hm_version(void);
  */
 HM_API int hm_context_create(int device, void* cuda_stream, hm_context* out);
 HM_API int hm_context_destroy(hm_context ctx);
+/* Waits for the context's stream; HM_ERR_NUMERICAL when a low-rank rounding
+   since the last synchronization met NaN or Inf (non-finite block data). */
 HM_API int hm_context_synchronize(hm_context ctx);
 /* SetOversample / Oversample (src/core/global.cpp:155-159). */
 HM_API int hm_set_oversample(hm_context ctx, int oversample);
@@ -173,6 +175,13 @@ HM_API int hm_conjugate(hm_matrix src, hm_matrix* dst);
 HM_API int hm_transpose_complex(hm_matrix src, hm_matrix* dst);
 HM_API int hm_destroy(hm_matrix h);
 
+/* Grid of the block structure: dim (2 or 3), sizes[dim] (xSize, ySize[,
+   zSize]), strong (1) or weak (0) admissibility (StronglyAdmissible,
+   src/HMat2d/HMat2d.cpp:436), and unknowns per grid point (1, or 2 for the
+   real form of a complex matrix).  Any pointer may be NULL. */
+HM_API int hm_structure(hm_matrix h, int* dim, int* sizes, int* strongly_admissible,
+                        int* unknowns_per_point);
+
 /* Height, width, number of levels, max rank, and the block census:
    counts[0..2] = node / low-rank / dense blocks, counts[3] = sum of low-rank
    ranks, bytes = device bytes of the block data. */
@@ -235,6 +244,16 @@ HM_API int hm_multiply_hmat_update(hm_matrix A, double alpha, hm_matrix B, doubl
 /* hmat_tools::EstimateTwoNorm (include/dmhm/hmat_tools.hpp:1504-1548). */
 HM_API int hm_estimate_two_norm(hm_matrix h, double theta, double confidence,
                                 double* estimate);
+
+/* DirectInvert (src/HMat2d/Invert-incl.hpp:17-125; HMat3d:
+   src/HMat3d/Invert-incl.hpp:14-122): A := inv(A) by recursive block
+   elimination with Schur complements, in the reference's order of block
+   products (each truncated to maxRank, randomized compressions drawing from
+   the context's serial generator as the reference's do), dense diagonal
+   leaves inverted by partial-pivoting elimination (hmat_tools::Invert,
+   src/hmat_tools/Invert.cpp:14-42).  Real matrices whose dense leaves have
+   at most 96 rows; HM_ERR_NUMERICAL when a leaf is singular. */
+HM_API int hm_direct_invert(hm_matrix h);
 
 /*
  * SchulzInvert(numIterations, theta, confidence, stopTol)
@@ -355,6 +374,13 @@ HM_API int hm_profile_read(hm_context ctx, int index, char* name, int name_cap,
    form: 0 mma.sync m8n8k4 .f64, 1 m16n8k4 .f64, 2 m16n8k8 .f64,
    3 m16n8k16 .f64, 4 scalar fma.rn.f64.  *tflops receives 1e-12 flop/s;
    *ms (may be NULL) the launch time. */
+/* Check of the failure path (no reference counterpart): runs the bounded
+   mbarrier wait of the tensor-core kernels on a barrier that nothing arrives
+   at, giving up after `polls` polls (1..2^26).  *timed_out = 1 when the wait
+   gave up, recorded its timeout and returned, as it must; the GPU context
+   stays usable.  A real kernel whose wait gives up reports HM_ERR_TIMEOUT. */
+HM_API int hm_check_bounded_wait(int device, long long polls, int* timed_out);
+
 HM_API int hm_measure_fp64_peak(int device, int form, int iterations, double* tflops,
                                 double* ms);
 

@@ -2,9 +2,16 @@
 // drivers use dmhm::HMat2d (tests/HMat2d/MultiplyHMat.cpp, Invert.cpp):
 // build the stencil operator from a Sparse matrix in hierarchical order,
 // multiply vectors and dense blocks, form A*A, run SchulzInvert.
+// Written against the reference's namespace dmhm (an alias of dmhm_b200),
+// with an AbstractHMat reference for the norm estimate, views of dense
+// blocks, and HMat2d<std::complex<double>> on the shifted Helmholtz-like
+// operator.
 // Usage: facade_check <dir> <nx> <ny> <levels> <rank> <nprobes>
-// Reads <dir>/coef.bin (natural order) and <dir>/probes.bin (column-major);
-// writes <dir>/{matvec1,matvec,hh,schulz3}.bin.
+//                     [<cside> <clevels> <crank> <kwave> <cprobes>]
+// Reads <dir>/coef.bin (natural order), <dir>/probes.bin (column-major) and,
+// for the complex part, <dir>/cprobes.bin (column-major, interleaved);
+// writes <dir>/{matvec1,matvec,matvec_view,norm,hh,schulz3}.bin and
+// <dir>/{cmatvec,cmatvec_adj}.bin.
 #include <cstdio>
 #include <cstdlib>
 #include <string>
@@ -12,7 +19,7 @@
 
 #include "dmhm_b200.hpp"
 
-using namespace dmhm_b200;
+using namespace dmhm;
 
 static std::vector<double> read_bin(const std::string& path, size_t n) {
     std::vector<double> v(n);
@@ -77,6 +84,34 @@ int main(int argc, char** argv) {
         for (int i = 0; i < N; ++i) B.Set(i, j, P[i + (size_t)j * N]);
     A.Multiply(1.0, B, Cd);
     write_bin(dir + "/matvec.bin", Cd.LockedBuffer(), (size_t)N * k);
+    // columns 1.. of B through a locked view, into a view of a wider block
+    {
+        Dense<double> Bv, Wide(N, k + 2), Cv;
+        Bv.LockedView(B, 0, 1, N, k - 1);
+        Cv.View(Wide, 0, 2, N, k - 1);
+        A.Multiply(1.0, Bv, Cv);
+        write_bin(dir + "/matvec_view.bin", Wide.LockedBuffer(0, 2), (size_t)N * (k - 1));
+        bool threw = false;
+        try {
+            Bv.Set(0, 0, 1.0);
+        } catch (const std::logic_error&) {
+            threw = true;
+        }
+        if (!threw) {
+            std::fprintf(stderr, "a locked view accepted a write\n");
+            return 1;
+        }
+    }
+    // the norm estimate through the AbstractHMat interface
+    {
+        const AbstractHMat<double>& abs = A;
+        const double est = hmat_tools::EstimateTwoNorm(abs, 1.5, 6.0);
+        write_bin(dir + "/norm.bin", &est, 1);
+        if (abs.Height() != N || !abs.StronglyAdmissible() || abs.NumLevels() != levels) {
+            std::fprintf(stderr, "AbstractHMat queries\n");
+            return 1;
+        }
+    }
 
     HMat2d<double> C;
     A.Multiply(1.0, A, C);
@@ -135,6 +170,56 @@ int main(int argc, char** argv) {
     if (p1 != p2 || p1.size() != X.PackedSize()) {
         std::fprintf(stderr, "pack round trip differs\n");
         return 1;
+    }
+    if (argc >= 12) {
+        // HMat2d<std::complex<double>>: diagonal 4 + 0.2i - (k h)^2, h = 1/(side+1),
+        // off-diagonals -1, rows ordered x-1, x+1, y-1, y+1, diagonal
+        typedef std::complex<double> Z;
+        const int side = std::atoi(argv[7]), cl = std::atoi(argv[8]), cr = std::atoi(argv[9]);
+        const double kw = std::atof(argv[10]);
+        const int ck = std::atoi(argv[11]);
+        const int n = side * side;
+        std::vector<double> cp = read_bin(dir + "/cprobes.bin", (size_t)2 * n * ck);
+        std::vector<int> cmap;
+        HMat2d<Z>::BuildNaturalToHierarchicalMap(cmap, side, side, cl);
+        std::vector<int> cinv(n);
+        for (int i = 0; i < n; ++i) cinv[cmap[i]] = i;
+        const double h = 1.0 / (side + 1);
+        Sparse<Z> CS;
+        CS.height = CS.width = n;
+        for (int i = 0; i < n; ++i) {
+            CS.rowOffsets.push_back((int)CS.nonzeros.size());
+            const int nat = cinv[i], x = nat % side, y = nat / side;
+            int nb[4], nn = 0;
+            if (x > 0) nb[nn++] = nat - 1;
+            if (x < side - 1) nb[nn++] = nat + 1;
+            if (y > 0) nb[nn++] = nat - side;
+            if (y < side - 1) nb[nn++] = nat + side;
+            for (int q = 0; q < nn; ++q) {
+                CS.nonzeros.push_back(Z(-1.0, 0.0));
+                CS.columnIndices.push_back(cmap[nb[q]]);
+            }
+            CS.nonzeros.push_back(Z(4.0 - (kw * h) * (kw * h), 0.2));
+            CS.columnIndices.push_back(cmap[nat]);
+        }
+        CS.rowOffsets.push_back((int)CS.nonzeros.size());
+        HMat2d<Z> CA(CS, cl, cr, true, side, side);
+        if (CA.Height() != n || CA.MaxRank() != cr) {
+            std::fprintf(stderr, "complex sizes\n");
+            return 1;
+        }
+        Dense<Z> CB(n, ck), CC, CD;
+        for (int j = 0; j < ck; ++j)
+            for (int i = 0; i < n; ++i)
+                CB.Set(i, j, Z(cp[2 * (i + (size_t)j * n)], cp[2 * (i + (size_t)j * n) + 1]));
+        CA.Multiply(Z(1.0, 0.0), CB, CC);
+        write_bin(dir + "/cmatvec.bin", reinterpret_cast<const double*>(CC.LockedBuffer()),
+                  (size_t)2 * n * ck);
+        CA.AdjointMultiply(Z(0.5, -0.25), CB, CD);
+        write_bin(dir + "/cmatvec_adj.bin", reinterpret_cast<const double*>(CD.LockedBuffer()),
+                  (size_t)2 * n * ck);
+        const AbstractHMat<Z>& cabs = CA;
+        if (!(hmat_tools::EstimateTwoNorm(cabs, 1.5, 6.0) > 0)) return 1;
     }
     Finalize();
     return 0;

@@ -820,7 +820,11 @@ def schulz256_leg(device, with_reference):
     in [1, 100) (N = 65536, numLevels 6: 64-point leaves, maxRank 32,
     oversample 4) down to ||I - X A|| < 1e-8:
       plain_fp64           the reference's method (fixed rank, FP64);
-      mixed_learned_1e-10  the early iterations in the low-precision phase
+      mixed_1e-10          the early iterations in the low-precision phase
+                           (TF32 range samples, FP32 roundings) while the last
+                           estimate is above 0.1, compression tolerance 1e-10;
+      mixed_learned_1e-10  the same with learned sample counts: the early
+                           iterations in the low-precision phase
                            (TF32 range samples, FP32 roundings) while the
                            last estimate is above 0.1, compression tolerance
                            1e-10, learned sample counts (predictor trained on
@@ -869,6 +873,7 @@ def schulz256_leg(device, with_reference):
     P = np.random.default_rng(6).standard_normal((sz[0] * sz[1], 4))
     ref = None
     for mode, tol, learned, switch in (("plain_fp64", 0.0, False, 0.0),
+                                       ("mixed_1e-10", cfg["tol"], False, cfg["mixed_switch"]),
                                        ("mixed_learned_1e-10", cfg["tol"], True,
                                         cfg["mixed_switch"])):
         ctx, S = make(sz, L, cfg["seed"], tol)
@@ -894,14 +899,16 @@ def schulz256_leg(device, with_reference):
                                                      np.linalg.norm(ref)),
                      "rank_sum": H.BlockCensus()["rank_sum"], "sampling": ctx.rank_stats()}
         del H, A, ctx
-    out["speedup_vs_plain_fp64"] = (out["plain_fp64"]["seconds"] /
-                                    out["mixed_learned_1e-10"]["seconds"])
+    out["speedup_vs_plain_fp64"] = {k: out["plain_fp64"]["seconds"] / out[k]["seconds"]
+                                    for k in ("plain_fp64", "mixed_1e-10", "mixed_learned_1e-10")}
+    out["learned_speedup_vs_same_without_model"] = (out["mixed_1e-10"]["seconds"] /
+                                                     out["mixed_learned_1e-10"]["seconds"])
     return out
 
 
 HELMHOLTZ = dict(count=48, sides=(32, 48, 64, 96, 128), k_range=(2.0, 10.0), rank=24,
                  oversample=4, rhs=8, stop_tol=1e-8, mixed_switch=0.1, seed=21, leaf_target=32,
-                 streams=8, dense_check_max_n=2304)
+                 streams=8, dense_check_max_n=2304, norm_check_max_n=1024)
 
 
 def helmholtz_levels(side, target):
@@ -928,7 +935,9 @@ def helmholtz_batch_leg(device, count=None, max_side=None):
     instances and right-hand-side solves per second over the whole batch
     (wall clock from the first build to the last result), and per instance
     the residual ||A X b - b|| / ||b|| and, for N <= 2304, the relative error
-    of X b against a dense solve of the same operator."""
+    of X b against a dense solve of the same operator; for N <= 1024 also
+    the true ||I - X A||_2, the spectral radius of I - X A and cond(A) by
+    dense algebra, beside the final estimate the stop test used."""
     import concurrent.futures as cf
     import dmhm_b200 as D
     from dmhm_b200 import operators as O
@@ -969,6 +978,16 @@ def helmholtz_batch_leg(device, count=None, max_side=None):
             Ad = O.dense_from_sparse(S)
             ref = np.linalg.solve(Ad, B)
             out["rel_err_vs_dense_solve"] = float(np.linalg.norm(Y - ref) / np.linalg.norm(ref))
+        if S.height <= cfg["norm_check_max_n"]:
+            # the stop test's estimate (the reference's EstimateTwoNorm:
+            # theta ||Z^k x||^(1/k), which tends to theta times the spectral
+            # radius of Z = I - X A) beside the true ||I - X A||_2 and the
+            # condition number of A, by dense algebra
+            Xd = X.Multiply(1.0, np.eye(S.height, dtype=np.complex128))
+            Z = np.eye(S.height) - Xd @ Ad
+            out["two_norm_I_minus_XA"] = float(np.linalg.norm(Z, 2))
+            out["spectral_radius_I_minus_XA"] = float(np.max(np.abs(np.linalg.eigvals(Z))))
+            out["cond_A"] = float(np.linalg.cond(Ad))
         del X, A
         return out
 

@@ -49,6 +49,7 @@ enum WType { W_LRLR, W_LRH, W_LRD, W_HLR, W_DLR, W_HH, W_DD };
 struct WTask {
     int type;
     int a, b;
+    int c = -1;           // the C block the product is folded into (sampled products)
     double alpha;
     int m, n, r;          // W: m x n; rank r (low-rank) or dense
     // storage: aliases into A/B or owned slots in the W arena
@@ -179,6 +180,7 @@ struct Planner {
         const int kc = kind(c);
         if (kc == KIND_LOWRANK) {
             int t = product(a, b, alpha);
+            w[t].c = c;
             lops.push(c, {w[t].type == W_DD ? L_DDC : L_SET, t, 0, 0, 0.0});
         } else if (kc == KIND_NODE) {
             HMB_REQUIRE(kind(a) != KIND_DENSE && kind(b) != KIND_DENSE, HM_ERR_UNSUPPORTED,
@@ -205,6 +207,7 @@ struct Planner {
         const int kc = kind(c);
         if (kc == KIND_LOWRANK) {
             int t = product(a, b, alpha);
+            w[t].c = c;
             lops.push(c, {w[t].type == W_DD ? L_DDC : L_RUPD, t, 0, 0, beta});
         } else if (kc == KIND_NODE) {
             HMB_REQUIRE(kind(a) != KIND_DENSE && kind(b) != KIND_DENSE, HM_ERR_UNSUPPORTED,
@@ -291,6 +294,10 @@ struct Arena {
 //   4, 5 mean rank of the low-rank leaves below A's / B's block / maxRank
 //   6, 7 share of dense entries below A's / B's block
 //   8 rank cap of the product / maxRank             9 dimension / 3
+//  10 mean rank of A's low-rank leaves at the C block's own position / maxRank
+//     (in a Schulz iteration A is the previous iterate, so this is the rank
+//     the same block kept one product earlier)
+//  11 the same over the C block's siblings (the other children of its parent)
 struct SubtreeStat {
     double rank_sum = 0, lr_count = 0, dense_entries = 0, lr_entries = 0;
     bool done = false;
@@ -350,6 +357,25 @@ std::vector<float> rank_features(const Structure& S, const HMatrix& A, const HMa
         f.push_back(frac(B1.dense_entries, B1.lr_entries));
         f.push_back((float)t.r / mr);
         f.push_back((float)S.dim / 3.0f);
+        float own = 0.0f, sib = 0.0f;
+        if (t.c >= 0) {
+            subtree_stats(S, A, t.c, sa);
+            if (sa[t.c].lr_count > 0) own = (float)(sa[t.c].rank_sum / sa[t.c].lr_count) / mr;
+            const int par = S.blocks[t.c].parent;
+            if (par >= 0) {
+                double rs = 0.0, lc = 0.0;
+                for (int q = 0; q < S.q * S.q; ++q) {
+                    const int chb = S.blocks[par].first_child + q;
+                    if (chb == t.c) continue;
+                    subtree_stats(S, A, chb, sa);
+                    rs += sa[chb].rank_sum;
+                    lc += sa[chb].lr_count;
+                }
+                if (lc > 0) sib = (float)(rs / lc) / mr;
+            }
+        }
+        f.push_back(own);
+        f.push_back(sib);
     }
     return f;
 }
@@ -369,26 +395,18 @@ __global__ void sq_norms_kernel(const double* const* __restrict__ p, const long 
     if (threadIdx.x == 0) out[blockIdx.x] = red[0];
 }
 
-// Squared Frobenius norms of the listed (pointer, length) arrays (host result).
-std::vector<double> sq_norms(Context& ctx, const std::vector<const double*>& ptr,
-                             const std::vector<long long>& len) {
-    std::vector<double> out(ptr.size(), 0.0);
-    if (ptr.empty()) return out;
+// Squared Frobenius norms of the listed arrays into out[0 .. n) on the
+// device (no host synchronization).
+void sq_norms_device(Context& ctx, const std::vector<const double*>& ptr,
+                     const std::vector<long long>& len, double* out) {
+    if (ptr.empty()) return;
     DeviceBuffer<const double*> dp;
     DeviceBuffer<long long> dl;
-    DeviceBuffer<double> dout;
     dp.upload(ptr, ctx.stream);
     dl.upload(len, ctx.stream);
-    dout.allocate(ptr.size(), ctx.stream);
-    {
-        LaunchScope ls(ctx, "probe_norms");
-        sq_norms_kernel<<<(unsigned)ptr.size(), 256, 0, ctx.stream>>>(dp.get(), dl.get(), dout.get());
-        HMB_CHECK_LAUNCH();
-    }
-    HMB_CUDA(cudaMemcpyAsync(out.data(), dout.get(), out.size() * sizeof(double),
-                             cudaMemcpyDeviceToHost, ctx.stream));
-    HMB_CUDA(cudaStreamSynchronize(ctx.stream));
-    return out;
+    LaunchScope ls(ctx, "probe_norms");
+    sq_norms_kernel<<<(unsigned)ptr.size(), 256, 0, ctx.stream>>>(dp.get(), dl.get(), out);
+    HMB_CHECK_LAUNCH();
 }
 
 // Relative error of every listed compression W ~= alpha A_a B_b, estimated
@@ -438,7 +456,11 @@ std::vector<double> probe_errors(Context& ctx, const Structure& S, const HMatrix
         ptr[i] = P0 + y_off[i];
         len[i] = (long long)w[ids[i]].m * q;
     }
-    const std::vector<double> ref = sq_norms(ctx, ptr, len);
+    // both norms (before and after subtracting U V^T G) land in one device
+    // array and come back with one synchronization
+    DeviceBuffer<double> nrm;
+    nrm.allocate(2 * ids.size(), ctx.stream);
+    sq_norms_device(ctx, ptr, len, nrm.get());
     std::vector<GemmOp> g1, g2;
     for (size_t i = 0; i < ids.size(); ++i) {
         const WTask& t = w[ids[i]];
@@ -448,7 +470,13 @@ std::vector<double> probe_errors(Context& ctx, const Structure& S, const HMatrix
     }
     launch_gemm_ops(ctx, g1, "probe_vg");
     launch_gemm_ops(ctx, g2, "probe_residual");
-    const std::vector<double> res = sq_norms(ctx, ptr, len);
+    sq_norms_device(ctx, ptr, len, nrm.get() + ids.size());
+    std::vector<double> both(2 * ids.size());
+    HMB_CUDA(cudaMemcpyAsync(both.data(), nrm.get(), both.size() * sizeof(double),
+                             cudaMemcpyDeviceToHost, ctx.stream));
+    HMB_CUDA(cudaStreamSynchronize(ctx.stream));
+    const double* ref = both.data();
+    const double* res = both.data() + ids.size();
     std::vector<double> rel(ids.size());
     for (size_t i = 0; i < ids.size(); ++i)
         rel[i] = ref[i] > 0.0 ? std::sqrt(res[i] / ref[i]) : (res[i] > 0.0 ? 1.0 : 0.0);
@@ -927,9 +955,14 @@ void hh_multiply_roots(Context& ctx, const HMatrix& A, const HMatrix& B, double 
     if (!hh.empty()) sample(hh);
     if (learned) {
         // probe check: redo with the plain sample count every compression
-        // whose estimated error exceeds the tolerance's scale
+        // whose estimated error exceeds the tolerance's scale; in the
+        // low-precision phase the FP32 roundings resolve no tolerance finer
+        // than 1e-6, which is then the scale (a plain redo could not do
+        // better there)
         const std::vector<double> err = probe_errors(ctx, S, A, B, P.w, hh);
-        const double limit = std::max(10.0 * ctx.compression_tol, 1e-13);
+        const double scale = ctx.low_precision ? std::max(ctx.compression_tol, kLowPrecisionTolFloor)
+                                               : ctx.compression_tol;
+        const double limit = std::max(10.0 * scale, 1e-13);
         std::vector<int> redo;
         for (size_t i = 0; i < hh.size(); ++i)
             if (!(err[i] <= limit) && P.w[hh[i]].k < k_plain[i]) redo.push_back((int)i);

@@ -45,7 +45,7 @@ template <> struct Prec<double> {
 };
 template <> struct Prec<float> {
     static constexpr float jtol = 1e-6f, tiny = 1e-12f;
-    static constexpr double tol_floor = 1e-6;
+    static constexpr double tol_floor = kLowPrecisionTolFloor;
 };
 
 __device__ __forceinline__ double r_sqrt(double x) { return sqrt(x); }

@@ -7,6 +7,10 @@
 
 namespace hmb {
 
+// Finest relative truncation tolerance the FP32 roundings of the
+// low-precision phase resolve (a coarser one applies as given).
+constexpr double kLowPrecisionTolFloor = 1e-6;
+
 enum RoundKind : int {
     ROUND_SET = 0,      // out = (alpha U1, V1)
     ROUND_CONCAT = 1,   // out = ([beta U2, alpha U1], [V2, V1])      (exact)

@@ -6,7 +6,7 @@
 
 namespace hmb {
 
-constexpr int kMlpFeatures = 10;
+constexpr int kMlpFeatures = 12;
 constexpr int kMlpHidden = 64;
 constexpr int kMlpParams =
     kMlpHidden * kMlpFeatures + kMlpHidden + kMlpHidden * kMlpHidden + kMlpHidden + kMlpHidden + 1;

@@ -8,7 +8,7 @@ central finite differences in tests/test_mlp.py and checks the GPU
 gradients in tests/test_mlp_gpu.py.  Computed in float64."""
 import numpy as np
 
-F, H = 10, 64
+F, H = 12, 64
 OW1, OB1 = 0, H * F
 OW2, OB2 = OB1 + H, OB1 + H + H * H
 OW3, OB3 = OB2 + H, OB2 + H + H

@@ -433,11 +433,14 @@ struct WideSmemT {
 };
 using WideSmem = WideSmemT<double>;
 
+// The copies carry no "memory" clobber: their shared-memory destinations are
+// read only after cp_async_wait (which has one) and a barrier, and without
+// it the compiler may keep the work-list fields that address the copies in
+// registers instead of reloading them from global memory after every copy.
 __device__ __forceinline__ void cp_async4(float* dst, const float* src, bool valid) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src),
-                 "r"(valid ? 4 : 0)
-                 : "memory");
+                 "r"(valid ? 4 : 0));
 }
 
 // TF32 tensor-core MMA 16 x 8 x 8, FP32 accumulation.  Fragments (g = lane/4,
@@ -460,8 +463,7 @@ __device__ __forceinline__ float round_tf32(double x) {
 __device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src),
-                 "r"(valid ? 8 : 0)
-                 : "memory");
+                 "r"(valid ? 8 : 0));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
@@ -580,8 +582,10 @@ __device__ __forceinline__ const int* chunk_prefix(const JobExec& J) { return PH
 
 // TF: the TF32 form (FP32 copy of the blocks and of the input, TF32
 // tensor-core MMA, FP32 accumulation, FP64 output).
+// At most 128 registers a thread, so that 4 CTAs share an SM (152 without
+// the bound: 3 CTAs per SM, 2 % slower on the 128 x 128, 64-column product).
 template <int PHASE, bool TF>
-__global__ void __launch_bounds__(WTHREADS)
+__global__ void __launch_bounds__(WTHREADS, 4)
 wide_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0, long long C, int G) {
     using E = typename std::conditional<TF, float, double>::type;
     extern __shared__ __align__(16) unsigned char wide_smem[];
@@ -781,7 +785,32 @@ wide_kernel(const JobExec* __restrict__ jobs, int njobs, const JobExec job0, lon
                 store_out(J, it, i, y * WT + c, v);
             }
         };
-        if (whole) {
+        if (whole && PHASE == 1) {
+            // the thread's 32 accumulators lie in 4 tile rows: their T
+            // offsets are loaded once, before the stores (which the compiler
+            // must otherwise assume may change them)
+            auto rslot = [](int k) { return TF ? (((k >> 4) << 1) | ((k >> 1) & 1)) : (k >> 3); };
+            long long rbase[4], rstep[4];
+            const long long kk = J.k;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int i = arow(TF ? (((q >> 1) << 4) | ((q & 1) << 1)) : q * 8);
+                const bool ok = i < rows;
+                rbase[q] = ok ? wt->trel[i] * kk + wt->tj[i] : 0;
+                rstep[q] = ok ? (long long)wt->tr[i] : 0;
+            }
+            double* Tp = J.T;
+            float* T32p = J.T32;
+#pragma unroll
+            for (int k = 0; k < 32; ++k) {
+                const int i = arow(k), c = acol(k);
+                if (i < rows && c < cols) {
+                    const long long o = rbase[rslot(k)] + (long long)(y * WT + c) * rstep[rslot(k)];
+                    if constexpr (TF) T32p[o] = round_tf32((double)acc[k]);
+                    else Tp[o] = (double)acc[k];
+                }
+            }
+        } else if (whole) {
 #pragma unroll
             for (int k = 0; k < 32; ++k) {
                 const int i = arow(k), c = acol(k);

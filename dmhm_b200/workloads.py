@@ -7,7 +7,7 @@
 
 The 128 x 128 operator is the five-point grid operator (c ~ U[1, 2), seed
 2), numLevels 5 (64-point leaves), maxRank 16, strong admissibility, every
-admissible block at full rank (SetToRandom): 274 MB of block data, more than
+admissible block at full rank (SetToRandom): 275.6 MB of block data, more than
 the 126 MB L2.  The 64 x 64 Schulz case has numLevels 4, maxRank 16 and
 oversample 4.  Each workload builds its operator, runs its products and
 prints "done"; run it under a profiler with a kernel filter and a launch

@@ -3,7 +3,8 @@
     python -m dmhm_b200.workloads matmul [k]   # 128 x 128 operator, k-column H x dense (k = 64)
     python -m dmhm_b200.workloads matvec       # the same operator, one vector, four products
     python -m dmhm_b200.workloads tf32 [k]     # TF32 H x dense, mma.sync form, three products
-    python -m dmhm_b200.workloads schulz64     # SchulzInvert(3) on the 64 x 64 operator
+    python -m dmhm_b200.workloads schulz64 [n] # SchulzInvert(n = 3) on the 64 x 64 operator
+    python -m dmhm_b200.workloads direct       # DirectInvert on the 32 x 32 operator
 
 The 128 x 128 operator is the five-point grid operator (c ~ U[1, 2), seed
 2), numLevels 5 (64-point leaves), maxRank 16, strong admissibility, every
@@ -83,6 +84,18 @@ def schulz64(iterations: int = 3):
     ctx.synchronize()
 
 
+def direct():
+    """DirectInvert on the 32 x 32 operator (numLevels 4: 16-point leaves,
+    maxRank 8, oversample 4)."""
+    sizes = (32, 32)
+    ctx = Context(0)
+    ctx.set_oversample(4)
+    S = operators.stencil(sizes, operators.uniform_coefficients(sizes, 2), 4)
+    H = HMat2d(S, 4, 8, True, *sizes, ctx=ctx)
+    H.DirectInvert()
+    ctx.synchronize()
+
+
 def main(argv):
     case = argv[0] if argv else "matmul"
     arg = int(argv[1]) if len(argv) > 1 else None
@@ -94,6 +107,8 @@ def main(argv):
         tf32(arg or 64)
     elif case == "schulz64":
         schulz64(arg or 3)
+    elif case == "direct":
+        direct()
     else:
         raise SystemExit(f"unknown workload {case}")
     print("done")

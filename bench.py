@@ -41,9 +41,9 @@ REF_DRIVER = os.path.join(ROOT, "oracle", "_ref", "dmhm_ref_driver")
 # workload, each from one ncu capture (dram__bytes_read.sum +
 # dram__bytes_write.sum) of `python -m dmhm_b200.workloads`: FP64 64-column
 # product phases and the one-vector product
-KERNEL_TRAFFIC = {"hmm_row_tiles": (257.7 + 12.2) * 1e6,
-                  "hmm_lowrank_inner": (127.5 + 46.4) * 1e6,
-                  "hmv_blocks": (276.4 + 3.3) * 1e6}
+KERNEL_TRAFFIC = {"hmm_row_tiles": (257.1 + 10.4) * 1e6,
+                  "hmm_lowrank_inner": (127.8 + 46.8) * 1e6,
+                  "hmv_blocks": (276.4 + 3.8) * 1e6}
 
 
 class Replicas:
@@ -797,6 +797,15 @@ def hh3d_leg(device):
         ctx.synchronize()
         secs = time.perf_counter() - t1
         stats1 = ctx.rank_stats()
+        # where a product's time goes: device time per kernel and host time
+        # per phase of one more product (events around every launch)
+        from dmhm_b200 import _lib
+        _lib.check(_lib.lib().hm_profile_enable(ctx.handle, 1))
+        Cp = A.Multiply(1.0, A)
+        prof = read_profile(ctx)
+        _lib.check(_lib.lib().hm_profile_enable(ctx.handle, 0))
+        del Cp
+        top = sorted(prof.items(), key=lambda kv: -kv[1]["ms"])[:10]
         cp = Cm.Multiply(1.0, P)
         if exact is None:
             exact = A.Multiply(1.0, A.Multiply(1.0, P))
@@ -807,7 +816,8 @@ def hh3d_leg(device):
                      "rel_err_vs_exact": float(np.linalg.norm(cp - exact) /
                                                np.linalg.norm(exact)),
                      "rank_sum": Cm.BlockCensus()["rank_sum"],
-                     "sampling": {k: stats1[k] - stats0[k] for k in stats1}}
+                     "sampling": {k: stats1[k] - stats0[k] for k in stats1},
+                     "profile_ms": {k: round(v["ms"], 3) for k, v in top}}
         del Cm, A, ctx
     out["learned_speedup_vs_plain"] = out["plain"]["seconds"] / out["learned"]["seconds"]
     return out

@@ -432,7 +432,8 @@ def gpu_arm(args):
         line["schulz256"] = schulz256_leg(local, rank == 0 and not args.no_cpu_baseline)
     if args.helmholtz_count > 0 and "helmholtz" in legs:
         line["helmholtz_batch"] = helmholtz_batch_leg(local, args.helmholtz_count,
-                                                      args.helmholtz_max_side or None)
+                                                      args.helmholtz_max_side or None,
+                                                      args.helmholtz_tol or None)
     if rank == 0:
         print(json.dumps(line))
     group.close()
@@ -956,7 +957,7 @@ def helmholtz_levels(side, target):
     return best[0]
 
 
-def helmholtz_batch_leg(device, count=None, max_side=None):
+def helmholtz_batch_leg(device, count=None, max_side=None, tol=None):
     """Batch of independent HMat2d<std::complex<double>> instances: shifted
     five-point Helmholtz-like operators (diagonal 4 + 0.2i - (k h)^2,
     off-diagonals -1, h = 1/(side+1), k uniform in [2, 10), sides drawn from
@@ -988,6 +989,8 @@ def helmholtz_batch_leg(device, count=None, max_side=None):
     ctxs = [D.Context(device) for _ in range(nthreads)]
     for c in ctxs:
         c.set_oversample(cfg["oversample"])
+        if tol:
+            c.set_compression_tolerance(tol)
 
     def solve(job):
         slot, (i, side, k) = job
@@ -1036,6 +1039,7 @@ def helmholtz_batch_leg(device, count=None, max_side=None):
                         f"(sides {sorted(set(t[1] for t in inst))}, maxRank {cfg['rank']}, "
                         f"oversample {cfg['oversample']}), mixed SchulzInvert to 1e-8, "
                         f"{cfg['rhs']} complex right-hand sides each, {nthreads} streams",
+            "compression_tolerance": tol or 0.0,
             "instances_per_s": len(inst) / wall, "rhs_solves_per_s": len(inst) * cfg["rhs"] / wall,
             "wall_s": wall, "max_residual": max(r["residual_AXb_minus_b"] for r in results),
             "max_rel_err_vs_dense": max((r["rel_err_vs_dense_solve"] for r in results
@@ -1068,6 +1072,8 @@ def main():
     # instances take tens of minutes: --helmholtz-count 48 --helmholtz-max-side 0)
     ap.add_argument("--helmholtz-count", type=int, default=8)
     ap.add_argument("--helmholtz-max-side", type=int, default=48)
+    # compression tolerance of the batch's products (0: fixed rank maxRank)
+    ap.add_argument("--helmholtz-tol", type=float, default=0.0)
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)

@@ -377,6 +377,12 @@ __device__ void do_round(const RoundOp& op_in, R* dyn, long long smem_elems, Rou
     if (m == 0 || n == 0) return;
     const int ku = ortho ? op.r1 : min(m, k);
     const int kv = dense ? n : min(n, k);
+    // A block no taller than its stack (m <= k): the QR of the U stack would
+    // only rotate the core's rows (Q_u is m x m), which changes neither the
+    // column inner products one-sided Jacobi works on nor the rounding, so
+    // the core is formed from the stack itself, M = U_cat R_v^T (or the
+    // dense block), and its rotated columns are the output U directly.
+    const bool skip_u = !ortho && m <= k;
     // The core and the rotations live in shared memory when they fit in
     // `smem_elems`; the stacked factors in the (L1-cached) work area.
     const long long need_mj = (long long)ku * kv + (long long)kv * kv;
@@ -433,7 +439,7 @@ __device__ void do_round(const RoundOp& op_in, R* dyn, long long smem_elems, Rou
     __syncthreads();
 
     // ---- QR of the stacks ------------------------------------------------
-    if (!ortho) cta_qr(Ucat, m, k, m, tauU, red);
+    if (!ortho && !skip_u) cta_qr(Ucat, m, k, m, tauU, red);
     if (!dense) cta_qr(Vcat, n, k, n, tauV, red);
 
     // ---- core M = R_u R_v^T (ku x kv) -------------------------------------
@@ -442,7 +448,11 @@ __device__ void do_round(const RoundOp& op_in, R* dyn, long long smem_elems, Rou
         if (ortho) {
             v = (i >= l) ? Vcat[l + (long long)i * n] : R(0);     // R_v^T
         } else if (dense) {
-            v = (l >= i) ? Ucat[i + (long long)l * m] : R(0);     // R_u (ku x n)
+            if (skip_u) v = Ucat[i + (long long)l * m];             // the block itself
+            else v = (l >= i) ? Ucat[i + (long long)l * m] : R(0);  // R_u (ku x n)
+        } else if (skip_u) {
+            for (int p = l; p < k; ++p)                              // U_cat R_v^T
+                v = r_fma(Ucat[i + (long long)p * m], Vcat[l + (long long)p * n], v);
         } else {
             for (int p = max(i, l); p < k; ++p)
                 v = r_fma(Ucat[i + (long long)p * m], Vcat[l + (long long)p * n], v);
@@ -492,7 +502,7 @@ __device__ void do_round(const RoundOp& op_in, R* dyn, long long smem_elems, Rou
             (i < kv && c < keep) ? (double)J[i + (long long)order[c] * kv] : 0.0;
     });
     __syncthreads();
-    if (!ortho) cta_apply_q(Ucat, m, min(m, k), m, tauU, op.uo, rout, m);
+    if (!ortho && !skip_u) cta_apply_q(Ucat, m, min(m, k), m, tauU, op.uo, rout, m);
     if (!dense) cta_apply_q(Vcat, n, min(n, k), n, tauV, op.vo, rout, n);
 }
 

@@ -133,10 +133,19 @@ def round_factors(U: np.ndarray, V: np.ndarray, rout: int, tol: float = 0.0,
     more QR of the core; Drmac and Veselic, SIAM J. Matrix Anal. Appl. 29,
     2008): R_4^T J = W gives M = W (Q_4 J)^T, so U_out = Q_u W[:, kept] and
     V_out = Q_v Q_4 J[:, kept] keep the same convention, in fewer sweeps on
-    graded cores.  Returns (U_out, V_out, sweeps)."""
-    Qu, Ru = sla.qr(np.asarray(U, dtype=dtype), mode="economic")
+    graded cores.  A block no taller than its stack (m <= k) skips the QR of
+    U: the core is U R_v^T = Q_u M, whose columns have M's inner products, so
+    the Jacobi rotations and the rounding are the same, and the rotated
+    columns are U_out directly.  Returns (U_out, V_out, sweeps)."""
+    U = np.asarray(U, dtype=dtype)
+    m, k = U.shape
     Qv, Rv = sla.qr(np.asarray(V, dtype=dtype), mode="economic")
-    core = Ru @ Rv.T
+    if m <= k:
+        Qu = np.eye(m, dtype=dtype)
+        core = U @ Rv.T
+    else:
+        Qu, Ru = sla.qr(U, mode="economic")
+        core = Ru @ Rv.T
     if precondition:
         Q4, R4 = sla.qr(core.T, mode="economic")
         M, J, sweeps = jacobi(R4.T, dtype)

@@ -257,16 +257,22 @@ void hmat_direct_invert(Context& ctx, HMatrix& X) {
     HMB_REQUIRE(X.S->dof == 1, HM_ERR_UNSUPPORTED, "DirectInvert is built for real matrices");
     HMB_REQUIRE(X.S->blocks[0].kind != KIND_LOWRANK, HM_ERR_UNSUPPORTED,
                 "Cannot invert low-rank matrices");
-    // the serial HMat2d / HMat3d products truncate to the fixed rank maxRank
+    // the serial HMat2d / HMat3d products truncate to the fixed rank maxRank,
+    // in FP64: the context's tolerance and low-precision phase are set aside
+    // for the call and restored afterwards
     const double tol = ctx.compression_tol;
+    const bool low = ctx.low_precision;
     ctx.compression_tol = 0.0;
+    ctx.low_precision = false;
     try {
         invert_node(ctx, X, 0);
     } catch (...) {
         ctx.compression_tol = tol;
+        ctx.low_precision = low;
         throw;
     }
     ctx.compression_tol = tol;
+    ctx.low_precision = low;
     ctx.check_numerical();
 }
 

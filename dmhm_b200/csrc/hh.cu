@@ -58,6 +58,7 @@ struct WTask {
     const double* D = nullptr;
     int ldU = 0, ldV = 0;
     long long u_off = -1, v_off = -1, d_off = -1, g_off = -1;
+    bool u_alias = false, v_alias = false;   // U is A's block's U / V is B's block's V
     // randomized sampling
     int k = 0, kq = 0;
     uint64_t omega = 0;
@@ -512,6 +513,17 @@ struct SymPlan {
     std::vector<int> crank, state_rank, op_kind;
     std::vector<int> k0, kq0;   // plain sample counts per task
     std::shared_ptr<BlockCache> blocks;
+    // Fixed by the plan's ranks, set by its first product: the W arena and
+    // sampling scratch layout (offsets in the tasks) and the tasks a cached
+    // product touches on the host -- the sampled products (node x node of
+    // nonzero rank) and the node x low-rank / low-rank x node products, whose
+    // factor is an H x dense product.  A product in 3-D has millions of
+    // tasks, nearly all of rank 0 or served by the cached leaf and block
+    // lists, so the per-product host work follows these lists only.
+    bool laid_out = false;
+    long long wa_used = 0, sa_used = 0;
+    std::vector<int> hh_ids, hlr_ids, lrh_ids;
+    std::vector<int> hh_pos;   // per task: its index in hh_ids, or -1
 };
 
 struct SymKey {
@@ -674,6 +686,79 @@ std::shared_ptr<SymPlan> get_plan(Context& ctx, const HMatrix& A, const HMatrix&
     return plan;
 }
 
+// The W arena and sampling scratch layout of a plan (offsets kept in its
+// tasks; the ranks, and with them every size, are part of the plan's key)
+// and its short task lists.  Low-rank factors that a product passes through
+// unchanged alias A's U or B's V instead of taking a slot.
+void lay_out_tasks(const Structure& S, const HMatrix& A, const HMatrix& B, SymPlan& plan) {
+    Arena wa, sa;
+    plan.hh_pos.assign(plan.w.size(), -1);
+    for (size_t i = 0; i < plan.w.size(); ++i) {
+        WTask& t = plan.w[i];
+        const Block& Ba = S.blocks[t.a];
+        const Block& Bb = S.blocks[t.b];
+        switch (t.type) {
+            case W_LRLR:
+                if (A.rank[t.a] <= B.rank[t.b]) {
+                    t.u_alias = true; t.ldU = Ba.m;
+                    t.v_off = wa.take((long long)t.n * t.r); t.ldV = t.n;
+                } else {
+                    t.u_off = wa.take((long long)t.m * t.r); t.ldU = t.m;
+                    t.v_alias = true; t.ldV = Bb.n;
+                }
+                t.g_off = wa.take((long long)B.rank[t.b] * A.rank[t.a]);
+                break;
+            case W_LRH:
+            case W_LRD:
+                t.u_alias = true; t.ldU = Ba.m;
+                t.v_off = wa.take((long long)t.n * t.r); t.ldV = t.n;
+                if (t.type == W_LRH && t.r > 0) plan.lrh_ids.push_back((int)i);
+                break;
+            case W_HLR:
+            case W_DLR:
+                t.u_off = wa.take((long long)t.m * t.r); t.ldU = t.m;
+                t.v_alias = true; t.ldV = Bb.n;
+                if (t.type == W_HLR && t.r > 0) plan.hlr_ids.push_back((int)i);
+                break;
+            case W_HH: {
+                // sampling scratch at the plain sample counts (the learned
+                // counts are never larger)
+                const int k = plan.k0[i], kq = plan.kq0[i];
+                t.u_off = wa.take((long long)t.m * t.r); t.ldU = t.m;
+                t.v_off = wa.take((long long)t.n * t.r); t.ldV = t.n;
+                t.s_omega = sa.take((long long)Bb.n * k);
+                t.s_x = sa.take((long long)Bb.m * k);
+                t.s_y = sa.take((long long)Ba.m * k);
+                t.s_q = sa.take((long long)Ba.m * kq);
+                t.s_tau = sa.take(k);
+                t.s_z1 = sa.take((long long)Ba.n * kq);
+                t.s_z = sa.take((long long)Bb.n * kq);
+                RoundOp probe{};
+                probe.kind = ROUND_ORTHO; probe.m = t.m; probe.n = t.n; probe.r1 = kq;
+                t.s_work = sa.take(round_work_size(probe));
+                if (t.r > 0) {
+                    plan.hh_pos[i] = (int)plan.hh_ids.size();
+                    plan.hh_ids.push_back((int)i);
+                }
+                break;
+            }
+            case W_DD:
+                t.d_off = wa.take((long long)t.m * t.n);
+                break;
+        }
+    }
+    plan.wa_used = wa.used;
+    plan.sa_used = sa.used;
+    plan.laid_out = true;
+}
+
+// A task's factor addresses in this product's buffers.
+void bind_task(WTask& t, double* W0, const HMatrix& A, const HMatrix& B) {
+    t.U = t.u_alias ? A.U(t.a) : (t.u_off >= 0 ? W0 + t.u_off : nullptr);
+    t.V = t.v_alias ? B.V(t.b) : (t.v_off >= 0 ? W0 + t.v_off : nullptr);
+    t.D = t.d_off >= 0 ? W0 + t.d_off : nullptr;
+}
+
 }  // namespace
 
 void hh_multiply(Context& ctx, const HMatrix& A, const HMatrix& B, double alpha, double beta,
@@ -723,17 +808,20 @@ void hh_multiply_roots(Context& ctx, const HMatrix& A, const HMatrix& B, double 
     const std::shared_ptr<SymPlan> plan =
         get_plan(ctx, A, B, C, alpha, beta, fresh_plan, maxRankC, roots);
     hs.reset(new HostScope(ctx, "hh_plan_copy"));
-    // The plan's task list is used in place: every per-product field
-    // (generator positions, arena offsets, pointers, sample counts) is
-    // rewritten below before it is read; sample counts start from the plan's.
+    // The plan's task list is used in place: its arena offsets are fixed
+    // with the plan; the per-product fields of the tasks this product reads
+    // (generator positions, factor addresses, sample counts) are rewritten
+    // below before they are read; sample counts start from the plan's.
     struct PlanView {
         std::vector<WTask>& w;
         const PerBlock<LOp>& lops;
         const PerBlock<DOp>& dops;
     } P{plan->w, plan->lops, plan->dops};
-    for (size_t i = 0; i < P.w.size(); ++i) {
+    if (!plan->laid_out) lay_out_tasks(S, A, B, *plan);
+    const std::vector<int>& hh = plan->hh_ids;
+    const std::vector<int>& hh_pos = plan->hh_pos;
+    for (int i : hh) {
         WTask& t = P.w[i];
-        if (t.type != W_HH) continue;
         // generator positions of the samples, from this call's starting state
         t.omega = lcg_skip_host(ctx.serial_state, t.omega_steps);
         t.k = plan->k0[i];
@@ -763,65 +851,24 @@ void hh_multiply_roots(Context& ctx, const HMatrix& A, const HMatrix& B, double 
     C.rank = crank;
     C.layout();
 
-    // W arena and sampling scratch
-    Arena wa, sa;
-    for (WTask& t : P.w) {
-        const Block& Ba = S.blocks[t.a];
-        const Block& Bb = S.blocks[t.b];
-        switch (t.type) {
-            case W_LRLR:
-                if (A.rank[t.a] <= B.rank[t.b]) {
-                    t.U = A.U(t.a); t.ldU = Ba.m;
-                    t.v_off = wa.take((long long)t.n * t.r); t.ldV = t.n;
-                } else {
-                    t.u_off = wa.take((long long)t.m * t.r); t.ldU = t.m;
-                    t.V = B.V(t.b); t.ldV = Bb.n;
-                }
-                t.g_off = wa.take((long long)B.rank[t.b] * A.rank[t.a]);
-                break;
-            case W_LRH:
-            case W_LRD:
-                t.U = A.U(t.a); t.ldU = Ba.m;
-                t.v_off = wa.take((long long)t.n * t.r); t.ldV = t.n;
-                break;
-            case W_HLR:
-            case W_DLR:
-                t.u_off = wa.take((long long)t.m * t.r); t.ldU = t.m;
-                t.V = B.V(t.b); t.ldV = Bb.n;
-                break;
-            case W_HH: {
-                t.u_off = wa.take((long long)t.m * t.r); t.ldU = t.m;
-                t.v_off = wa.take((long long)t.n * t.r); t.ldV = t.n;
-                t.s_omega = sa.take((long long)Bb.n * t.k);
-                t.s_x = sa.take((long long)Bb.m * t.k);
-                t.s_y = sa.take((long long)Ba.m * t.k);
-                t.s_q = sa.take((long long)Ba.m * t.kq);
-                t.s_tau = sa.take(t.k);
-                t.s_z1 = sa.take((long long)Ba.n * t.kq);
-                t.s_z = sa.take((long long)Bb.n * t.kq);
-                RoundOp probe{};
-                probe.kind = ROUND_ORTHO; probe.m = t.m; probe.n = t.n; probe.r1 = t.kq;
-                t.s_work = sa.take(round_work_size(probe));
-                break;
-            }
-            case W_DD:
-                t.d_off = wa.take((long long)t.m * t.n);
-                break;
-        }
-    }
-    double* W0 = ctx.scratch(0, wa.used);
-    double* S0 = ctx.scratch(1, sa.used);
-    for (WTask& t : P.w) {
-        if (t.u_off >= 0) t.U = W0 + t.u_off;
-        if (t.v_off >= 0) t.V = W0 + t.v_off;
-        if (t.d_off >= 0) t.D = W0 + t.d_off;
+    // W arena and sampling scratch (laid out with the plan)
+    double* W0 = ctx.scratch(0, plan->wa_used);
+    double* S0 = ctx.scratch(1, plan->sa_used);
+    // leaf and block lists cached with the plan replay position-independently;
+    // building them reads every task's factors, a replay only the listed ones
+    const bool a_is_b = A.data.get() == B.data.get();
+    std::shared_ptr<BlockCache> bc = plan->blocks;
+    if (bc && (bc->tol != ctx.compression_tol || bc->a_is_b != a_is_b)) bc.reset();
+    if (bc && bc->leaves_cached) {
+        for (int i : hh) bind_task(P.w[i], W0, A, B);
+        for (int i : plan->hlr_ids) bind_task(P.w[i], W0, A, B);
+        for (int i : plan->lrh_ids) bind_task(P.w[i], W0, A, B);
+    } else {
+        for (WTask& t : P.w) bind_task(t, W0, A, B);
     }
 
     // ---------------- randomized sampling ----------------
     hs.reset(new HostScope(ctx, "hh_sampling"));
-    std::vector<int> hh;
-    for (int i = 0; i < (int)P.w.size(); ++i)
-        if (P.w[i].type == W_HH && P.w[i].r > 0) hh.push_back(i);
     const bool log_ranks = ctx.rank_log && ctx.compression_tol > 0.0 && !hh.empty();
     const bool learned = ctx.rank_model != nullptr && !hh.empty();
     std::vector<float> feats;
@@ -846,8 +893,6 @@ void hh_multiply_roots(Context& ctx, const HMatrix& A, const HMatrix& B, double 
     // kept ranks of the sampled products (truncating runs: later operations
     // read them on the device, the log reads them back)
     DeviceBuffer<int> kept;
-    std::vector<int> hh_pos(P.w.size(), -1);
-    for (size_t i = 0; i < hh.size(); ++i) hh_pos[hh[i]] = (int)i;
     if (ctx.compression_tol > 0.0 && !hh.empty()) kept.allocate(hh.size(), st);
     // the sampling pipeline for the listed tasks, at their current k
     auto sample = [&](const std::vector<int>& ids) {
@@ -939,16 +984,18 @@ void hh_multiply_roots(Context& ctx, const HMatrix& A, const HMatrix& B, double 
     // low-rank x node
     {
         std::vector<MatJob> jobs;
-        for (const WTask& t : P.w)
-            if (t.type == W_HLR && t.r > 0)
-                jobs.push_back({&A, t.a, false, t.alpha, 0.0, B.U(t.b), S.blocks[t.b].m,
-                                const_cast<double*>(t.U), t.m, t.r});
+        for (int i : plan->hlr_ids) {
+            const WTask& t = P.w[i];
+            jobs.push_back({&A, t.a, false, t.alpha, 0.0, B.U(t.b), S.blocks[t.b].m,
+                            const_cast<double*>(t.U), t.m, t.r});
+        }
         run_jobs(ctx, jobs);
         jobs.clear();
-        for (const WTask& t : P.w)
-            if (t.type == W_LRH && t.r > 0)
-                jobs.push_back({&B, t.b, true, t.alpha, 0.0, A.V(t.a), S.blocks[t.a].n,
-                                const_cast<double*>(t.V), t.n, t.r});
+        for (int i : plan->lrh_ids) {
+            const WTask& t = P.w[i];
+            jobs.push_back({&B, t.b, true, t.alpha, 0.0, A.V(t.a), S.blocks[t.a].n,
+                            const_cast<double*>(t.V), t.n, t.r});
+        }
         run_jobs(ctx, jobs);
     }
     hs.reset(new HostScope(ctx, "hh_sample_pipeline"));
@@ -1007,9 +1054,6 @@ void hh_multiply_roots(Context& ctx, const HMatrix& A, const HMatrix& B, double 
     // ---------------- leaf products ----------------
     // Cached with the plan's block lists (position-independent, reloc.h):
     // they depend on the plan and on whether A and B are one matrix.
-    const bool a_is_b = A.data.get() == B.data.get();
-    std::shared_ptr<BlockCache> bc = plan->blocks;
-    if (bc && (bc->tol != ctx.compression_tol || bc->a_is_b != a_is_b)) bc.reset();
     RelocBases leaf_bases{};
     leaf_bases.d[0] = W0;
     leaf_bases.d[1] = const_cast<double*>(A.data.get());
@@ -1061,7 +1105,7 @@ void hh_multiply_roots(Context& ctx, const HMatrix& A, const HMatrix& B, double 
         }
         // position-independent copies; kept once the block lists are cached
         Relocator rel;
-        rel.add(0, W0, wa.used);
+        rel.add(0, W0, plan->wa_used);
         rel.add(1, A.data.get(), A.total);
         rel.add(2, B.data.get(), B.total);
         std::vector<GemmOp> t1 = g1, t2 = g2;
@@ -1265,7 +1309,7 @@ void hh_multiply_roots(Context& ctx, const HMatrix& A, const HMatrix& B, double 
 
         // position-independent copy for the cache
         Relocator rel;
-        rel.add(0, W0, wa.used);
+        rel.add(0, W0, plan->wa_used);
         rel.add(1, A.data.get(), A.total);
         rel.add(2, B.data.get(), B.total);
         rel.add(3, C.data.get(), C.total);

@@ -1219,7 +1219,19 @@ void hh_multiply_roots(Context& ctx, const HMatrix& A, const HMatrix& B, double 
                 long long wmax = 0;
                 const size_t first = rops.size();
                 int prev = -1;   // op whose output is (cu, cv)
-                for (int j = 0; j < nops; ++j) {
+                // An update by a product of rank 0 with beta = 1 that keeps
+                // the state's rank leaves the state as it is (its rounding
+                // would be an exact copy): it is not emitted, and the last op
+                // that may change the state writes into C (op 0 when none
+                // may: a copy of C's storage).
+                auto keeps_state = [&](int j) {
+                    return ops[j].type == L_RUPD && P.w[ops[j].w].r == 0 && ops[j].beta == 1.0 &&
+                           op_kind[obase + j] == ROUND_CONCAT;
+                };
+                int last = nops - 1;
+                while (last > 0 && keeps_state(last)) --last;
+                int written = 0;   // ops so far that took a state slot
+                for (int j = 0; j <= last; ++j) {
                     const LOp& op = ops[j];
                     const int rnew = state_rank[obase + j];
                     if (op.type == L_RESET) {
@@ -1227,8 +1239,9 @@ void hh_multiply_roots(Context& ctx, const HMatrix& A, const HMatrix& B, double 
                         prev = -1;
                         continue;
                     }
-                    double* ou = (j + 1 == nops) ? C.U(c)
-                                                        : P0 + ((j & 1) ? slot1[c] : slot0[c]);
+                    if (j < last && keeps_state(j)) continue;
+                    double* ou = (j == last) ? C.U(c)
+                                             : P0 + ((written++ & 1) ? slot1[c] : slot0[c]);
                     double* ov = ou + (long long)Cb.m * rnew;
                     const WTask& t = P.w[op.w];
                     RoundOp r{};
@@ -1290,10 +1303,12 @@ void hh_multiply_roots(Context& ctx, const HMatrix& A, const HMatrix& B, double 
                                         Ba.n, Ba.m, Bb.m, Cb.m, 0, 0});
                     } else {
                         const WTask& t = P.w[op.w];
-                        if (t.r == 0)
-                            gops.push_back({C.D(c), nullptr, C.D(c), op.beta, 0.0, Cb.m, Cb.n, -1,
-                                            Cb.m, 0, Cb.m, 0, 0});
-                        else
+                        if (t.r == 0) {
+                            // a product of rank 0: C = beta C (nothing to do for beta = 1)
+                            if (op.beta != 1.0)
+                                gops.push_back({C.D(c), nullptr, C.D(c), op.beta, 0.0, Cb.m, Cb.n,
+                                                -1, Cb.m, 0, Cb.m, 0, 0});
+                        } else
                             gops.push_back({t.U + op.row0, t.V + op.col0, C.D(c), 1.0, op.beta, Cb.m,
                                             Cb.n, t.r, t.ldU, t.ldV, Cb.m, 0, 1});
                     }

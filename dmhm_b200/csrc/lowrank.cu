@@ -175,13 +175,72 @@ __device__ void cta_apply_q(const R* A, int m, int kk, int lda, const R* tau, RB
 }
 
 __device__ __forceinline__ int rr_pos(int i, int step, int n) {
-    return i == 0 ? 0 : 1 + (i - 1 + step) % (n - 1);
+    // (i - 1 + step) mod (n - 1) for 0 <= i - 1 + step < 2 (n - 1)
+    const int x = i - 1 + step;
+    return i == 0 ? 0 : 1 + (x >= n - 1 ? x - (n - 1) : x);
+}
+
+// One column pair (p, q) of round-robin step `step` (pair index k of n/2),
+// handled by LANES lanes of a warp (hl = this lane's index among them); all
+// lanes of the warp take part in the shuffles, live pair or not.  Rotates
+// the pair when its columns are not yet orthogonal to the threshold, with
+// the rotation's cosine and sine written without a division:
+// h = sqrt(d^2 + 4c^2), s = |d| + h, r = 1/sqrt(2hs) give cos = s r and
+// sin = sign(dc) 2|c| r (the rotation by the angle whose tangent t is the
+// smaller root of t^2 + 2 zeta t - 1 = 0, zeta = d / (2c), d = b - a), and
+// t c = sign(d) 4 c^2 h r^2 updates the squared norms.
+template <int LANES, typename R>
+__device__ __forceinline__ void jacobi_pair(R* M, int rows, int cols, R* J, R* nrm, int* flag,
+                                            int k, int hl, int step, int n, R tiny, R jt2) {
+    int p = 0, q = 1;
+    if (k < n / 2) {
+        p = rr_pos(k, step, n);
+        q = rr_pos(n - 1 - k, step, n);
+    }
+    const bool live = k < n / 2 && p < cols && q < cols;
+    if (p > q) { int t = p; p = q; q = t; }
+    R* gp = M + (long long)p * rows;
+    R* gq = M + (long long)q * rows;
+    R c = 0;
+    if (live)
+        for (int i = hl; i < rows; i += LANES) c = r_fma(gp[i], gq[i], c);
+#pragma unroll
+    for (int o = LANES / 2; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    const R a = live ? nrm[p] : R(0), b = live ? nrm[q] : R(0);
+    if (live && c != R(0) && a > tiny && b > tiny && c * c > jt2 * (a * b)) {
+        const R d = b - a;
+        const R h = r_sqrt(r_fma(d, d, R(4) * c * c));
+        const R s = r_abs(d) + h;
+        const R r = r_rsqrt(R(2) * h * s);
+        const R cs = s * r;
+        const R sn = r_copysign(R(2) * r_abs(c), d * c) * r;
+        for (int i = hl; i < rows; i += LANES) {
+            const R x = gp[i], y = gq[i];
+            gp[i] = cs * x - sn * y;
+            gq[i] = sn * x + cs * y;
+        }
+        R* jp = J + (long long)p * cols;
+        R* jq = J + (long long)q * cols;
+        for (int i = hl; i < cols; i += LANES) {
+            const R x = jp[i], y = jq[i];
+            jp[i] = cs * x - sn * y;
+            jq[i] = sn * x + cs * y;
+        }
+        if (hl == 0) {
+            const R tc = r_copysign(R(4) * c * c, d) * h * r * r;
+            nrm[p] = a - tc;
+            nrm[q] = b + tc;
+            *flag = 1;
+        }
+    }
 }
 
 // One-sided (Hestenes) Jacobi: rotates the columns of M (rows x cols) until
 // they are mutually orthogonal, accumulating the rotations in J (cols x cols,
 // J starts as I), so M_in = M_out J^T.  Round-robin ordering: cols/2
-// disjoint pairs per step, one warp per pair.  Bounded number of sweeps.
+// disjoint pairs per step, all pairs of a step at once (a half-warp per
+// pair; up to 16 columns, all pairs in warp 0, a quarter-warp each, which
+// spares the steps the CTA barrier).  Bounded number of sweeps.
 // Pairs with a column below rounding level (squared norm under 1e-32 times
 // the squared Frobenius norm of M) are left alone: rotating noise against
 // noise never settles, and such columns carry no singular value above
@@ -202,10 +261,9 @@ __device__ void cta_jacobi(R* M, int rows, int cols, R* J, int* flag, R* red, R*
     __syncthreads();
     if (cols < 2) return;
     const int n = cols + (cols & 1);
-    // one half-warp (16 lanes) per pair: all cols/2 pairs of a step at once
-    // for up to 32 columns.  Squared column norms are kept in nrm (exact at
-    // the start of every sweep, then updated by the rotations), so a pair
-    // reduces only its inner product.
+    // Squared column norms are kept in nrm (exact at the start of every
+    // sweep, then updated by the rotations), so a pair reduces only its
+    // inner product.
     const int hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
     constexpr R jt2 = Prec<R>::jtol * Prec<R>::jtol;
     for (int sweep = 0; sweep < kJacobiSweeps; ++sweep) {
@@ -249,54 +307,26 @@ __device__ void cta_jacobi(R* M, int rows, int cols, R* J, int* flag, R* red, R*
             if (threadIdx.x == 0) *flag = 0;
             __syncthreads();
         }
-        for (int step = 0; step < n - 1; ++step) {
-            // warp-uniform trip count: both half-warps of a warp iterate
-            // together (their shuffles span the whole warp)
-            for (int kb = 2 * warp; kb < n / 2; kb += 2 * kW) {
-                const int k = kb + (hw & 1);
-                int p = 0, q = 1;
-                if (k < n / 2) {
-                    p = rr_pos(k, step, n);
-                    q = rr_pos(n - 1 - k, step, n);
-                }
-                const bool live = k < n / 2 && p < cols && q < cols;
-                if (p > q) { int t = p; p = q; q = t; }
-                R* gp = M + (long long)p * rows;
-                R* gq = M + (long long)q * rows;
-                R c = 0;
-                if (live)
-                    for (int i = hl; i < rows; i += 16) c = r_fma(gp[i], gq[i], c);
-#pragma unroll
-                for (int o = 8; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-                const R a = live ? nrm[p] : R(0), b = live ? nrm[q] : R(0);
-                if (live && c != R(0) && a > tiny && b > tiny && c * c > jt2 * (a * b)) {
-                    // t = tan of the rotation angle, the smaller root of
-                    // t^2 + 2 zeta t - 1 = 0 with zeta = (b - a) / (2c),
-                    // written as 2|c| / (|b - a| + sqrt((b - a)^2 + 4c^2))
-                    const R d = b - a;
-                    const R t = r_copysign(R(2) * r_abs(c), d * c) /
-                                (r_abs(d) + r_sqrt(r_fma(d, d, R(4) * c * c)));
-                    const R cs = r_rsqrt(r_fma(t, t, R(1))), sn = cs * t;
-                    for (int i = hl; i < rows; i += 16) {
-                        const R x = gp[i], y = gq[i];
-                        gp[i] = cs * x - sn * y;
-                        gq[i] = sn * x + cs * y;
-                    }
-                    R* jp = J + (long long)p * cols;
-                    R* jq = J + (long long)q * cols;
-                    for (int i = hl; i < cols; i += 16) {
-                        const R x = jp[i], y = jq[i];
-                        jp[i] = cs * x - sn * y;
-                        jq[i] = sn * x + cs * y;
-                    }
-                    if (hl == 0) {
-                        nrm[p] = r_fma(-t, c, a);
-                        nrm[q] = r_fma(t, c, b);
-                        *flag = 1;
-                    }
+        if (n <= 16) {
+            // at most 8 pairs a step: warp 0 alone, 4 lanes per pair, so the
+            // steps need only warp-level synchronization
+            if (warp == 0) {
+                for (int step = 0; step < n - 1; ++step) {
+                    jacobi_pair<4>(M, rows, cols, J, nrm, flag, lane >> 2, lane & 3, step, n, tiny,
+                                   jt2);
+                    __syncwarp();
                 }
             }
             __syncthreads();
+        } else {
+            for (int step = 0; step < n - 1; ++step) {
+                // warp-uniform trip count: both half-warps of a warp iterate
+                // together (their shuffles span the whole warp)
+                for (int kb = 2 * warp; kb < n / 2; kb += 2 * kW)
+                    jacobi_pair<16>(M, rows, cols, J, nrm, flag, kb + (hw & 1), hl, step, n, tiny,
+                                    jt2);
+                __syncthreads();
+            }
         }
         const int again = *flag;
         __syncthreads();
@@ -313,7 +343,9 @@ __device__ void cta_order_columns(const R* M, int rows, int cols, R* norms, int*
         R s = 0;
         for (int i = lane; i < rows; i += 32) s = r_fma(g[i], g[i], s);
         s = warp_sum(s);
-        if (lane == 0) norms[c] = s;
+        // a NaN norm (non-finite block data, which the numerical flag
+        // reports) sorts last, so that order stays a permutation
+        if (lane == 0) norms[c] = s == s ? s : R(-1);
     }
     __syncthreads();
     for (int j = threadIdx.x; j < cols; j += kT) {

@@ -33,6 +33,7 @@ constexpr int kT = 256;
 constexpr int kW = kT / 32;
 constexpr int kMaxK = 128;         // largest stacked rank handled
 constexpr long long kSmemBytes = 65536;   // M and J up to 64 x 64 FP64
+constexpr int kQB = 4;           // columns a warp updates together when applying reflectors
 constexpr int kJacobiSweeps = 40;  // bounded; converges in ~6-12
 
 // Per-precision constants: Jacobi's orthogonality threshold (relative to the
@@ -147,30 +148,57 @@ __device__ void cta_qr(R* A, int m, int n, int ld, R* tau, R* red) {
 // B := Q B with Q = H_0 H_1 ... H_{kk-1} from cta_qr (B is m x p;
 // arithmetic in R, B may be stored in another type).  Column c of B is
 // updated by warp c % kW through all reflectors, so no barrier is needed
-// between them.
-template <typename R, typename RB>
-__device__ void cta_apply_q(const R* A, int m, int kk, int lda, const R* tau, RB* B, int p,
-                            int ldb) {
+// between them; a warp with several columns takes NB of them at a time and
+// reduces their inner products together (independent shuffle chains
+// overlap).  Each column sees the same operations in the same order either
+// way.
+template <int NB, typename R, typename RB>
+__device__ __forceinline__ void warp_apply_q(const R* A, int m, int kk, int lda, const R* tau,
+                                             RB* B, int p, int ldb) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int c = warp; c < p; c += kW) {
-        RB* bcol = B + (long long)c * ldb;
+    for (int c = warp; c < p; c += NB * kW) {
         for (int j = kk - 1; j >= 0; --j) {
             const R t = tau[j];
             if (t == R(0)) continue;
             const R* v = A + j + (long long)j * lda;
             const int len = m - j;
-            RB* bc = bcol + j;
-            const R b0 = (R)bc[0];
-            R w = 0;
-            for (int i = 1 + lane; i < len; i += 32) w += v[i] * (R)bc[i];
-            w = warp_sum(w) + b0;
-            const R tw = t * w;
+            R w[NB], b0[NB];
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                const int cb = c + b * kW;
+                w[b] = 0;
+                b0[b] = 0;
+                if (cb < p) {
+                    const RB* bc = B + (long long)cb * ldb + j;
+                    b0[b] = (R)bc[0];
+                    for (int i = 1 + lane; i < len; i += 32) w[b] += v[i] * (R)bc[i];
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                for (int b = 0; b < NB; ++b) w[b] += __shfl_xor_sync(0xffffffffu, w[b], o);
             __syncwarp();
-            if (lane == 0) bc[0] = (RB)(b0 - tw);
-            for (int i = 1 + lane; i < len; i += 32) bc[i] = (RB)((R)bc[i] - tw * v[i]);
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                const int cb = c + b * kW;
+                if (cb < p) {
+                    RB* bc = B + (long long)cb * ldb + j;
+                    const R tw = t * (w[b] + b0[b]);
+                    if (lane == 0) bc[0] = (RB)(b0[b] - tw);
+                    for (int i = 1 + lane; i < len; i += 32) bc[i] = (RB)((R)bc[i] - tw * v[i]);
+                }
+            }
             __syncwarp();
         }
     }
+}
+
+template <typename R, typename RB>
+__device__ void cta_apply_q(const R* A, int m, int kk, int lda, const R* tau, RB* B, int p,
+                            int ldb) {
+    if (p > kW) warp_apply_q<kQB>(A, m, kk, lda, tau, B, p, ldb);
+    else warp_apply_q<1>(A, m, kk, lda, tau, B, p, ldb);
     __syncthreads();
 }
 
@@ -475,22 +503,54 @@ __device__ void do_round(const RoundOp& op_in, R* dyn, long long smem_elems, Rou
     if (!dense) cta_qr(Vcat, n, k, n, tauV, red);
 
     // ---- core M = R_u R_v^T (ku x kv) -------------------------------------
-    for_each_entry(ku, kv, [&](int i, int l) {
-        R v = 0;
-        if (ortho) {
-            v = (i >= l) ? Vcat[l + (long long)i * n] : R(0);     // R_v^T
-        } else if (dense) {
-            if (skip_u) v = Ucat[i + (long long)l * m];             // the block itself
-            else v = (l >= i) ? Ucat[i + (long long)l * m] : R(0);  // R_u (ku x n)
-        } else if (skip_u) {
-            for (int p = l; p < k; ++p)                              // U_cat R_v^T
-                v = r_fma(Ucat[i + (long long)p * m], Vcat[l + (long long)p * n], v);
-        } else {
-            for (int p = max(i, l); p < k; ++p)
-                v = r_fma(Ucat[i + (long long)p * m], Vcat[l + (long long)p * n], v);
+    if (ortho || dense) {
+        for_each_entry(ku, kv, [&](int i, int l) {
+            R v;
+            if (ortho) v = (i >= l) ? Vcat[l + (long long)i * n] : R(0);  // R_v^T
+            else if (skip_u) v = Ucat[i + (long long)l * m];                // the block itself
+            else v = (l >= i) ? Ucat[i + (long long)l * m] : R(0);          // R_u (ku x n)
+            M[i + (long long)l * ku] = v;
+        });
+    } else {
+        // U_cat R_v^T (skip_u) or R_u R_v^T, entry (i, l) summed over p from
+        // l (or max(i, l)) to k - 1; 2 x 2 entries a thread, so each loaded
+        // factor entry serves several products.  The entries of a tile start
+        // at the tile's smallest p, the factors' entries outside their
+        // triangles entering as exact zeros, which leaves every sum as it
+        // would be alone (0 + 0 x = 0 until its own first term).
+        constexpr int TR = 2, TC = 2;
+        const int tr = (ku + TR - 1) / TR, tc = (kv + TC - 1) / TC;
+        for (int tile = threadIdx.x; tile < tr * tc; tile += kT) {
+            const int i0 = TR * (tile % tr), l0 = TC * (tile / tr);
+            R acc[TR][TC];
+#pragma unroll
+            for (int r = 0; r < TR; ++r)
+#pragma unroll
+                for (int c = 0; c < TC; ++c) acc[r][c] = R(0);
+            for (int p = skip_u ? l0 : max(i0, l0); p < k; ++p) {
+                R a[TR], b[TC];
+#pragma unroll
+                for (int r = 0; r < TR; ++r) {
+                    const int i = i0 + r;
+                    a[r] = (i < ku && (skip_u || p >= i)) ? Ucat[i + (long long)p * m] : R(0);
+                }
+#pragma unroll
+                for (int c = 0; c < TC; ++c) {
+                    const int l = l0 + c;
+                    b[c] = (l < kv && p >= l) ? Vcat[l + (long long)p * n] : R(0);
+                }
+#pragma unroll
+                for (int r = 0; r < TR; ++r)
+#pragma unroll
+                    for (int c = 0; c < TC; ++c) acc[r][c] = r_fma(a[r], b[c], acc[r][c]);
+            }
+#pragma unroll
+            for (int r = 0; r < TR; ++r)
+#pragma unroll
+                for (int c = 0; c < TC; ++c)
+                    if (i0 + r < ku && l0 + c < kv) M[i0 + r + (long long)(l0 + c) * ku] = acc[r][c];
         }
-        M[i + (long long)l * ku] = v;
-    });
+    }
     __syncthreads();
 
     // ---- SVD of the core ---------------------------------------------------

@@ -91,15 +91,17 @@ struct Context {
     // (made on first use, freed with the context).
     double* pinned_scalar();
     double* pinned = nullptr;
-    // Device word set by kernels whose bounded waits gave up (zero = fine).
+    // Device word set by kernels whose bounded waits gave up (zero = fine);
+    // read and cleared by check_numerical().
     int* error_word();
     DeviceBuffer<int> errword;
     // Device word set by a low-rank rounding whose core held NaN or Inf
     // (zero = fine); read and cleared by check_numerical().
     int* numerical_word();
     DeviceBuffer<int> numword;
-    // Synchronizes the stream and throws HM_ERR_NUMERICAL (clearing the
-    // word) when a rounding since the last check met a non-finite value.
+    // Synchronizes the stream and throws HM_ERR_TIMEOUT when a bounded wait
+    // gave up, HM_ERR_NUMERICAL when a rounding met a non-finite value, since
+    // the last check (clearing the word).
     void check_numerical();
 };
 

@@ -1274,6 +1274,14 @@ int* Context::numerical_word() {
 
 void Context::check_numerical() {
     HMB_CUDA(cudaStreamSynchronize(stream));
+    if (errword.get()) {
+        int e = 0;
+        HMB_CUDA(cudaMemcpy(&e, errword.get(), sizeof(int), cudaMemcpyDeviceToHost));
+        if (e) {
+            HMB_CUDA(cudaMemset(errword.get(), 0, sizeof(int)));
+            throw Error(HM_ERR_TIMEOUT, "a bounded device wait gave up (no progress)");
+        }
+    }
     if (!numword.get()) return;
     int h = 0;
     HMB_CUDA(cudaMemcpy(&h, numword.get(), sizeof(int), cudaMemcpyDeviceToHost));

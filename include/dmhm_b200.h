@@ -57,7 +57,8 @@ HM_API int hm_version(void);
 HM_API int hm_context_create(int device, void* cuda_stream, hm_context* out);
 HM_API int hm_context_destroy(hm_context ctx);
 /* Waits for the context's stream; HM_ERR_NUMERICAL when a low-rank rounding
-   since the last synchronization met NaN or Inf (non-finite block data). */
+   since the last synchronization met NaN or Inf (non-finite block data),
+   HM_ERR_TIMEOUT when a bounded device wait gave up. */
 HM_API int hm_context_synchronize(hm_context ctx);
 /* SetOversample / Oversample (src/core/global.cpp:155-159). */
 HM_API int hm_set_oversample(hm_context ctx, int oversample);

@@ -32,9 +32,7 @@ namespace {
 constexpr int kT = 256;
 constexpr int kW = kT / 32;
 constexpr int kMaxK = 128;         // largest stacked rank handled
-// dynamic shared memory a CTA: M and J up to 64 x 64 FP64, the stacked
-// factors too where they fit beside them (more would cost CTAs per SM)
-constexpr long long kSmemBytes = 65536;
+constexpr long long kSmemBytes = 65536;   // M and J up to 64 x 64 FP64
 constexpr int kQB = 4;           // columns a warp updates together when applying reflectors
 constexpr int kJacobiSweeps = 40;  // bounded; converges in ~6-12
 
@@ -268,10 +266,9 @@ __device__ __forceinline__ void jacobi_pair(R* M, int rows, int cols, R* J, R* n
 // One-sided (Hestenes) Jacobi: rotates the columns of M (rows x cols) until
 // they are mutually orthogonal, accumulating the rotations in J (cols x cols,
 // J starts as I), so M_in = M_out J^T.  Round-robin ordering: cols/2
-// disjoint pairs per step, all pairs of a step at once where they fit (up to
-// 16 columns: all pairs in warp 0, 4 lanes each, which spares the steps the
-// CTA barrier; up to 64: 8 lanes a pair over the CTA; beyond: a half-warp a
-// pair, in rounds).  Bounded number of sweeps.
+// disjoint pairs per step, all pairs of a step at once (a half-warp per
+// pair; up to 16 columns, all pairs in warp 0, a quarter-warp each, which
+// spares the steps the CTA barrier).  Bounded number of sweeps.
 // Pairs with a column below rounding level (squared norm under 1e-32 times
 // the squared Frobenius norm of M) are left alone: rotating noise against
 // noise never settles, and such columns carry no singular value above
@@ -349,14 +346,6 @@ __device__ void cta_jacobi(R* M, int rows, int cols, R* J, int* flag, R* red, R*
                 }
             }
             __syncthreads();
-        } else if (n <= 4 * kW * 2) {
-            // at most 32 pairs a step: 8 lanes per pair, every pair of the
-            // step at once
-            for (int step = 0; step < n - 1; ++step) {
-                jacobi_pair<8>(M, rows, cols, J, nrm, flag, 4 * warp + (lane >> 3), lane & 7, step,
-                               n, tiny, jt2);
-                __syncthreads();
-            }
         } else {
             for (int step = 0; step < n - 1; ++step) {
                 // warp-uniform trip count: both half-warps of a warp iterate
@@ -455,16 +444,9 @@ __device__ void do_round(const RoundOp& op_in, R* dyn, long long smem_elems, Rou
     // dense block), and its rotated columns are the output U directly.
     const bool skip_u = !ortho && m <= k;
     // The core and the rotations live in shared memory when they fit in
-    // `smem_elems`, and after them the stacked factors when they fit too (V's
-    // stack first: every kind but DENSE factors and applies it); otherwise
-    // the (L1-cached) work area holds them.
+    // `smem_elems`; the stacked factors in the (L1-cached) work area.
     const long long need_mj = (long long)ku * kv + (long long)kv * kv;
     const bool mj_smem = need_mj <= smem_elems;
-    const long long need_v = dense ? 0 : (long long)n * k;
-    const long long need_u = ortho ? 0 : (long long)m * k;
-    const bool v_smem = mj_smem && need_v > 0 && need_mj + need_v <= smem_elems;
-    const bool u_smem =
-        mj_smem && need_u > 0 && need_mj + (v_smem ? need_v : 0) + need_u <= smem_elems;
     R* w = reinterpret_cast<R*>(op.work);
     R* Ucat = w;
     if (!ortho) w += (long long)m * k;
@@ -474,8 +456,6 @@ __device__ void do_round(const RoundOp& op_in, R* dyn, long long smem_elems, Rou
     w += k;
     R* tauV = w;
     w += k;
-    if (v_smem) Vcat = dyn + need_mj;
-    if (u_smem) Ucat = dyn + need_mj + (v_smem ? need_v : 0);
     R* M;
     R* J;
     if (mj_smem) {
@@ -714,9 +694,8 @@ void upload_round_list(Context& ctx, const std::vector<RoundOp>& ops,
     // The core and the rotations of an op live in shared memory when they
     // fit the launch's size, otherwise in the (L1-cached) global work area;
     // the size is the largest need of the non-dense ops (dense compressions
-    // with larger cores take the global path), their stacked factors
-    // included, up to kSmemBytes, so that more CTAs share an SM.
-    long long need_max = 0, full_max = 0;
+    // with larger cores take the global path), so that more CTAs share an SM.
+    long long need_max = 0;
     for (const RoundOp& op : ops) {
         if (op.kind == ROUND_SET || op.kind == ROUND_CONCAT) continue;
         const bool dense = op.kind == ROUND_DENSE;
@@ -727,13 +706,9 @@ void upload_round_list(Context& ctx, const std::vector<RoundOp>& ops,
         const long long kv = dense ? op.n : std::min<long long>(op.n, k);
         const long long need = ku * kv + kv * kv;
         if (!dense || need <= 3072) need_max = std::max(need_max, need);
-        if (!dense)
-            full_max = std::max(full_max, need + op.n * k +
-                                              (op.kind == ROUND_ORTHO ? 0 : op.m * k));
     }
-    // the stacks of the non-dense ops too where they fit the same budget
-    out.smem_double = std::min<long long>(std::max(need_max, full_max), kSmemBytes / 8);
-    out.smem_float = std::min<long long>(std::max(need_max, full_max), kSmemBytes / 4);
+    out.smem_double = std::min<long long>(need_max, kSmemBytes / 8);
+    out.smem_float = std::min<long long>(need_max, kSmemBytes / 4);
     out.nw = (int)begin.size() - 1;
     std::vector<int> workers(out.nw);
     for (int w = 0; w < out.nw; ++w) workers[w] = w;

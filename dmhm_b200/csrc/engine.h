@@ -19,7 +19,9 @@ namespace hmb {
 // Per-block table entry the kernels read (32 bytes).
 struct DevBlock {
     int kind, m, n, rank;
-    int row_off, col_off, pad0, pad1;
+    int row_off, col_off;
+    int rank_before;   // sum of the low-rank ranks of the blocks before this one
+    int pad1;
     long long off;   // element offset of U (low-rank, V follows at off+m*rank) or D
 };
 

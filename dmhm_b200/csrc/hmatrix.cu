@@ -4,6 +4,7 @@
 // (n x r), column-major with leading dimensions m and n (A_b = U V^T,
 // include/dmhm/core/low_rank.hpp:22-38); dense leaves keep D (m x n).  Blocks
 // are laid out in depth-first order so that a subtree's data is contiguous.
+#include <climits>
 #include <algorithm>
 
 #include <deque>
@@ -38,6 +39,7 @@ void HMatrix::layout() {
 void HMatrix::upload_table() {
     const Structure& St = *S;
     std::vector<DevBlock> t(St.blocks.size());
+    long long before = 0;
     for (size_t b = 0; b < St.blocks.size(); ++b) {
         const Block& B = St.blocks[b];
         DevBlock d{};
@@ -47,7 +49,9 @@ void HMatrix::upload_table() {
         d.rank = B.kind == KIND_LOWRANK ? rank[b] : 0;
         d.row_off = B.row_off;
         d.col_off = B.col_off;
+        d.rank_before = (int)std::min<long long>(before, INT_MAX);
         d.off = off[b];
+        before += d.rank;
         t[b] = d;
     }
     table.upload(t, ctx->stream);

@@ -5,17 +5,17 @@
 // time-critical loops where an allocator call may block or fail.
 // hm_multiply_vector_noalloc serves them.  It computes the same product as
 // hm_multiply_dense with one right-hand side, but keeps its intermediate
-// values (the per-block inner products V^T x, and a per-block offset table)
-// in one statically allocated device array of this library instead of
-// allocating per call.  Dense leaves and low-rank blocks are processed one
+// values (the per-block inner products V^T x, placed by the rank offsets
+// that the matrix's block table carries) in one statically allocated
+// device array of this library instead of allocating per call.  Dense leaves and low-rank blocks are processed one
 // CTA per block, and each block adds its contribution to the output with
 // atomic additions, so the summation order may differ from
 // hm_multiply_dense in the last bits.
 //
 // The array holds kNoAllocScratchDoubles doubles (4 MiB); every GPU that
 // loads the library holds it until the process exits.  A matrix needs
-// (number of blocks + sum of the low-rank ranks) entries; larger matrices
-// are rejected with HM_ERR_UNSUPPORTED.  All calls share the array and the
+// (sum of the low-rank ranks) entries; larger matrices are rejected with
+// HM_ERR_UNSUPPORTED.  All calls share the array and the
 // array keeps whatever the last call left in it, so calls that overlap on
 // the GPU (on different streams, or from different host threads without
 // ordering) race on it and must not be issued.
@@ -50,33 +50,6 @@ double* scratch_address(int device) {
     return addr[device];
 }
 
-// scratch[b] = exclusive prefix sum of the low-rank ranks over blocks < b
-// (stored as integer bit patterns); one CTA.
-__global__ void noalloc_prefix_kernel(const DevBlock* __restrict__ table, int nblocks,
-                                      double* scratch) {
-    __shared__ long long carry;
-    __shared__ long long part[kT];
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    for (int base = 0; base < nblocks; base += kT) {
-        const int b = base + threadIdx.x;
-        long long v = 0;
-        if (b < nblocks && table[b].kind == KIND_LOWRANK) v = table[b].rank;
-        part[threadIdx.x] = v;
-        __syncthreads();
-        for (int o = 1; o < kT; o <<= 1) {   // inclusive scan
-            long long add = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
-            __syncthreads();
-            part[threadIdx.x] += add;
-            __syncthreads();
-        }
-        if (b < nblocks) scratch[b] = __longlong_as_double(carry + part[threadIdx.x] - v);
-        __syncthreads();
-        if (threadIdx.x == kT - 1) carry += part[kT - 1];
-        __syncthreads();
-    }
-}
-
 __global__ void noalloc_scale_kernel(double* y, int n, double beta) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         y[i] = beta == 0.0 ? 0.0 : beta * y[i];
@@ -87,11 +60,11 @@ __global__ void noalloc_inner_kernel(const DevBlock* __restrict__ table, int nbl
                                      const double* __restrict__ data,
                                      const double* __restrict__ x, double* scratch, int trans) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double* T = scratch + nblocks;
+    double* T = scratch;
     for (int b = blockIdx.x; b < nblocks; b += gridDim.x) {
         const DevBlock B = table[b];
         if (B.kind != KIND_LOWRANK || B.rank == 0 || B.m == 0 || B.n == 0) continue;
-        const long long t0 = __double_as_longlong(scratch[b]);
+        const long long t0 = B.rank_before;
         const int nin = trans ? B.m : B.n;
         const double* W = data + B.off + (trans ? 0LL : (long long)B.m * B.rank);
         const double* xs = x + (trans ? B.row_off : B.col_off);
@@ -111,7 +84,7 @@ __global__ void noalloc_outer_kernel(const DevBlock* __restrict__ table, int nbl
                                      const double* __restrict__ data,
                                      const double* __restrict__ x, const double* scratch,
                                      double* y, double alpha, int trans) {
-    const double* T = scratch + nblocks;
+    const double* T = scratch;
     for (int b = blockIdx.x; b < nblocks; b += gridDim.x) {
         const DevBlock B = table[b];
         if (B.kind == KIND_NODE || B.m == 0 || B.n == 0) continue;
@@ -121,16 +94,26 @@ __global__ void noalloc_outer_kernel(const DevBlock* __restrict__ table, int nbl
             const double* D = data + B.off;
             const double* xs = x + (trans ? B.row_off : B.col_off);
             const int nin = trans ? B.m : B.n;
-            for (int i = threadIdx.x; i < nout; i += kT) {
-                double s = 0.0;
-                if (!trans)
+            if (!trans) {
+                // row i of D: neighbouring threads read neighbouring rows
+                for (int i = threadIdx.x; i < nout; i += kT) {
+                    double s = 0.0;
                     for (int j = 0; j < nin; ++j) s = fma(D[i + (long long)j * B.m], xs[j], s);
-                else
-                    for (int j = 0; j < nin; ++j) s = fma(D[j + (long long)i * B.m], xs[j], s);
-                atomicAdd(ys + i, alpha * s);
+                    atomicAdd(ys + i, alpha * s);
+                }
+            } else {
+                // column i of D: one warp, lanes along the column
+                const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+                for (int i = warp; i < nout; i += kT / 32) {
+                    const double* col = D + (long long)i * B.m;
+                    double s = 0.0;
+                    for (int j = lane; j < nin; j += 32) s = fma(col[j], xs[j], s);
+                    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+                    if (lane == 0) atomicAdd(ys + i, alpha * s);
+                }
             }
         } else if (B.rank > 0) {
-            const long long t0 = __double_as_longlong(scratch[b]);
+            const long long t0 = B.rank_before;
             const double* W = data + B.off + (trans ? (long long)B.m * B.rank : 0LL);
             for (int i = threadIdx.x; i < nout; i += kT) {
                 double s = 0.0;
@@ -151,10 +134,10 @@ void multiply_vector_noalloc(HMatrix& H, int transpose, double alpha, const doub
     long long rank_sum = 0;
     for (int b : S.leaves)
         if (S.blocks[b].kind == KIND_LOWRANK) rank_sum += H.rank[b];
-    const long long need = (long long)nblocks + rank_sum;
+    const long long need = rank_sum;
     HMB_REQUIRE(need <= kNoAllocScratchDoubles, HM_ERR_UNSUPPORTED,
                 "hm_multiply_vector_noalloc: the matrix needs " + std::to_string(need) +
-                    " scratch entries (blocks + low-rank ranks); the static scratch holds " +
+                    " scratch entries (the sum of its low-rank ranks); the static scratch holds " +
                     std::to_string(kNoAllocScratchDoubles));
     HMB_REQUIRE(x != nullptr && y != nullptr, HM_ERR_ARGUMENT, "NULL vector");
     HMB_CUDA(cudaSetDevice(ctx.device));
@@ -162,8 +145,7 @@ void multiply_vector_noalloc(HMatrix& H, int transpose, double alpha, const doub
     const int n_out = transpose ? H.width() : H.height();
     const int grid = std::max(1, std::min(nblocks, 8 * ctx.num_sms));
     cudaStream_t st = ctx.stream;
-    g_launches.fetch_add(4, std::memory_order_relaxed);
-    noalloc_prefix_kernel<<<1, kT, 0, st>>>(H.table.get(), nblocks, scratch);
+    g_launches.fetch_add(3, std::memory_order_relaxed);
     noalloc_scale_kernel<<<std::max(1, std::min(ceil_div(n_out, kT), 4 * ctx.num_sms)), kT, 0,
                            st>>>(y, n_out, beta);
     noalloc_inner_kernel<<<grid, kT, 0, st>>>(H.table.get(), nblocks, H.data.get(), x, scratch,

@@ -304,7 +304,7 @@ HM_API int hm_add_constant_to_diagonal(hm_matrix h, double alpha);
  * memory manager already holds the GPU's memory, or a time-critical loop must
  * not call the allocator).  Intermediates live in one static 4 MiB device
  * array of the library, so the matrix may need at most 524288 entries of
- * (blocks + sum of low-rank ranks); larger matrices return
+ * (the sum of its low-rank ranks); larger matrices return
  * HM_ERR_UNSUPPORTED.  The first call on a device looks up the array's
  * address; make that first call before any stream capture.  All calls share
  * the array: calls that overlap on the GPU race and must not be issued.

@@ -91,6 +91,8 @@ SIGNATURES = {
     "hm_multiply_dense_tf32": [_P, _D, _P, _I, _D, _P, _I, _I],
     "hm_set_tf32_kernel": [_P, _I],
     "hm_tf32_kernel_choice": [_P, _P, _I, _I, _PI],
+    "hm_set_fp64_split": [_P, _I],
+    "hm_fp64_split_choice": [_P, _P, _I, _I, _PI],
     "hm_rank_feature_count": [],
     "hm_rank_param_count": [],
     "hm_rank_model_create": [_P, _U64, C.POINTER(_P)],

@@ -319,6 +319,28 @@ int hm_tf32_kernel_choice(hm_matrix h, const double* B, int ldb, int nrhs, int* 
     });
 }
 
+int hm_set_fp64_split(hm_context ctx, int which) {
+    return guarded([&] {
+        HMB_REQUIRE(ctx, HM_ERR_ARGUMENT, "ctx is NULL");
+        HMB_REQUIRE(which >= 0 && which <= 2, HM_ERR_ARGUMENT, "which must be 0, 1 or 2");
+        ctx->c.fp64_split = which;
+    });
+}
+
+int hm_fp64_split_choice(hm_matrix h, const double* B, int ldb, int nrhs, int* which) {
+    return guarded([&] {
+        HMB_REQUIRE(h && which && (nrhs == 0 || B), HM_ERR_ARGUMENT, "NULL argument");
+        owner_of(h);
+        HMB_REQUIRE(h->h.S != nullptr, HM_ERR_ARGUMENT, "empty H-matrix");
+        HMB_REQUIRE(nrhs > 0 && ldb >= std::max(1, h->h.width()), HM_ERR_ARGUMENT,
+                    "bad right-hand sides");
+        // the whole product, as hm_multiply_dense runs it (a tuning run
+        // writes into scratch, so no output is needed)
+        MatJob J{&h->h, 0, false, 1.0, 0.0, B, ldb, nullptr, std::max(1, h->h.height()), nrhs};
+        *which = fp64_split_for(*h->h.ctx, {J});
+    });
+}
+
 int hm_get_compression_tolerance(hm_context ctx, double* tol) {
     return guarded([&] {
         HMB_REQUIRE(ctx && tol, HM_ERR_ARGUMENT, "NULL argument");

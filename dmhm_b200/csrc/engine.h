@@ -84,6 +84,12 @@ struct Context {
     // bucket), 1 tcgen05 (at most 64 columns, ranks <= 256), 2 mma.sync.
     int tf32_kernel = 0;
     std::map<std::pair<uint64_t, int>, int> tf32_tuned;
+    // FP64 products of 9 to 16 columns: 0 autotuned per (layout of the first
+    // job's matrix, job count, column count), 1 one pass of the tensor-core
+    // 64 x 64 tiles, 2 passes of at most 8 columns through the streaming
+    // kernels.
+    int fp64_split = 0;
+    std::map<std::tuple<uint64_t, int, int>, int> fp64_split_tuned;
     // Grow-only device scratch reused by consecutive H*H products on this
     // context's stream (W arena, sampling arena, state slots, rounding work):
     // a product's kernels finish before the next product's start.
@@ -211,6 +217,9 @@ std::shared_ptr<JobTemplate> get_template(Context& ctx, const HMatrix& H, int ro
 // more than 8 columns multiply on the TF32 tensor cores (FP32 copies of the
 // blocks and inputs, FP32 accumulation, FP64 output).
 void run_jobs(Context& ctx, const std::vector<MatJob>& jobs, bool tf32 = false);
+// How run_jobs runs an FP64 job list (tuning it if need be): 1 one pass of
+// the tensor-core tiles, 2 passes of at most 8 columns (matmul.cu).
+int fp64_split_for(Context& ctx, const std::vector<MatJob>& jobs);
 // One-vector product of one job streamed block by block (matvec.cu); false
 // when the matrix does not fit that kernel (the caller uses run_jobs' lists).
 bool multiply_vector_streamed(Context& ctx, const MatJob& job);

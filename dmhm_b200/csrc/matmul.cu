@@ -1315,7 +1315,102 @@ int* Context::zeroed_counters(long long n) {
     return counters.get();
 }
 
+namespace {
+
+void run_jobs_direct(Context& ctx, const std::vector<MatJob>& jobs, bool tf32);
+
+// The jobs in passes of at most 8 columns (the streaming kernels).
+void run_jobs_split(Context& ctx, const std::vector<MatJob>& jobs, int kmax) {
+    for (int c0 = 0; c0 < kmax; c0 += 8) {
+        std::vector<MatJob> pass(jobs);
+        for (MatJob& J : pass) {
+            J.k = std::max(0, std::min(8, J.k - c0));
+            if (J.k == 0) continue;
+            J.in += (long long)c0 * J.ldin;
+            J.out += (long long)c0 * J.ldout;
+        }
+        run_jobs_direct(ctx, pass, false);
+    }
+}
+
+// Wide pass (1) or 8-column passes (2) for an FP64 job list of 9 to 16
+// columns.  Which is faster depends on the operator: on the 256^2 operator
+// (maxRank 32) two streaming passes are 27 % faster at 9 columns and 7 % at
+// 12; on 32^2 the tensor-core pass is faster from 9 columns.  Timed once per
+// (layout, job count, column count) on copies of the jobs writing into
+// scratch with beta = 0 (one untimed and three timed runs of each).
+int fp64_split_choice(Context& ctx, const std::vector<MatJob>& jobs, int kmax) {
+    if (ctx.fp64_split != 0) return ctx.fp64_split;
+    get_template(ctx, *jobs[0].H, jobs[0].root, jobs[0].trans, 64);   // makes the layout group
+    const auto key = std::make_tuple(jobs[0].H->group->hash, (int)jobs.size(), kmax);
+    auto f = ctx.fp64_split_tuned.find(key);
+    if (f != ctx.fp64_split_tuned.end()) return f->second;
+    HostScope hs(ctx, "fp64_split_autotune");
+    std::vector<MatJob> trial(jobs);
+    long long total = 0;
+    std::vector<long long> off(jobs.size());
+    for (size_t j = 0; j < jobs.size(); ++j) {
+        const Block& R = jobs[j].H->S->blocks[jobs[j].root];
+        const int nout = jobs[j].trans ? R.n : R.m;
+        off[j] = total;
+        total += (long long)std::max(nout, 1) * std::max(jobs[j].k, 0);
+    }
+    DeviceBuffer<double> scratch;
+    scratch.allocate((size_t)std::max<long long>(total, 1), ctx.stream);
+    for (size_t j = 0; j < jobs.size(); ++j) {
+        const Block& R = jobs[j].H->S->blocks[jobs[j].root];
+        trial[j].out = scratch.get() + off[j];
+        trial[j].ldout = std::max(jobs[j].trans ? R.n : R.m, 1);
+        trial[j].beta = 0.0;
+    }
+    cudaEvent_t e0, e1;
+    HMB_CUDA(cudaEventCreate(&e0));
+    HMB_CUDA(cudaEventCreate(&e1));
+    float ms[2] = {0.0f, 0.0f};
+    for (int which = 1; which <= 2; ++which) {
+        auto run = [&] {
+            if (which == 1) run_jobs_direct(ctx, trial, false);
+            else run_jobs_split(ctx, trial, kmax);
+        };
+        run();
+        HMB_CUDA(cudaEventRecord(e0, ctx.stream));
+        for (int r = 0; r < 3; ++r) run();
+        HMB_CUDA(cudaEventRecord(e1, ctx.stream));
+        HMB_CUDA(cudaEventSynchronize(e1));
+        HMB_CUDA(cudaEventElapsedTime(&ms[which - 1], e0, e1));
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const int best = ms[1] < ms[0] ? 2 : 1;
+    ctx.fp64_split_tuned[key] = best;
+    return best;
+}
+
+}  // namespace
+
+int fp64_split_for(Context& ctx, const std::vector<MatJob>& jobs) {
+    int kmax = 0;
+    for (const MatJob& J : jobs) kmax = std::max(kmax, J.k);
+    if (jobs.empty() || kmax <= 8 || kmax > 16) return kmax > 8 ? 1 : 2;
+    return fp64_split_choice(ctx, jobs, kmax);
+}
+
 void run_jobs(Context& ctx, const std::vector<MatJob>& jobs, bool tf32) {
+    if (jobs.empty()) return;
+    if (!tf32) {
+        int kmax = 0;
+        for (const MatJob& J : jobs) kmax = std::max(kmax, J.k);
+        if (kmax > 8 && kmax <= 16 && fp64_split_choice(ctx, jobs, kmax) == 2) {
+            run_jobs_split(ctx, jobs, kmax);
+            return;
+        }
+    }
+    run_jobs_direct(ctx, jobs, tf32);
+}
+
+namespace {
+
+void run_jobs_direct(Context& ctx, const std::vector<MatJob>& jobs, bool tf32) {
     if (jobs.empty()) return;
     cudaStream_t st = ctx.stream;
     std::vector<std::shared_ptr<JobTemplate>> tmpl;
@@ -1483,5 +1578,7 @@ void run_jobs(Context& ctx, const std::vector<MatJob>& jobs, bool tf32) {
     // row tiles without entries: output = beta * output
     launch_zero_tiles(ctx, tmpl, jobs, jobs_d, job0);
 }
+
+}  // namespace
 
 }  // namespace hmb

@@ -225,6 +225,18 @@ HM_API int hm_multiply_dense_tf32(hm_matrix h, double alpha, const double* B, in
                                   double beta, double* C, int ldc, int nrhs);
 HM_API int hm_set_tf32_kernel(hm_context ctx, int which);
 HM_API int hm_tf32_kernel_choice(hm_matrix h, const double* B, int ldb, int nrhs, int* which);
+/*
+ * FP64 products of 9 to 16 columns (hm_multiply_dense and the H*H sampling
+ * products) run either as one pass of the FP64 tensor-core 64 x 64 tiles (1)
+ * or as passes of at most 8 columns through the streaming kernels (2); which
+ * is faster depends on the operator.  hm_set_fp64_split(ctx, 0) (the
+ * default) times both the first time a (layout, job count, column count)
+ * occurs and keeps the faster; hm_fp64_split_choice reports (and if need be
+ * tunes) the form hm_multiply_dense uses for nrhs columns (DEVICE B).  No
+ * counterpart in the reference (it calls one BLAS routine per block).
+ */
+HM_API int hm_set_fp64_split(hm_context ctx, int which);
+HM_API int hm_fp64_split_choice(hm_matrix h, const double* B, int ldb, int nrhs, int* which);
 
 /*
  * H*H products with randomized low-rank compression.

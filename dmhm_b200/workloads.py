@@ -5,6 +5,7 @@
     python -m dmhm_b200.workloads tf32 [k]     # TF32 H x dense, mma.sync form, three products
     python -m dmhm_b200.workloads schulz64 [n] # SchulzInvert(n = 3) on the 64 x 64 operator
     python -m dmhm_b200.workloads direct       # DirectInvert on the 32 x 32 operator
+    python -m dmhm_b200.workloads hh3d [n]     # n (= 3) products A A of the 32^3 operator
 
 The 128 x 128 operator is the five-point grid operator (c ~ U[1, 2), seed
 2), numLevels 5 (64-point leaves), maxRank 16, strong admissibility, every
@@ -96,6 +97,23 @@ def direct():
     ctx.synchronize()
 
 
+def hh3d(products: int = 3):
+    """C = A A for the 32 x 32 x 32 seven-point operator (c ~ U[1, 2), seed
+    3; numLevels 4: 64-point leaves, maxRank 24, oversample 8, compression
+    tolerance 1e-10), `products` times."""
+    from .hmat import HMat3d
+    sizes = (32, 32, 32)
+    ctx = Context(0)
+    ctx.set_oversample(8)
+    ctx.set_compression_tolerance(1e-10)
+    S = operators.stencil(sizes, operators.uniform_coefficients(sizes, 3), 4)
+    A = HMat3d(S, 4, 24, True, *sizes, ctx=ctx)
+    for _ in range(products):
+        C_ = A.Multiply(1.0, A)
+        ctx.synchronize()
+        del C_
+
+
 def main(argv):
     case = argv[0] if argv else "matmul"
     arg = int(argv[1]) if len(argv) > 1 else None
@@ -109,6 +127,8 @@ def main(argv):
         schulz64(arg or 3)
     elif case == "direct":
         direct()
+    elif case == "hh3d":
+        hh3d(arg or 3)
     else:
         raise SystemExit(f"unknown workload {case}")
     print("done")

@@ -502,6 +502,33 @@ __device__ void do_round(const RoundOp& op_in, R* dyn, long long smem_elems, Rou
     }
     __syncthreads();
 
+    // ---- a dense block that is exactly zero ------------------------------
+    // (a product of two leaves whose couplings do not meet, as across a gap
+    // in the A A of a sparse operator).  Its rounding is known: Jacobi finds
+    // nothing to rotate (J = I), every column norm is zero, so the columns
+    // keep their order, and the kept columns are U = 0 and V = the unit
+    // vectors, with the rank the tolerance rule gives (1 with a tolerance,
+    // else the rank cap).  It is written directly.
+    if (dense) {
+        if (tid == 0) sh.flag = 0;
+        __syncthreads();
+        for (long long e = tid; e < (long long)m * n; e += kT)
+            if (!(Ucat[e] == R(0))) sh.flag = 1;
+        __syncthreads();
+        const bool zero = sh.flag == 0;
+        __syncthreads();
+        if (zero) {
+            int keep = min(rout, min(m, n));
+            if (op.tol > 0.0 && keep > 0) keep = 1;
+            if (tid == 0 && op.rank_out) *op.rank_out = keep;
+            for_each_entry(m, rout, [&](int i, int c) { op.uo[i + (long long)c * m] = 0.0; });
+            for_each_entry(n, rout, [&](int i, int c) {
+                op.vo[i + (long long)c * n] = (c < keep && i == c) ? 1.0 : 0.0;
+            });
+            return;
+        }
+    }
+
     // ---- QR of the stacks ------------------------------------------------
     if (!ortho && !skip_u) cta_qr(Ucat, m, k, m, tauU, red);
     if (!dense) cta_qr(Vcat, n, k, n, tauV, red);
